@@ -1,0 +1,255 @@
+/*
+ * geauxdock_b200.h -- C ABI of the B200 replica-exchange Monte Carlo docking engine.
+ *
+ * This is the drop-in boundary for the device half of GeauxDock's docking run
+ * (reference: src/run.cu:33-288 `Run`, src/kernel_cuda.cuh:5-13 kernels). Every entry
+ * point takes plain pointers and sizes, returns an int status (GD_OK == 0, negative
+ * GD_ERR_* on failure), never exits the process, and records a message retrievable
+ * with gd_last_error_string(). One context owns one CUDA stream on one device; calls
+ * on one context must not race (thread-compatible, not thread-safe).
+ *
+ * Byte layouts that the reference writes to disk or hands between its host and device
+ * halves are reproduced exactly: gd_energy == Energy (src/dock.h:108-128),
+ * gd_replica == Replica (src/dock.h:302-309), gd_record_step == LigRecordSingleStep
+ * (src/dock.h:361-367), gd_lig_record == LigRecord (src/dock.h:377-381),
+ * gd_temp == Temp (src/dock.h:288-293), gd_enepara == EnePara (src/dock_soa.h:99-137),
+ * gd_enepara_raw == EnePara0 (src/dock.h:256-272).
+ */
+#ifndef GEAUXDOCK_B200_H
+#define GEAUXDOCK_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- capacities (same values as the reference's src/size.h:19-122) ---- */
+#define GD_MAXLIG 100          /* ligand heavy atoms */
+#define GD_MAXPRO 10000        /* protein effective points */
+#define GD_MAXTP1 30           /* protein point types */
+#define GD_MAXTP2 24           /* ligand atom types */
+#define GD_MAXTP3 50           /* electrostatic point codes */
+#define GD_MAXTP4 20           /* residue codes */
+#define GD_MAXWEI 10           /* 9 energy terms + total */
+#define GD_MAXMCS 256          /* MCS fields per position */
+#define GD_MAXTMP 40           /* temperatures */
+#define GD_MAXPOS 1000         /* MCS positions */
+#define GD_MAXKDE 10000        /* KDE points */
+#define GD_STEPS_PER_DUMP 2000 /* reference record capacity (plus one for step 0) */
+#define GD_MCS_INVALID_COORD 728492.0f
+
+/* ---- status codes ---- */
+#define GD_OK 0
+#define GD_ERR_INVALID (-1)    /* bad argument or inconsistent description */
+#define GD_ERR_CUDA (-2)       /* a CUDA runtime call failed */
+#define GD_ERR_NOMEM (-3)      /* device or host allocation failed */
+#define GD_ERR_CAPACITY (-4)   /* a size exceeds a compiled capacity */
+#define GD_ERR_TIMEOUT (-5)    /* a bounded device wait gave up */
+#define GD_ERR_STATE (-6)      /* call out of order (e.g. run before init) */
+#define GD_ERR_NODEVICE (-7)   /* no usable sm_100 device */
+#define GD_ERR_RECORD_FULL (-8)/* a replica's record buffer overflowed */
+
+/* move proposal kinds */
+#define GD_MOVE_UNIFORM 0      /* m' = m + s*(2u-1): reference Move_d (src/kernel_cuda_l1_montecarlo.cu:100) */
+#define GD_MOVE_GAUSSIAN 1     /* m' = m + s*N(0,1) */
+
+/* ---- reference-identical record / state layouts ---- */
+typedef struct { float e[GD_MAXWEI]; float cms; float rmsd; } gd_energy;            /* 48 B */
+typedef struct { int idx_rep; int idx_prt; int idx_tmp; int idx_lig; } gd_replica;  /* 16 B */
+typedef struct {
+  gd_replica replica;
+  gd_energy energy;
+  float movematrix[6];     /* translation x y z, Euler rotation x y z */
+  int step;
+} gd_record_step;                                                                   /* 92 B */
+typedef struct { gd_record_step step[GD_STEPS_PER_DUMP + 1]; int next_ptr; } gd_lig_record;
+typedef struct { float t; float minus_beta; int order; } gd_temp;
+
+/* Folded force-field tables, the kernel-ready form produced by OptimizeEnepara
+ * (reference src/util.C:717-760). Indices: [ligand type][protein type]. */
+typedef struct {
+  float p1a[GD_MAXTP2][GD_MAXTP1];
+  float p2a[GD_MAXTP2][GD_MAXTP1];
+  float lj0, lj1;
+  float el0;
+  float el1;
+  float ele[GD_MAXTP3];
+  float a1;
+  float b1;
+  float pmf0[GD_MAXTP2][GD_MAXTP1];
+  float pmf1[GD_MAXTP2][GD_MAXTP1];
+  float hdb0[GD_MAXTP2][GD_MAXTP1];
+  float hdb1[GD_MAXTP2][GD_MAXTP1];
+  float hpp[GD_MAXTP4];
+  float hpl0[GD_MAXTP2];
+  float hpl1[GD_MAXTP2];
+  float hpl2[GD_MAXTP2];
+  float kde2;
+  float kde3;
+  float w[GD_MAXWEI];
+  float a_para[GD_MAXWEI];
+  float b_para[GD_MAXWEI];
+} gd_enepara;
+
+/* Raw force-field parameters as read from the `paras` file (reference EnePara0,
+ * src/dock.h:256-272; parsed by loadEnePara, src/load.C:1477-1660).
+ * Indices: [protein type][ligand type][k]. */
+typedef struct {
+  float vdw[GD_MAXTP1][GD_MAXTP2][2];
+  float ele[GD_MAXTP3];
+  float pmf[GD_MAXTP1][GD_MAXTP2][2];
+  float hpp[GD_MAXTP4];
+  float hpl[GD_MAXTP2][2];
+  float hdb[GD_MAXTP1][GD_MAXTP2][2];
+  float lj[3];
+  float el[2];
+  float kde;
+  float w[GD_MAXWEI];
+  float a_para[GD_MAXWEI];
+  float b_para[GD_MAXWEI];
+} gd_enepara_raw;
+
+/* One docking complex: what one reference `Run` call receives
+ * (src/run.h:8-19). All arrays are host pointers, copied by gd_create.
+ * Conformer-major layouts: element (conformer c, atom/point i) is at [c*count + i]. */
+typedef struct {
+  int n_lig;  /* ligand conformers (reference ComplexSize.n_lig) */
+  int n_prt;  /* protein conformers (n_prt) */
+  int n_tmp;  /* temperatures (n_tmp) */
+  int lna;    /* ligand atoms */
+  int pnp;    /* protein effective points */
+  int pnk;    /* KDE points */
+  int pos;    /* MCS positions (>= 1; the reference takes log(0/0) otherwise) */
+  /* ligand conformers: coord_orig in the ligand-centre frame, per conformer centre (lab frame) */
+  const float *lig_x, *lig_y, *lig_z;   /* [n_lig*lna] */
+  const float *lig_center;              /* [n_lig*3] */
+  const int *lig_t;                     /* [n_lig*lna] atom type 0..GD_MAXTP2-1 */
+  const float *lig_c;                   /* [n_lig*lna] charge */
+  const int *lig_n;                     /* [n_lig*lna] SDF atom number (MCS field index - 1) */
+  /* protein conformers, folded per point as CopyProteinResidue does (src/util.C:574-597) */
+  const float *prt_x, *prt_y, *prt_z;   /* [n_prt*pnp] */
+  const int *prt_t;                     /* point type 0..GD_MAXTP1-1 */
+  const int *prt_c;                     /* point class */
+  const float *prt_ele;                 /* ele[t] (t != 0) or ele[d + 30] */
+  const int *prt_seq3r;                 /* PSP column (seq3[r]) */
+  const int *prt_hflag;                 /* (c == 0 && d == 12) || c == 2 */
+  const float *prt_hpp;                 /* hpp[d] */
+  const float *pocket_center;           /* [3] */
+  /* pocket-specific potential, row-major [GD_MAXTP2][psp_ld], read at [lig type][seq3r] */
+  const float *psp;
+  int psp_ld;
+  /* KDE points */
+  const float *kde_x, *kde_y, *kde_z;   /* [pnk] */
+  const int *kde_t;                     /* [pnk] */
+  /* MCS positions: row-major [pos][mcs_ld] indexed by SDF atom number + 1 */
+  const float *mcs_x, *mcs_y, *mcs_z;
+  const float *mcs_tcc;                 /* [pos] */
+  int mcs_ld;
+  const gd_temp *temp;                  /* [n_tmp] */
+} gd_complex_desc;
+
+/* Monte Carlo parameters (reference McPara, src/dock.h:335-345, plus the RNG choice). */
+typedef struct {
+  int steps_per_exchange;   /* steps per gd_mc_run call (reference default 10) */
+  int steps_per_dump;       /* record capacity per replica is steps_per_dump + 1 */
+  float move_scale[6];      /* translation x y z, rotation x y z */
+  int move_kind;            /* GD_MOVE_UNIFORM or GD_MOVE_GAUSSIAN */
+  int record;               /* 1: append accepted steps to the per-replica records */
+  uint64_t seed;            /* Philox4x32-10 key */
+} gd_mc_params;
+
+/* CTA tile of the fused Monte Carlo kernel. */
+typedef struct {
+  int replicas_per_cta;     /* replicas sharing one protein tile in one CTA */
+  int chunk_points;         /* protein points staged per shared-memory buffer */
+} gd_tile;
+
+/* Per-replica Monte Carlo state (checkpoint unit). */
+typedef struct {
+  float movematrix_old[6];
+  gd_energy energy_old;
+  gd_replica replica;
+  int n_accept;             /* accepted MC moves */
+  int n_exchange;           /* accepted temperature swaps involving this slot */
+} gd_replica_state;
+
+typedef struct gd_ctx gd_ctx;
+
+/* ---- host-side parameter preparation (reference L2, src/util.C) ---- */
+
+/* OptimizeEnepara (src/util.C:717-760). */
+int gd_fold_enepara(const gd_enepara_raw *raw, gd_enepara *out);
+/* SetTemperature (src/util.C:797-840): geometric ladder, minus_beta = -1/T. */
+int gd_set_temperature(int num_temp, float floor_temp, float ceiling_temp, gd_temp *out);
+/* SetReplica (src/util.C:842-861): flat index n_tmp*n_lig*p + n_lig*t + l. */
+int gd_set_replica(int n_prt, int n_tmp, int n_lig, gd_replica *out);
+
+/* ---- context lifetime ---- */
+
+/* Copies every input to the device. Replaces Run's allocations and cudaMemcpyToSymbol
+ * calls (src/run.cu:57-246). Complex k's replicas occupy the global index range
+ * [offset_k, offset_k + n_prt*n_tmp*n_lig), offsets in the order given. */
+int gd_create(const gd_enepara *ff, const gd_complex_desc *complexes, int n_complexes,
+              const gd_mc_params *mc, int device, gd_ctx **out);
+int gd_destroy(gd_ctx *ctx);
+int gd_num_replicas(const gd_ctx *ctx, int *n_rep);
+int gd_replica_offset(const gd_ctx *ctx, int complex_index, int *offset);
+int gd_set_tile(gd_ctx *ctx, int complex_index, const gd_tile *tile);
+int gd_get_tile(const gd_ctx *ctx, int complex_index, gd_tile *tile);
+
+/* ---- the Monte Carlo path ---- */
+
+/* MonteCarlo_Init_d + ResetCounter_d + InitAcs_d (src/kernel_cuda_l1_montecarlo.cu:12-67,
+ * src/kernel_cuda_l1_resetcounter.cu:12-22, src/kernel_cuda_l3_util.cu:16-23): energy of
+ * the initial pose, contact reference map from each complex's first replica, step-0 record. */
+int gd_mc_init(gd_ctx *ctx);
+/* ResetCounter_d (src/kernel_cuda_l1_resetcounter.cu:12-22). */
+int gd_reset_records(gd_ctx *ctx, int rep_begin, int rep_end);
+/* MonteCarlo_d (src/kernel_cuda_l1_montecarlo.cu:72-127): steps_per_exchange steps for
+ * replicas rep_begin..rep_end (inclusive); record step numbers are s1 + s2 + s3. */
+int gd_mc_run(gd_ctx *ctx, int rep_begin, int rep_end, int s1, int s2);
+/* ExchangeReplicas_d (src/kernel_cuda_l1_exchangereplicas.cu:7-137); mode_l is accepted
+ * for signature parity and ignored (the reference only implements mode_l = 4). */
+int gd_exchange(gd_ctx *ctx, int mode_l, int mode_t);
+/* The reference's per-dump loop body (src/kernel_cuda_lancher_siglegpu.cu:25-32) over
+ * n_steps steps from step s1, captured once into a CUDA graph and replayed:
+ * gd_mc_run + (if exchange) gd_exchange with mode_t = !((s2 / steps_per_exchange) % 2). */
+int gd_mc_run_fused(gd_ctx *ctx, int s1, int n_steps, int exchange);
+int gd_sync(gd_ctx *ctx);
+
+/* ---- results ---- */
+
+/* Copies LigRecord-identical records (capacity steps_per_dump + 1 must equal
+ * GD_STEPS_PER_DUMP + 1) for rep_begin..rep_end into host[0..]. */
+int gd_get_records(gd_ctx *ctx, gd_lig_record *host, int rep_begin, int rep_end);
+/* Same data for any capacity: steps[(r - rep_begin) * cap + i], next_ptr[r - rep_begin]. */
+int gd_get_records_raw(gd_ctx *ctx, gd_record_step *steps, int *next_ptr, int rep_begin,
+                       int rep_end, int cap);
+int gd_get_etotal(gd_ctx *ctx, float *etotal, int rep_begin, int rep_end);
+int gd_get_replicas(gd_ctx *ctx, gd_replica *replicas, int rep_begin, int rep_end);
+int gd_get_state(gd_ctx *ctx, gd_replica_state *state, int rep_begin, int rep_end);
+int gd_set_state(gd_ctx *ctx, const gd_replica_state *state, int rep_begin, int rep_end);
+/* Device-side error word of the last kernels (0 when clean). */
+int gd_get_device_error(gd_ctx *ctx, int *code);
+
+/* Energy (9 normalized terms, weighted total, cms, rmsd) of n_poses poses given as
+ * movematrix[6] each, for one (complex, protein conformer, ligand conformer).
+ * cms is measured against the complex's contact reference (built by gd_mc_init). */
+int gd_eval_energy(gd_ctx *ctx, int complex_index, int prt_conf, int lig_conf,
+                   const float *movematrix, int n_poses, gd_energy *out);
+
+/* Per-step trace for bit-exact replay: when enabled, gd_mc_run logs for each replica and
+ * step the proposal's total energy and the accept flag; trace[(r * max_steps) + s]. */
+int gd_trace_enable(gd_ctx *ctx, int max_steps);
+int gd_trace_get(gd_ctx *ctx, float *e_new_total, int *accepted, int *n_steps);
+
+const char *gd_last_error_string(void);
+const char *gd_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GEAUXDOCK_B200_H */
