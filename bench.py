@@ -1,0 +1,373 @@
+"""Throughput of the replica-exchange Monte Carlo docking path (MC replica-steps/s).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: config 1 (P = 3,000 protein points x 11 conformers, L = 40 ligand atoms x 31
+conformers, 20 temperatures: 6,820 replicas; Gaussian moves; exchange every 10 steps), seeded
+synthetic data. One bench step = one exchange interval: 10 MC steps of every replica
+(gd_mc_run) + one temperature exchange (gd_exchange). K timed steps after W warm-up steps.
+
+ours:      device time from CUDA events recorded on the library's own stream around each
+           step, L2 flushed between steps (outside the events), max over ranks; `e2e` is a
+           whole run through the C ABI from host buffers (gd_create uploads, init, K steps,
+           record download) timed on the host; `cpu_baseline` is the oracle's FP32 OpenMP
+           restatement on a bounded sample (rank 0, N = 1).
+reference: the reference's path restated on the host cores (the reference's own hot path is
+           GPU-only and its CPU port does not build): the oracle's FP32 OpenMP Monte Carlo on
+           a bounded sample per step, all host threads, same metric.
+Multi-GPU (torchrun): every rank runs its own config-1 system (own RNG stream), no data-path
+collective (replicas shard without exchange across shards): weak scaling.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "MC replica-steps/s (plain batched REMC)"
+UNIT = "replica-steps/s"
+
+
+def load_raw():
+    from geaxdock_gpu_b200 import abi
+    z = np.load(os.path.join(ROOT, "tests", "golden", "ref_1a07C1.npz"))
+    return abi.enepara_raw_from_array(z["enepara_raw"])
+
+
+def workload(seed):
+    from geaxdock_gpu_b200 import system
+    return system.config(1, load_raw(), seed=seed)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax.append(float(p[2]))
+                power.append(float(p[3]))
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "power_w_median": statistics.median(power) if power else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def algorithmic_flops_per_replica_step(eng, w, n_sample=24):
+    """FLOPs per replica-step by the counting convention: 36 per ligand-protein pair, plus
+    hpc 12 / hdb 8 / psp 1 per conditional hit, KDE 11 per matched pair, MCS 9 per valid atom,
+    with the hit counts measured by the oracle on a sample of the current poses."""
+    from oracle import pyoracle as po
+    cx, ff = w.complexes[0], w.ff
+    st = eng.state()
+    rm = po.ref_map(ff, cx)
+    rng = np.random.default_rng(0)
+    tot = 0.0
+    picks = rng.choice(cx.n_rep, n_sample, replace=False)
+    for r in picks:
+        p = r // (cx.n_tmp * cx.n_lig)
+        l = r % cx.n_lig
+        o = po.pose_energy(ff, cx, int(p), int(l), st["movematrix_old"][r], rm, 64)
+        tot += (36.0 * cx.lna * cx.pnp + 12.0 * o["hits_hpc"] + 8.0 * o["hits_hdb"] +
+                1.0 * o["hits_psp"] + 11.0 * o["hits_kde"] + 9.0 * o["hits_mcs"])
+    return tot / n_sample
+
+
+def cpu_baseline_sample(w, seconds=12.0, nthreads=0):
+    """Oracle FP32 OpenMP restatement on a bounded replica sample of the same workload."""
+    from oracle import pyoracle as po
+    cx, ff = w.complexes[0], w.ff
+    params = w.params
+    params.record = 0
+    mc = po.MC(ff, cx, params, stream=0, precision=32)
+    mc.init()
+    nt = nthreads or po.max_threads()
+    t0 = time.perf_counter()
+    mc.run_range(0, nt, 0, 0, 1, nt)  # probe: one step on nt replicas
+    rate = nt / max(time.perf_counter() - t0, 1e-3)  # replica-steps/s
+    n_rep = int(min(cx.n_rep, max(nt, nt * round(seconds * rate / 10 / nt))))
+    t0 = time.perf_counter()
+    mc.run_range(0, n_rep, 0, 1, 10, nt)
+    dt = time.perf_counter() - t0
+    return {"value": n_rep * 10 / dt, "unit": UNIT, "cores": nt, "kind": "port",
+            "sample": "%d replicas x 10 MC steps of the config-1 system (%.1f s)" % (n_rep, dt)}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from oracle import pyoracle as po
+    w = workload(42)
+    cx, ff, params = w.complexes[0], w.ff, w.params
+    params.record = 0
+    nt = po.max_threads()
+    mc = po.MC(ff, cx, params, stream=0, precision=32)
+    mc.init()
+    t0 = time.perf_counter()
+    mc.run_range(0, nt, 0, 0, 1, nt)
+    per_batch = max(time.perf_counter() - t0, 1e-3)  # one step of nt replicas
+    n_rep = int(min(cx.n_rep, max(nt, nt * int(2.0 / (10 * per_batch)))))
+    s2 = 0
+    for _ in range(args.warmup):
+        mc.run_range(0, n_rep, 0, s2, 10, nt)
+        s2 += 10
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        mc.run_range(0, n_rep, 0, s2, 10, nt)
+        times.append(time.perf_counter() - t0)
+        s2 += 10
+    tot = sum(times)
+    value = n_rep * 10 * args.steps / tot
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic (seeded, config-1 shapes)", "impl": "reference",
+           "config": {"workload": "config1: P=3000 x 11 conf, L=40 x 31 conf, T=20, 6820 "
+                                  "replicas, gaussian moves, exchange/10",
+                      "replicas_sampled": n_rep},
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": nt, "kind": "port",
+                            "sample": "%d of 6820 replicas x 10 MC steps per bench step" % n_rep},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from geaxdock_gpu_b200 import abi, engine
+
+    dev = local_rank
+    torch.cuda.set_device(dev)
+    w = workload(42 + rank)
+    cx, ff, params = w.complexes[0], w.ff, w.params
+    spe = params.steps_per_exchange
+    intervals_per_dump = params.steps_per_dump // spe
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+
+    # ---------------- device-timed throughput ----------------
+    eng = engine.Engine(ff, [cx], params, device=dev)
+    stream = torch.cuda.ExternalStream(eng.cuda_stream(), device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda:%d" % dev)
+    eng.mc_init()
+    eng.sync()
+    it = 0
+
+    def one_step(ev=None):
+        nonlocal it
+        if it and it % intervals_per_dump == 0:
+            eng.reset_records()
+        s1 = (it // intervals_per_dump) * params.steps_per_dump
+        s2 = (it % intervals_per_dump) * spe
+        if ev is not None:
+            ev[0].record(stream)
+        eng.mc_run(s1, s2)
+        if ev is not None:
+            ev[1].record(stream)
+        eng.exchange(int(not ((s2 // spe) % 2)))
+        if ev is not None:
+            ev[2].record(stream)
+        it += 1
+
+    for _ in range(args.warmup):
+        one_step()
+    eng.sync()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    clocks = ClockSampler(dev)
+    clocks.start()
+    evs = []
+    for _ in range(args.steps):
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        one_step(e)
+        with torch.cuda.stream(stream):
+            flush.add_(1.0)  # 256 MB write between steps: L2 (126 MB) flushed
+        evs.append(e)
+    eng.sync()
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop()
+    step_ms = [a.elapsed_time(c) for a, b, c in evs]
+    mc_ms = [a.elapsed_time(b) for a, b, c in evs]
+    tot_ms = sum(step_ms)
+    if dist:
+        t = torch.tensor([tot_ms], dtype=torch.float64, device="cuda:%d" % dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tot_ms = float(t.item())
+    rs_per_step = cx.n_rep * spe
+    value = world * rs_per_step * args.steps / (tot_ms * 1e-3)
+    flops_rs = algorithmic_flops_per_replica_step(eng, w) if rank == 0 else 0.0
+    eng.close()
+    del flush
+
+    if rank != 0:
+        return
+    mc_avg_ms = sum(mc_ms) / len(mc_ms)
+    flops_launch = flops_rs * rs_per_step
+    achieved = flops_launch / (mc_avg_ms * 1e-3) / 1e12
+    peak = None
+    try:
+        import ctypes as C
+        v = C.c_double()
+        if engine.lib().gd_probe_fp32_peak(dev, 5, C.byref(v)) == 0:
+            peak = v.value
+    except Exception:
+        peak = None
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "gd_mc_kernel_config1_traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get("bytes_per_launch")
+        except Exception:
+            traffic = None
+    roofline = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": (achieved / peak) if peak else None, "traffic": traffic,
+                "kernel": "gd_mc_kernel", "launch_ms": mc_avg_ms,
+                "flop_per_replica_step": flops_rs,
+                "peak_source": "measured FP32 FMA probe (gd_probe_fp32_peak), same run"}
+
+    # ---------------- end to end through the C ABI (host buffers) ----------------
+    e2e = None
+    if not args.no_e2e:
+        import ctypes as C
+        h2d = 0
+        for name in ("lig_x", "lig_y", "lig_z", "lig_center", "lig_t", "lig_c", "lig_n", "prt_x",
+                     "prt_y", "prt_z", "prt_t", "prt_c", "prt_ele", "prt_seq3r", "prt_hflag",
+                     "prt_hpp", "psp", "kde_x", "kde_y", "kde_z", "kde_t", "mcs_x", "mcs_y",
+                     "mcs_z", "mcs_tcc", "temp"):
+            h2d += getattr(cx, name).nbytes
+        h2d += C.sizeof(abi.EnePara)
+        t0 = time.perf_counter()
+        e = engine.Engine(ff, [cx], params, device=dev)
+        e.mc_init()
+        it2 = 0
+        d2h = 0
+        for _ in range(args.steps):
+            if it2 and it2 % intervals_per_dump == 0:
+                e.reset_records()
+            s2 = (it2 % intervals_per_dump) * spe
+            e.mc_run((it2 // intervals_per_dump) * params.steps_per_dump, s2)
+            e.exchange(int(not ((s2 // spe) % 2)))
+            et = e.etotal()  # the step's result read back to the host
+            d2h += et.nbytes
+            it2 += 1
+        steps, nxt = e.records()
+        d2h += steps.nbytes + nxt.nbytes
+        e.close()
+        dt = time.perf_counter() - t0
+        e2e = {"value": rs_per_step * args.steps / dt, "unit": UNIT,
+               "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+               "scope": "gd_create + gd_mc_init + K x (gd_mc_run + gd_exchange + gd_get_etotal)"
+                        " + gd_get_records_raw + gd_destroy, host wall clock"}
+
+    cpu = None
+    if world == 1 and not args.no_cpu:
+        cpu = cpu_baseline_sample(w)
+
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic (seeded, config-1 shapes)",
+           "config": {"workload": "config1: P=3000 x 11 conf, L=40 x 31 conf, T=20, 6820 "
+                                  "replicas per GPU, gaussian moves, exchange/10",
+                      "step": "10 MC steps + 1 exchange, all replicas",
+                      "l2": "flushed between steps (256 MB write)",
+                      "tile": list(engine_tile(cx, ff, params, dev)),
+                      "parallelism": "replica shards, no collective" if world > 1 else "1 GPU"},
+           "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+           "gpu_launches": 2 * args.steps + args.steps // max(1, intervals_per_dump)}
+    print(json.dumps(out), flush=True)
+
+
+def engine_tile(cx, ff, params, dev):
+    from geaxdock_gpu_b200 import engine
+    with engine.Engine(ff, [cx], params, device=dev) as e:
+        return e.tile()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

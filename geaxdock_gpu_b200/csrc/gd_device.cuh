@@ -1,0 +1,114 @@
+/*
+ * gd_device.cuh -- device-resident data layout of the B200 Monte Carlo docking engine.
+ *
+ * HBM layout (one context, all complexes of a batch):
+ *   ligand conformers   float4 (x, y, z, charge) + int2 (type, MCS field) per atom,
+ *                       conformer-major; placed coordinates never touch HBM.
+ *   protein conformers  points sorted by (point type, kind) per conformer and padded to a
+ *                       multiple of 4: float4 (x, y, z, ele) + float2 (hydrophobic hpp or 0,
+ *                       PSP column or -1) per point; a segment table (start, end, type, kind)
+ *                       per conformer. kind 0: plain, 1: hydrophobic, 2: hydrophobic + PSP.
+ *   pair parameters     per (ligand type, protein type) 12 floats, folded for the kernel.
+ *   contact reference   per conformer and ligand atom, the list of reference contacts as
+ *                       float4 (x, y, z, contact threshold): tp is counted over this sparse
+ *                       list, so the pair loop only counts contacts.
+ *   replica state       movematrix_old[6], Energy (48 B), Replica (16 B), counters; records
+ *                       in the reference's LigRecordSingleStep layout.
+ * Protein tiles are staged from HBM/L2 into shared memory with cp.async.bulk (TMA engine)
+ * into a double buffer completed on mbarriers.
+ */
+#ifndef GD_DEVICE_CUH
+#define GD_DEVICE_CUH
+
+#include <cstdint>
+
+#include "../../include/geauxdock_b200.h"
+
+#define GD_MAX_SEG 96          /* (30 point types) x (3 kinds), rounded up */
+#define GD_MAX_TPB 512
+#define GD_MAX_SLOTS 128       /* replicas per CTA */
+#define GD_NQ 12               /* per-lane partial sums handed to the reducer */
+
+/* device error word bits */
+#define GD_DEV_ERR_TIMEOUT 1
+#define GD_DEV_ERR_RECORD_FULL 2
+#define GD_DEV_ERR_CONFIG 4
+
+struct GdPairParam {
+  float p1a, p2a, p1l, thr;    /* LJ numerators; p1a*lj0; contact threshold on d^2 */
+  float pmf0, pmf1, hc1, hc0;  /* pmf; hdb argument h = r*hc1 + hc0 (scaled for exp2) */
+  float hs, hneed, pad0, pad1; /* hdb scale (0 when hdb0 <= 0.1); 1 if the hdb term is live */
+};
+
+struct GdDevComplex {
+  int n_lig, n_prt, n_tmp, lna;
+  int pnp, pnp_pad, pnk, pos;
+  int rep_offset, n_rep, psp_ld, mcs_ld;
+  int stream, nref_total, pad0, pad1;
+  float pocket[4];
+  const float4 *lig_pos;      /* [n_lig*lna] */
+  const int2 *lig_meta;       /* [n_lig*lna] type, MCS index (n + 1) */
+  const float *lig_center;    /* [n_lig*3] */
+  const float4 *pt_pos;       /* [n_prt*pnp_pad] */
+  const float2 *pt_aux;       /* [n_prt*pnp_pad] */
+  const int4 *seg;            /* [n_prt*GD_MAX_SEG] */
+  const int *seg_count;       /* [n_prt] */
+  const float4 *kde;          /* [pnk] x, y, z, type (exact small integer as float) */
+  const float *mcs_x, *mcs_y, *mcs_z; /* [pos*mcs_ld] */
+  const float *mcs_tcc;       /* [pos] */
+  const float *psp;           /* [GD_MAXTP2*psp_ld] */
+  const float *minus_beta;    /* [n_tmp] */
+  const int *ref_start;       /* [n_prt*(lna+1)] */
+  const float4 *ref_pts;      /* [ref_start[n_prt*(lna+1)-1]] */
+};
+
+/* One CTA's unit of work: `count` consecutive replicas of one protein conformer. */
+struct GdTileDesc {
+  int complex_index, prt_conf, rep_begin, count;  /* rep_begin: global replica index */
+};
+
+struct GdForceConst {
+  float lj1, el0, el1, a1, b1, inv_el1;
+  float kde2, kde3;
+  float a_para[GD_MAXWEI], b_para[GD_MAXWEI], w[GD_MAXWEI];
+  float hpl0[GD_MAXTP2], hpl1[GD_MAXTP2], hpl2[GD_MAXTP2];
+};
+
+/* Arguments of the fused Monte Carlo / energy kernel. */
+struct GdMcArgs {
+  const GdDevComplex *cx;     /* [n_complex] */
+  const GdPairParam *pp;      /* [GD_MAXTP2*GD_MAXTP1] */
+  const GdTileDesc *tiles;    /* [n_tiles] */
+  int n_tiles;
+  int *tile_counter;          /* persistent-CTA work queue head */
+  int mode;                   /* 0: MC steps, 1: init (energy at movematrix 0), 2: eval poses */
+  int n_steps;                /* steps in this launch (mode 0) */
+  int step0;                  /* step number of the first step (s1 + s2), added to *step_base */
+  const int *step_base;       /* device cursor for graph replays (null: 0) */
+  int chunk;                  /* protein points per shared-memory buffer (multiple of 4) */
+  int move_kind;
+  uint64_t seed;
+  float move_scale[6];
+  /* replica state, global replica index */
+  gd_replica *replica;
+  float *mm_old;              /* [n_rep*6] */
+  gd_energy *e_old;
+  float *etotal;
+  int *n_accept;
+  /* records */
+  gd_record_step *rec;        /* [n_rep*rec_cap] or null */
+  int *rec_next;              /* [n_rep] */
+  int rec_cap;
+  /* trace (replay) */
+  float *trace_e;             /* [n_rep*trace_cap] or null */
+  int *trace_acc;
+  int trace_cap, trace_step0;
+  /* pose evaluation (mode 2): pose i of the tile uses mm_in[(rep_begin - 0 + j)*6] */
+  const float *mm_in;
+  const int *lig_conf_in;     /* per pose ligand conformer (mode 2) */
+  gd_energy *e_out;
+  unsigned *err;              /* device error word */
+  long long timeout_ns;       /* bounded waits */
+};
+
+#endif

@@ -166,12 +166,14 @@ GD_HD void gd_box_muller(uint32_t a, uint32_t b, float *z0, float *z1) {
 }
 
 /* ---------------- proposal for one replica and one step ---------------- */
-/* Draws the six move deltas and the accept uniform for (replica, step). */
-GD_HD void gd_draw_step(uint64_t seed, uint32_t replica, uint32_t step, int move_kind,
-                        const float scale[6], float delta[6], float *u_accept) {
+/* Draws the six move deltas and the accept uniform for (stream, replica, step).
+ * stream identifies the complex (so a complex run alone or inside a batch draws the same
+ * numbers); replica is the complex-local flat index n_tmp*n_lig*p + n_lig*t + l. */
+GD_HD void gd_draw_step(uint64_t seed, uint32_t stream, uint32_t replica, uint32_t step,
+                        int move_kind, const float scale[6], float delta[6], float *u_accept) {
   const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
-  const gd_u32x4 a = gd_philox4x32_10(replica, step, 0u, GD_RNG_MOVE, k0, k1);
-  const gd_u32x4 b = gd_philox4x32_10(replica, step, 0u, GD_RNG_MOVE2, k0, k1);
+  const gd_u32x4 a = gd_philox4x32_10(replica, step, stream, GD_RNG_MOVE, k0, k1);
+  const gd_u32x4 b = gd_philox4x32_10(replica, step, stream, GD_RNG_MOVE2, k0, k1);
   if (move_kind == 1) {
     float z[6];
     gd_box_muller(a.v[0], a.v[1], &z[0], &z[1]);
@@ -185,11 +187,12 @@ GD_HD void gd_draw_step(uint64_t seed, uint32_t replica, uint32_t step, int move
   *u_accept = gd_u01(b.v[2]);
 }
 
-/* Exchange uniform for (complex-local group, exchange call, pair). */
-GD_HD float gd_draw_exchange(uint64_t seed, uint32_t group, uint32_t exchange_call,
-                             uint32_t pair) {
-  const gd_u32x4 a = gd_philox4x32_10(group, exchange_call, pair, GD_RNG_EXCHANGE,
-                                      (uint32_t)seed, (uint32_t)(seed >> 32));
+/* Exchange uniform for (stream, complex-local group p*n_lig + l, exchange call, pair). */
+GD_HD float gd_draw_exchange(uint64_t seed, uint32_t stream, uint32_t group,
+                             uint32_t exchange_call, uint32_t pair) {
+  const gd_u32x4 a = gd_philox4x32_10(group, exchange_call, stream,
+                                      GD_RNG_EXCHANGE | (pair << 8), (uint32_t)seed,
+                                      (uint32_t)(seed >> 32));
   return gd_u01(a.v[0]);
 }
 

@@ -1,0 +1,277 @@
+"""Host-side mirror of the reference's docking run over the C ABI.
+
+The reference drives its kernels from `Run` (src/run.cu:33-288) with the loop in
+src/kernel_cuda_lancher_siglegpu.cu:17-63: ResetCounter_d + MonteCarlo_Init_d, then per dump
+MonteCarlo_d every steps_per_exchange steps, ExchangeReplicas_d with alternating mode_t, a
+LigRecord download and an append of accepted steps to map<int, vector<LigRecordSingleStep>>.
+`Engine` exposes the same operations (`mc_init`, `mc_run`, `exchange`, `reset_records`,
+`records`) plus the graph-captured fused loop (`run_fused`) and `run`, the whole reference
+loop. Every call goes to libgeauxdock_b200.so; there is no CPU path: if the library or a
+B200 is missing the constructor raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Dict, List, Sequence
+
+import numpy as np
+
+from . import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgeauxdock_b200.so")
+
+_lib = None
+
+
+class GDError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__("geauxdock error %d: %s" % (code, msg))
+        self.code = code
+
+
+def lib() -> C.CDLL:
+    """Loads the CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError("libgeauxdock_b200.so is missing; run `python -m geaxdock_gpu_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    vp, ip, fp = C.c_void_p, C.POINTER(C.c_int), abi.FP
+    sig = {
+        "gd_fold_enepara": [C.POINTER(abi.EneParaRaw), C.POINTER(abi.EnePara)],
+        "gd_set_temperature": [C.c_int, C.c_float, C.c_float, C.POINTER(abi.Temp)],
+        "gd_set_replica": [C.c_int, C.c_int, C.c_int, C.POINTER(abi.Replica)],
+        "gd_create": [C.POINTER(abi.EnePara), C.POINTER(abi.ComplexDesc), C.c_int,
+                      C.POINTER(abi.McParams), C.c_int, C.POINTER(vp)],
+        "gd_destroy": [vp],
+        "gd_num_replicas": [vp, ip],
+        "gd_replica_offset": [vp, C.c_int, ip],
+        "gd_set_tile": [vp, C.c_int, C.POINTER(abi.Tile)],
+        "gd_get_tile": [vp, C.c_int, C.POINTER(abi.Tile)],
+        "gd_mc_init": [vp],
+        "gd_reset_records": [vp, C.c_int, C.c_int],
+        "gd_mc_run": [vp, C.c_int, C.c_int, C.c_int, C.c_int],
+        "gd_exchange": [vp, C.c_int, C.c_int],
+        "gd_mc_run_fused": [vp, C.c_int, C.c_int, C.c_int],
+        "gd_sync": [vp],
+        "gd_get_records": [vp, vp, C.c_int, C.c_int],
+        "gd_get_records_raw": [vp, vp, vp, C.c_int, C.c_int, C.c_int],
+        "gd_get_etotal": [vp, fp, C.c_int, C.c_int],
+        "gd_get_replicas": [vp, vp, C.c_int, C.c_int],
+        "gd_get_state": [vp, vp, C.c_int, C.c_int],
+        "gd_set_state": [vp, vp, C.c_int, C.c_int],
+        "gd_get_device_error": [vp, ip],
+        "gd_eval_energy": [vp, C.c_int, C.c_int, C.c_int, fp, C.c_int, vp],
+        "gd_trace_enable": [vp, C.c_int],
+        "gd_trace_get": [vp, fp, ip, ip],
+        "gd_get_stream": [vp, C.POINTER(vp)],
+        "gd_set_rng_stream": [vp, C.c_int, C.c_int],
+        "gd_set_wait_timeout": [vp, C.c_longlong],
+    }
+    for name, args in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = C.c_int
+    L.gd_last_error_string.restype = C.c_char_p
+    L.gd_version.restype = C.c_char_p
+    _lib = L
+    return L
+
+
+def check(rc: int):
+    if rc != abi.GD_OK:
+        raise GDError(rc, lib().gd_last_error_string().decode())
+
+
+def fold_enepara(raw: abi.EneParaRaw) -> abi.EnePara:
+    """OptimizeEnepara (src/util.C:717-760) through the library."""
+    out = abi.EnePara()
+    check(lib().gd_fold_enepara(C.byref(raw), C.byref(out)))
+    return out
+
+
+def set_temperature(n: int, floor_t: float, ceil_t: float) -> np.ndarray:
+    """SetTemperature (src/util.C:797-840)."""
+    t = (abi.Temp * n)()
+    check(lib().gd_set_temperature(n, floor_t, ceil_t, t))
+    return np.frombuffer(bytes(t), dtype=abi.TEMP_DTYPE).copy()
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class Engine:
+    """One B200 context: a batch of complexes, their replicas and records."""
+
+    def __init__(self, ff: abi.EnePara, complexes: Sequence[abi.ComplexArrays],
+                 params: abi.McParams, device: int = 0):
+        self.complexes = list(complexes)
+        self.params = params
+        self.ff = ff
+        descs = (abi.ComplexDesc * len(self.complexes))(*[c.desc() for c in self.complexes])
+        h = C.c_void_p()
+        check(lib().gd_create(C.byref(ff), descs, len(self.complexes), C.byref(params), device,
+                              C.byref(h)))
+        self.h = h
+        n = C.c_int()
+        check(lib().gd_num_replicas(self.h, C.byref(n)))
+        self.n_rep = n.value
+        self.offsets = []
+        for k in range(len(self.complexes)):
+            o = C.c_int()
+            check(lib().gd_replica_offset(self.h, k, C.byref(o)))
+            self.offsets.append(o.value)
+        self.cap = params.steps_per_dump + 1
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().gd_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- reference-shaped operations ----
+    def mc_init(self):
+        check(lib().gd_mc_init(self.h))
+
+    def reset_records(self, r0=0, r1=None):
+        check(lib().gd_reset_records(self.h, r0, self.n_rep - 1 if r1 is None else r1))
+
+    def mc_run(self, s1: int, s2: int, r0=0, r1=None):
+        check(lib().gd_mc_run(self.h, r0, self.n_rep - 1 if r1 is None else r1, s1, s2))
+
+    def exchange(self, mode_t: int, mode_l: int = 4):
+        check(lib().gd_exchange(self.h, mode_l, mode_t))
+
+    def run_fused(self, s1: int, n_steps: int, exchange: bool = True):
+        check(lib().gd_mc_run_fused(self.h, s1, n_steps, 1 if exchange else 0))
+
+    def sync(self):
+        check(lib().gd_sync(self.h))
+
+    def set_tile(self, replicas_per_cta: int, chunk_points: int, complex_index: int = -1):
+        t = abi.Tile()
+        t.replicas_per_cta, t.chunk_points = replicas_per_cta, chunk_points
+        check(lib().gd_set_tile(self.h, complex_index, C.byref(t)))
+
+    def cuda_stream(self) -> int:
+        """The context's cudaStream_t as an integer handle."""
+        s = C.c_void_p()
+        check(lib().gd_get_stream(self.h, C.byref(s)))
+        return s.value or 0
+
+    def set_rng_stream(self, complex_index: int, stream: int):
+        check(lib().gd_set_rng_stream(self.h, complex_index, stream))
+
+    def set_wait_timeout(self, ns: int):
+        check(lib().gd_set_wait_timeout(self.h, ns))
+
+    def tile(self, complex_index=0):
+        t = abi.Tile()
+        check(lib().gd_get_tile(self.h, complex_index, C.byref(t)))
+        return t.replicas_per_cta, t.chunk_points
+
+    # ---- results ----
+    def records(self, r0=0, r1=None):
+        r1 = self.n_rep - 1 if r1 is None else r1
+        n = r1 - r0 + 1
+        steps = np.zeros((n, self.cap), abi.RECORD_DTYPE)
+        nxt = np.zeros(n, np.int32)
+        check(lib().gd_get_records_raw(self.h, _p(steps), _p(nxt), r0, r1, self.cap))
+        return steps, nxt
+
+    def lig_records(self, r0=0, r1=None) -> bytes:
+        """LigRecord array bytes (reference layout, src/dock.h:377-381)."""
+        r1 = self.n_rep - 1 if r1 is None else r1
+        buf = (abi.LigRecord * (r1 - r0 + 1))()
+        check(lib().gd_get_records(self.h, buf, r0, r1))
+        return bytes(buf)
+
+    def etotal(self, r0=0, r1=None):
+        r1 = self.n_rep - 1 if r1 is None else r1
+        out = np.zeros(r1 - r0 + 1, np.float32)
+        check(lib().gd_get_etotal(self.h, abi.fptr(out), r0, r1))
+        return out
+
+    def replicas(self, r0=0, r1=None):
+        r1 = self.n_rep - 1 if r1 is None else r1
+        out = np.zeros(r1 - r0 + 1, abi.REPLICA_DTYPE)
+        check(lib().gd_get_replicas(self.h, _p(out), r0, r1))
+        return out
+
+    def state(self, r0=0, r1=None):
+        r1 = self.n_rep - 1 if r1 is None else r1
+        out = np.zeros(r1 - r0 + 1, abi.STATE_DTYPE)
+        check(lib().gd_get_state(self.h, _p(out), r0, r1))
+        return out
+
+    def set_state(self, st: np.ndarray, r0=0):
+        st = np.ascontiguousarray(st, abi.STATE_DTYPE)
+        check(lib().gd_set_state(self.h, _p(st), r0, r0 + st.shape[0] - 1))
+
+    def device_error(self) -> int:
+        e = C.c_int()
+        check(lib().gd_get_device_error(self.h, C.byref(e)))
+        return e.value
+
+    def eval_energy(self, complex_index: int, prt_conf: int, lig_conf: int,
+                    movematrix: np.ndarray) -> np.ndarray:
+        mm = np.ascontiguousarray(movematrix, np.float32).reshape(-1, 6)
+        out = np.zeros(mm.shape[0], abi.ENERGY_DTYPE)
+        check(lib().gd_eval_energy(self.h, complex_index, prt_conf, lig_conf, abi.fptr(mm),
+                                   mm.shape[0], _p(out)))
+        return out
+
+    def trace_enable(self, max_steps: int):
+        check(lib().gd_trace_enable(self.h, max_steps))
+        self._trace_cap = max_steps
+
+    def trace(self):
+        e = np.zeros((self.n_rep, self._trace_cap), np.float32)
+        a = np.zeros((self.n_rep, self._trace_cap), np.int32)
+        n = C.c_int()
+        check(lib().gd_trace_get(self.h, abi.fptr(e), a.ctypes.data_as(C.POINTER(C.c_int)),
+                                 C.byref(n)))
+        return e, a
+
+    # ---- the reference's whole docking loop ----
+    def run(self, min_records: int, exchange: bool = True, max_dumps: int = 1000) \
+            -> Dict[int, List[np.void]]:
+        """Run (src/run.cu) + kernel_cuda_lancher_siglegpu.cu: dumps of steps_per_dump steps
+        until at least `min_records` accepted steps are gathered; returns the per-replica
+        lists of accepted steps (map<int, vector<LigRecordSingleStep>>)."""
+        spd, spe = self.params.steps_per_dump, self.params.steps_per_exchange
+        out: Dict[int, List[np.void]] = {r: [] for r in range(self.n_rep)}
+        self.reset_records()
+        self.mc_init()
+        s1, total = 0, 0
+        for _ in range(max_dumps):
+            if total >= min_records:
+                break
+            if s1 != 0:
+                self.reset_records()
+            for s2 in range(0, spd, spe):
+                self.mc_run(s1, s2)
+                if exchange:
+                    self.exchange(int(not ((s2 // spe) % 2)))
+            steps, nxt = self.records()
+            for r in range(self.n_rep):
+                out[r].extend(steps[r, :nxt[r]])
+                total += int(nxt[r])
+            s1 += spd
+        self.steps_total = s1
+        return out

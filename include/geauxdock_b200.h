@@ -196,8 +196,16 @@ int gd_create(const gd_enepara *ff, const gd_complex_desc *complexes, int n_comp
 int gd_destroy(gd_ctx *ctx);
 int gd_num_replicas(const gd_ctx *ctx, int *n_rep);
 int gd_replica_offset(const gd_ctx *ctx, int complex_index, int *offset);
+/* Tile of the fused kernel for one complex (-1: all); one CTA size per context. */
 int gd_set_tile(gd_ctx *ctx, int complex_index, const gd_tile *tile);
 int gd_get_tile(const gd_ctx *ctx, int complex_index, gd_tile *tile);
+/* RNG stream id of a complex (default: its index in the batch). Draws depend only on
+ * (seed, stream, complex-local replica, step), so a complex run alone with the stream id it
+ * has in a batch reproduces its batched trajectory. */
+int gd_set_rng_stream(gd_ctx *ctx, int complex_index, int stream);
+/* Limit (ns) of every bounded device wait; a wait that runs out ends the kernel with
+ * GD_ERR_TIMEOUT from gd_sync. Default 2 s. */
+int gd_set_wait_timeout(gd_ctx *ctx, long long timeout_ns);
 
 /* ---- the Monte Carlo path ---- */
 
@@ -218,6 +226,8 @@ int gd_exchange(gd_ctx *ctx, int mode_l, int mode_t);
  * gd_mc_run + (if exchange) gd_exchange with mode_t = !((s2 / steps_per_exchange) % 2). */
 int gd_mc_run_fused(gd_ctx *ctx, int s1, int n_steps, int exchange);
 int gd_sync(gd_ctx *ctx);
+/* The context's CUDA stream (a cudaStream_t), for callers that order or time work on it. */
+int gd_get_stream(gd_ctx *ctx, void **stream);
 
 /* ---- results ---- */
 
@@ -247,6 +257,10 @@ int gd_trace_get(gd_ctx *ctx, float *e_new_total, int *accepted, int *n_steps);
 
 const char *gd_last_error_string(void);
 const char *gd_version(void);
+
+/* Measured FP32 FMA throughput of `device` in TFLOP/s (2 FLOP per FMA, best of `repeats`):
+ * the roofline denominator for the FP32-bound pair-energy kernel. No reference counterpart. */
+int gd_probe_fp32_peak(int device, int repeats, double *tflops);
 
 #ifdef __cplusplus
 }

@@ -209,10 +209,10 @@ float gdo_expf(float x) { return gd_expf(x); }
 float gdo_logf(float x) { return gd_logf(x); }
 void gdo_sincosf(float x, float *s, float *c) { gd_sincosf(x, s, c); }
 
-void gdo_draw_steps(uint64_t seed, int move_kind, const float scale[6], int n,
+void gdo_draw_steps(uint64_t seed, uint32_t stream, int move_kind, const float scale[6], int n,
                     const uint32_t *replica, const uint32_t *step, float *delta6, float *u) {
   for (int i = 0; i < n; ++i)
-    gd_draw_step(seed, replica[i], step[i], move_kind, scale, delta6 + 6 * i, u + i);
+    gd_draw_step(seed, stream, replica[i], step[i], move_kind, scale, delta6 + 6 * i, u + i);
 }
 
 void gdo_metropolis_batch(int n, const float *e_new, const float *e_old, const float *mb,
@@ -220,8 +220,9 @@ void gdo_metropolis_batch(int n, const float *e_new, const float *e_old, const f
   for (int i = 0; i < n; ++i) out[i] = gd_metropolis(e_new[i], e_old[i], mb[i], u[i]);
 }
 
-float gdo_draw_exchange(uint64_t seed, uint32_t group, uint32_t call, uint32_t pair) {
-  return gd_draw_exchange(seed, group, call, pair);
+float gdo_draw_exchange(uint64_t seed, uint32_t stream, uint32_t group, uint32_t call,
+                        uint32_t pair) {
+  return gd_draw_exchange(seed, stream, group, call, pair);
 }
 
 int gdo_max_threads(void) {
@@ -237,7 +238,7 @@ struct gdo_mc {
   gd_enepara ff;
   gd_complex_desc cx;
   gd_mc_params mc;
-  int offset, n_rep, cap, precision, n_exchange_calls;
+  int stream, n_rep, cap, precision, n_exchange_calls;
   gd_replica *replica;
   float *mm_old;
   gd_energy *e_old;
@@ -250,12 +251,12 @@ struct gdo_mc {
 };
 
 gdo_mc *gdo_mc_create(const gd_enepara *ff, const gd_complex_desc *cx, const gd_mc_params *mc,
-                      int replica_offset, int precision) {
+                      int stream, int precision) {
   gdo_mc *m = (gdo_mc *)calloc(1, sizeof(gdo_mc));
   m->ff = *ff;
   m->cx = *cx;
   m->mc = *mc;
-  m->offset = replica_offset;
+  m->stream = stream;
   m->precision = precision;
   m->n_rep = cx->n_prt * cx->n_tmp * cx->n_lig;
   m->cap = mc->steps_per_dump + 1;
@@ -355,7 +356,7 @@ static void run_one(gdo_mc *m, int r, int s1, int s2, int n_steps) {
   for (int s3 = 0; s3 < n_steps; ++s3) {
     const int step = s1 + s2 + s3;
     float delta[6], u, mm[6];
-    gd_draw_step(m->mc.seed, (uint32_t)(m->offset + r), (uint32_t)step, m->mc.move_kind,
+    gd_draw_step(m->mc.seed, (uint32_t)m->stream, (uint32_t)r, (uint32_t)step, m->mc.move_kind,
                  m->mc.move_scale, delta, &u);
     for (int i = 0; i < 6; ++i) mm[i] = GD_ADD(m->mm_old[r * 6 + i], delta[i]);
     gd_energy en;
@@ -382,8 +383,8 @@ void gdo_mc_run(gdo_mc *m, int s1, int s2, int n_steps, int nthreads) {
   gdo_mc_run_range(m, 0, m->n_rep, s1, s2, n_steps, nthreads);
 }
 
-void gdo_exchange_apply(const gd_complex_desc *cx, uint64_t seed, int exchange_call,
-                        int mode_t, gd_replica *replica, const float *etotal,
+void gdo_exchange_apply(const gd_complex_desc *cx, uint64_t seed, int stream,
+                        int exchange_call, int mode_t, gd_replica *replica, const float *etotal,
                         int32_t *acs) {
   const int nt = cx->n_tmp, nl = cx->n_lig;
   int temps[GD_MAXTMP], orders[GD_MAXTMP];
@@ -405,7 +406,8 @@ void gdo_exchange_apply(const gd_complex_desc *cx, uint64_t seed, int exchange_c
         const int tt = temps[o1];
         const float mb1 = cx->temp[temps[o1]].minus_beta;
         const float mb2 = cx->temp[temps[o2]].minus_beta;
-        const float u = gd_draw_exchange(seed, group, (uint32_t)exchange_call, (uint32_t)pair);
+        const float u = gd_draw_exchange(seed, (uint32_t)stream, group, (uint32_t)exchange_call,
+                                         (uint32_t)pair);
         if (gd_exchange_accept(en[o1], en[o2], mb1, mb2, u)) {
           temps[o1] = temps[o2];
           temps[o2] = tt;
@@ -420,8 +422,8 @@ void gdo_exchange_apply(const gd_complex_desc *cx, uint64_t seed, int exchange_c
 }
 
 void gdo_mc_exchange(gdo_mc *m, int mode_t) {
-  gdo_exchange_apply(&m->cx, m->mc.seed, m->n_exchange_calls, mode_t, m->replica, m->etotal,
-                     m->acs);
+  gdo_exchange_apply(&m->cx, m->mc.seed, m->stream, m->n_exchange_calls, mode_t, m->replica,
+                     m->etotal, m->acs);
   m->n_exchange_calls += 1;
 }
 

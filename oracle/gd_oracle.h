@@ -73,17 +73,19 @@ void gdo_philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0,
 float gdo_expf(float x);
 float gdo_logf(float x);
 void gdo_sincosf(float x, float *s, float *c);
-void gdo_draw_steps(uint64_t seed, int move_kind, const float scale[6], int n,
+void gdo_draw_steps(uint64_t seed, uint32_t stream, int move_kind, const float scale[6], int n,
                     const uint32_t *replica, const uint32_t *step, float *delta6, float *u);
 void gdo_metropolis_batch(int n, const float *e_new, const float *e_old, const float *mb,
                           const float *u, int32_t *out);
-float gdo_draw_exchange(uint64_t seed, uint32_t group, uint32_t call, uint32_t pair);
+float gdo_draw_exchange(uint64_t seed, uint32_t stream, uint32_t group, uint32_t call,
+                        uint32_t pair);
 
 /* ---- one complex's Monte Carlo chain set (MonteCarlo_Init_d / MonteCarlo_d /
  *      ExchangeReplicas_d restated) ---- */
 typedef struct gdo_mc gdo_mc;
+/* stream: the complex's RNG stream id (its index in a batch; 0 for a single complex). */
 gdo_mc *gdo_mc_create(const gd_enepara *ff, const gd_complex_desc *cx, const gd_mc_params *mc,
-                      int replica_offset, int precision);
+                      int stream, int precision);
 void gdo_mc_destroy(gdo_mc *m);
 int gdo_mc_num_replicas(const gdo_mc *m);
 void gdo_mc_init(gdo_mc *m);
@@ -102,8 +104,8 @@ const uint8_t *gdo_mc_refmap(const gdo_mc *m);
 int gdo_mc_exchange_calls(const gdo_mc *m);
 void gdo_mc_set_exchange_calls(gdo_mc *m, int n);
 /* Exchange restated over caller-owned arrays (for replaying device results). */
-void gdo_exchange_apply(const gd_complex_desc *cx, uint64_t seed, int exchange_call,
-                        int mode_t, gd_replica *replica, const float *etotal,
+void gdo_exchange_apply(const gd_complex_desc *cx, uint64_t seed, int stream,
+                        int exchange_call, int mode_t, gd_replica *replica, const float *etotal,
                         int32_t *acs_exchange);
 
 int gdo_max_threads(void);

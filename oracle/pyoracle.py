@@ -55,9 +55,9 @@ def lib():
         L.gdo_logf.argtypes = [C.c_float]
         L.gdo_logf.restype = C.c_float
         L.gdo_sincosf.argtypes = [C.c_float, fp, fp]
-        L.gdo_draw_steps.argtypes = [C.c_uint64, C.c_int, fp, C.c_int, u32p, u32p, fp, fp]
+        L.gdo_draw_steps.argtypes = [C.c_uint64, C.c_uint32, C.c_int, fp, C.c_int, u32p, u32p, fp, fp]
         L.gdo_metropolis_batch.argtypes = [C.c_int, fp, fp, fp, fp, ip]
-        L.gdo_draw_exchange.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32]
+        L.gdo_draw_exchange.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32]
         L.gdo_draw_exchange.restype = C.c_float
         L.gdo_mc_create.argtypes = [C.POINTER(abi.EnePara), C.POINTER(abi.ComplexDesc),
                                     C.POINTER(abi.McParams), C.c_int, C.c_int]
@@ -77,7 +77,7 @@ def lib():
         L.gdo_mc_exchange_calls.argtypes = [vp]
         L.gdo_mc_set_exchange_calls.argtypes = [vp, C.c_int]
         L.gdo_exchange_apply.argtypes = [C.POINTER(abi.ComplexDesc), C.c_uint64, C.c_int, C.c_int,
-                                         vp, fp, ip]
+                                         C.c_int, vp, fp, ip]
         _lib = L
     return _lib
 
@@ -172,7 +172,7 @@ def sincosf(x):
     return s.value, c.value
 
 
-def draw_steps(seed, move_kind, scale, replica, step):
+def draw_steps(seed, move_kind, scale, replica, step, stream=0):
     replica = np.ascontiguousarray(replica, np.uint32)
     step = np.ascontiguousarray(step, np.uint32)
     n = replica.size
@@ -180,7 +180,7 @@ def draw_steps(seed, move_kind, scale, replica, step):
     delta = np.zeros((n, 6), np.float32)
     u = np.zeros(n, np.float32)
     u32p = C.POINTER(C.c_uint32)
-    lib().gdo_draw_steps(seed, move_kind, abi.fptr(scale), n, replica.ctypes.data_as(u32p),
+    lib().gdo_draw_steps(seed, stream, move_kind, abi.fptr(scale), n, replica.ctypes.data_as(u32p),
                          step.ctypes.data_as(u32p), abi.fptr(delta), abi.fptr(u))
     return delta, u
 
@@ -193,29 +193,28 @@ def metropolis(e_new, e_old, mb, u):
     return out
 
 
-def draw_exchange(seed, group, call, pair):
-    return lib().gdo_draw_exchange(seed, group, call, pair)
+def draw_exchange(seed, group, call, pair, stream=0):
+    return lib().gdo_draw_exchange(seed, stream, group, call, pair)
 
 
-def exchange_apply(cx: abi.ComplexArrays, seed, call, mode_t, replica, etotal, acs=None):
+def exchange_apply(cx: abi.ComplexArrays, seed, call, mode_t, replica, etotal, acs=None, stream=0):
     """Restated ExchangeReplicas_d on caller arrays; replica (REPLICA_DTYPE) updated in place."""
     d = cx.desc()
     etotal = np.ascontiguousarray(etotal, np.float32)
-    lib().gdo_exchange_apply(C.byref(d), seed, call, mode_t, _ptr(replica), abi.fptr(etotal),
+    lib().gdo_exchange_apply(C.byref(d), seed, stream, call, mode_t, _ptr(replica), abi.fptr(etotal),
                              None if acs is None else abi.iptr(acs))
 
 
 class MC:
     """One complex's chain set: MonteCarlo_Init_d / MonteCarlo_d / ExchangeReplicas_d restated."""
 
-    def __init__(self, ff, cx: abi.ComplexArrays, params: abi.McParams, replica_offset=0,
-                 precision=32):
+    def __init__(self, ff, cx: abi.ComplexArrays, params: abi.McParams, stream=0, precision=32):
         self.cx = cx
         self._desc = cx.desc()
         self._ff = ff
         self._params = params
         self.h = lib().gdo_mc_create(C.byref(ff), C.byref(self._desc), C.byref(params),
-                                     replica_offset, precision)
+                                     stream, precision)
         self.n_rep = lib().gdo_mc_num_replicas(self.h)
         self.cap = params.steps_per_dump + 1
 

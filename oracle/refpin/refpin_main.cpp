@@ -359,7 +359,7 @@ int main(int argc, char **argv) {
         const int maxpair = nt / 2 - (nt % 2 == 0) * (mode_t == 1);
         for (int pair = 0; pair < maxpair; ++pair)
           g_shim_uniforms.push_back(
-              gd_draw_exchange(seed, (uint32_t)(pp * cs.n_lig + l), (uint32_t)e, (uint32_t)pair));
+              gd_draw_exchange(seed, 0u, (uint32_t)(pp * cs.n_lig + l), (uint32_t)e, (uint32_t)pair));
       }
     ExchangeReplicas_d(4, mode_t);
     for (int r = 0; r < n_rep; ++r) {

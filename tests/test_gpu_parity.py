@@ -1,0 +1,284 @@
+"""GPU parity: the CUDA path (through the C ABI) against the oracle.
+
+Tolerances: energies per term within 1e-5 relative to the FP64 oracle on the same FP32 placed
+coordinates, with the conditioning-aware scale of tests/tolerance.py; contact counts (cms)
+exact up to FP32 rounding of the MCC formula; accept / exchange decisions and replica
+permutations bit-exact given the same Philox stream.
+"""
+import numpy as np
+import pytest
+
+from geaxdock_gpu_b200 import abi, engine, system
+from oracle import pyoracle as po
+from tests.golden.fixtures import load_ref
+from tests.tolerance import rel_errors
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+
+
+@pytest.fixture(scope="module")
+def raw():
+    z, _, _ = load_ref("1a07C1")
+    return abi.enepara_raw_from_array(z["enepara_raw"])
+
+
+def _energy_check(eng, ff, cx, ci, ip, il, mm, refmap):
+    got = eng.eval_energy(ci, ip, il, mm)
+    worst = np.zeros(10)
+    for i in range(mm.shape[0]):
+        o = po.pose_energy(ff, cx, ip, il, mm[i], refmap, 64)
+        worst = np.maximum(worst, rel_errors(got["e"][i], o, ff))
+        assert abs(got["cms"][i] - o["cms"]) <= 2e-6, (i, got["cms"][i], o["cms"])
+        assert abs(got["rmsd"][i] - o["rmsd"]) <= 1e-5 * max(1.0, o["rmsd"])
+    return worst
+
+
+@pytest.mark.parametrize("name", ["1a07C1", "1robA1"])
+def test_eval_energy_reference_complexes(name):
+    z, cx, ff = load_ref(name)
+    rm = z["ref_matrix"].astype(np.uint8)
+    with engine.Engine(ff, [cx], abi.mc_params()) as eng:
+        for ip in range(min(cx.n_prt, 3)):
+            sel = np.nonzero(z["pose_idx"][:, 0] == ip)[0]
+            for il in np.unique(z["pose_idx"][sel, 1])[:4]:
+                mm = z["pose_mm"][sel[z["pose_idx"][sel, 1] == il]]
+                worst = _energy_check(eng, ff, cx, 0, ip, int(il), mm, rm)
+                assert worst.max() <= TOL, (ip, il, worst)
+
+
+@pytest.mark.parametrize("cfg", [0, 1])
+def test_eval_energy_synthetic(raw, cfg):
+    w = system.config(cfg, raw)
+    cx, ff = w.complexes[0], w.ff
+    rm = po.ref_map(ff, cx)
+    rng = np.random.default_rng(5)
+    mm = np.concatenate([rng.normal(0, 1.5, (24, 3)), rng.uniform(-3.2, 3.2, (24, 3))], 1)
+    with engine.Engine(ff, [cx], w.params) as eng:
+        for ip in range(min(cx.n_prt, 2)):
+            worst = _energy_check(eng, ff, cx, 0, ip, 1, mm.astype(np.float32), rm)
+            assert worst.max() <= TOL, worst
+
+
+@pytest.mark.parametrize("chunk", [64, 512, 4096])
+def test_chunk_pipeline_gives_same_energies(raw, chunk):
+    """Streaming (chunks < points) and resident protein tiles agree term by term."""
+    w = system.config(1, raw)
+    cx, ff = w.complexes[0], w.ff
+    rm = po.ref_map(ff, cx)
+    mm = np.random.default_rng(9).normal(0, 0.5, (16, 6)).astype(np.float32)
+    with engine.Engine(ff, [cx], w.params) as eng:
+        k, _ = eng.tile()
+        eng.set_tile(k, chunk)
+        worst = _energy_check(eng, ff, cx, 0, 3, 2, mm, rm)
+        assert worst.max() <= TOL
+
+
+def _init_and_compare(eng, ff, cx, w_params):
+    eng.mc_init()
+    eng.sync()
+    st = eng.state()
+    rm = po.ref_map(ff, cx)
+    for r in range(0, cx.n_rep, max(1, cx.n_rep // 16)):
+        p = r // (cx.n_tmp * cx.n_lig)
+        l = r % cx.n_lig
+        o = po.pose_energy(ff, cx, p, l, np.zeros(6, np.float32), rm, 64)
+        assert rel_errors(st["energy_old"]["e"][r], o, ff).max() <= TOL
+    steps, nxt = eng.records()
+    assert np.all(nxt == 1)
+    assert np.all(steps[:, 0]["step"] == 0)
+    return st
+
+
+def _replay(eng, cx, params, n_dumps_steps, trace_e, trace_acc, st0, exch_log):
+    """Bit-exact replay of Metropolis decisions and exchanges from the device's own energies."""
+    n_rep = cx.n_rep
+    spe = params.steps_per_exchange
+    e_old = st0["energy_old"]["e"][:, 9].copy()
+    mm = st0["movematrix_old"].copy()
+    idx_tmp = st0["replica"]["idx_tmp"].copy()
+    mb_tab = cx.temp["minus_beta"]
+    reps = np.arange(n_rep, dtype=np.uint32)
+    for s in range(n_dumps_steps):
+        delta, u = po.draw_steps(params.seed, params.move_kind, np.array(params.move_scale[:]),
+                                 reps, np.full(n_rep, s, np.uint32))
+        mmn = (mm + delta).astype(np.float32)
+        acc = po.metropolis(trace_e[:, s], e_old, mb_tab[idx_tmp], u)
+        assert np.array_equal(acc, trace_acc[:, s]), ("step", s, np.nonzero(acc != trace_acc[:, s]))
+        m = acc.astype(bool)
+        mm[m] = mmn[m]
+        e_old[m] = trace_e[m, s]
+        if (s + 1) % spe == 0:
+            e = (s + 1) // spe - 1
+            before, etot, after = exch_log[e]
+            assert np.array_equal(before, idx_tmp)
+            assert np.array_equal(etot, e_old)
+            rep = np.zeros(n_rep, abi.REPLICA_DTYPE)
+            rep["idx_tmp"] = idx_tmp
+            po.exchange_apply(cx, params.seed, e, int(not (e % 2)), rep, e_old)
+            assert np.array_equal(rep["idx_tmp"], after)
+            idx_tmp = after
+    return mm, e_old
+
+
+@pytest.mark.parametrize("move_kind", [abi.MOVE_UNIFORM, abi.MOVE_GAUSSIAN])
+def test_trajectory_replay_bit_exact(raw, move_kind):
+    z, cx, ff = load_ref("1a07C1")
+    params = abi.mc_params(steps_per_exchange=10, steps_per_dump=200, move_kind=move_kind,
+                           move_scale=(0.2, 0.2, 0.2, 0.1, 0.1, 0.1), seed=1234)
+    n_steps = 60
+    with engine.Engine(ff, [cx], params) as eng:
+        st0 = _init_and_compare(eng, ff, cx, params)
+        eng.trace_enable(n_steps)
+        log = []
+        for e in range(n_steps // 10):
+            eng.mc_run(0, e * 10)
+            before = eng.replicas()["idx_tmp"].copy()
+            et = eng.etotal()
+            eng.exchange(int(not (e % 2)))
+            log.append((before, et, eng.replicas()["idx_tmp"].copy()))
+        eng.sync()
+        te, ta = eng.trace()
+        mm, e_old = _replay(eng, cx, params, n_steps, te, ta, st0, log)
+        st = eng.state()
+        assert np.array_equal(st["movematrix_old"].view(np.uint32), mm.view(np.uint32))
+        assert np.array_equal(st["energy_old"]["e"][:, 9], e_old)
+        assert np.array_equal(st["n_accept"], ta.sum(axis=1))
+        # records: one per accepted step after the step-0 record, with their step numbers
+        steps, nxt = eng.records()
+        assert np.array_equal(nxt, 1 + ta.sum(axis=1))
+        for r in range(0, cx.n_rep, 17):
+            want = np.nonzero(ta[r])[0]
+            assert np.array_equal(steps[r, 1:nxt[r]]["step"], want)
+        # acceptance must be neither 0 nor 1 for the replay to mean something
+        assert 0.05 < ta.mean() < 0.98
+
+
+def test_fused_graph_equals_stepwise(raw):
+    w = system.config(0, raw)
+    cx, ff = w.complexes[0], w.ff
+    params = w.params
+    params.steps_per_dump = 100
+    with engine.Engine(ff, [cx], params) as a, engine.Engine(ff, [cx], params) as b:
+        a.mc_init()
+        b.mc_init()
+        for e in range(6):
+            a.mc_run(0, e * 10)
+            a.exchange(int(not (e % 2)))
+        b.run_fused(0, 60, exchange=True)
+        a.sync()
+        b.sync()
+        sa, sb = a.state(), b.state()
+        assert np.array_equal(sa.view(np.uint8), sb.view(np.uint8))
+        ra, na = a.records()
+        rb, nb = b.records()
+        assert np.array_equal(na, nb)
+        # a second replay of the cached graph continues the same chain
+        for e in range(6, 12):
+            a.mc_run(0, e * 10)
+            a.exchange(int(not (e % 2)))
+        b.run_fused(60, 60, exchange=True)
+        a.sync()
+        b.sync()
+        assert np.array_equal(a.state().view(np.uint8), b.state().view(np.uint8))
+
+
+def test_batch_equals_alone(raw):
+    """Config-2 style batch (uneven ligands and pockets): each complex's trajectory in the
+    batch is bit-identical to running it alone with the same stream id and tile."""
+    w = system.config(2, raw, n_ligands=6)
+    params = w.params
+    params.steps_per_dump = 40
+    with engine.Engine(w.ff, w.complexes, params) as eng:
+        eng.set_tile(4, 256)
+        eng.mc_init()
+        eng.run_fused(0, 20, exchange=True)
+        eng.sync()
+        st = eng.state()
+        for k in (0, 3, 5):
+            cx = w.complexes[k]
+            off = eng.offsets[k]
+            with engine.Engine(w.ff, [cx], params) as one:
+                one.set_rng_stream(0, k)
+                one.set_tile(4, 256)
+                one.mc_init()
+                one.run_fused(0, 20, exchange=True)
+                one.sync()
+                s1 = one.state()
+                mine = st[off:off + cx.n_rep].copy()
+                mine["replica"]["idx_rep"] -= 0
+                assert np.array_equal(s1["movematrix_old"], mine["movematrix_old"])
+                assert np.array_equal(s1["energy_old"].view(np.uint8), mine["energy_old"].view(np.uint8))
+                assert np.array_equal(s1["replica"]["idx_tmp"], mine["replica"]["idx_tmp"])
+
+
+def test_cpu_baseline_statistics_match(raw):
+    """Same Philox stream on the FP32 OpenMP CPU restatement: per-temperature energy samples
+    are indistinguishable (two-sample KS p > 0.01) and most decisions coincide."""
+    from scipy import stats
+    w = system.config(0, raw)
+    cx, ff, params = w.complexes[0], w.ff, w.params
+    params.record = 0
+    n_ex = 20
+    cpu = po.MC(ff, cx, params, stream=0, precision=32)
+    cpu.init()
+    with engine.Engine(ff, [cx], params) as eng:
+        eng.mc_init()
+        g_e, c_e, g_t, c_t = [], [], [], []
+        for e in range(n_ex):
+            eng.mc_run(0, e * 10)
+            cpu.run(0, e * 10, 10)
+            if e >= 5:
+                gs, cs_ = eng.state(), cpu.get()
+                g_e.append(gs["energy_old"]["e"][:, 9].copy())
+                c_e.append(cs_["e_old"]["e"][:, 9].copy())
+                g_t.append(gs["replica"]["idx_tmp"].copy())
+                c_t.append(cs_["replica"]["idx_tmp"].copy())
+            eng.exchange(int(not (e % 2)))
+            cpu.exchange(int(not (e % 2)))
+        eng.sync()
+        ge, ce = np.array(g_e), np.array(c_e)
+        gt, ct = np.array(g_t), np.array(c_t)
+        for t in range(cx.n_tmp):
+            a, b = ge[gt == t], ce[ct == t]
+            assert stats.ks_2samp(a, b).pvalue > 0.01, t
+        st, cs_ = eng.state(), cpu.get()
+        same = np.mean(st["n_accept"] == cs_["n_accept"])
+        assert same > 0.9, same
+
+
+def test_record_overflow_is_reported(raw):
+    z, cx, ff = load_ref("1a07C1")
+    params = abi.mc_params(steps_per_exchange=10, steps_per_dump=3, move_scale=(0, 0, 0, 0, 0, 0))
+    with engine.Engine(ff, [cx], params) as eng:
+        eng.mc_init()
+        eng.mc_run(0, 0)  # zero moves are always accepted: 10 records > capacity 4
+        with pytest.raises(engine.GDError) as e:
+            eng.sync()
+        assert e.value.code == abi.GD_ERR_RECORD_FULL
+        steps, nxt = eng.records()
+        assert np.all(nxt == 4)
+
+
+def test_bounded_wait_times_out_without_fault(raw):
+    """A wait that runs out ends the kernel with GD_ERR_TIMEOUT; the context stays usable."""
+    w = system.config(1, raw)
+    cx, ff = w.complexes[0], w.ff
+    params = w.params
+    params.record = 0
+    with engine.Engine(ff, [cx], params) as eng:
+        k, _ = eng.tile()
+        eng.set_tile(k, 64)  # streaming tiles: many waits
+        eng.mc_init()
+        eng.sync()
+        eng.set_wait_timeout(0)
+        eng.mc_run(0, 0)
+        with pytest.raises(engine.GDError) as e:
+            eng.sync()
+        assert e.value.code == abi.GD_ERR_TIMEOUT
+        eng.set_wait_timeout(2_000_000_000)
+        eng.mc_init()
+        eng.mc_run(0, 0)
+        eng.sync()
+        assert np.all(np.isfinite(eng.etotal()))
