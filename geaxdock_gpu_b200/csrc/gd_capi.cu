@@ -247,7 +247,7 @@ void build_tiles(const gd_ctx *c, int r0, int r1, std::vector<GdTileDesc> &out) 
 size_t smem_bytes(const gd_ctx *c) {
   int kmax = 1;
   for (const auto &x : c->info) kmax = std::max(kmax, x.k);
-  const size_t slot = 128; /* sizeof(gd::Slot) */
+  const size_t slot = GD_SLOT_BYTES;
   return 16 + (size_t)2 * c->chunk * 24 + (size_t)c->threads * 16 + (size_t)10 * c->threads * 8 +
          (size_t)kmax * slot;
 }
@@ -297,11 +297,19 @@ GdMcArgs base_args(gd_ctx *c) {
   return a;
 }
 
+int set_kernel_attrs(size_t smem) {
+  CK(cudaFuncSetAttribute(gd::gd_mc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)smem));
+  CK(cudaFuncSetAttribute(gd::gd_mc_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                          cudaSharedmemCarveoutMaxShared));
+  return GD_OK;
+}
+
 int launch_mc(gd_ctx *c, GdMcArgs a, const GdTileDesc *d_tiles, int n_tiles, int *counter) {
   if (n_tiles <= 0) return GD_OK;
   const size_t smem = smem_bytes(c);
-  CK(cudaFuncSetAttribute(gd::gd_mc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)smem));
+  int rc = set_kernel_attrs(smem);
+  if (rc) return rc;
   a.tiles = d_tiles;
   a.n_tiles = n_tiles;
   a.tile_counter = counter;
@@ -524,8 +532,10 @@ int gd_create(const gd_enepara *ff, const gd_complex_desc *cxs, int n_complexes,
         q.pmf0 = ff->pmf0[i][j];
         q.pmf1 = ff->pmf1[i][j];
         const bool live = ff->hdb0[i][j] > 0.1f;
-        q.hc1 = (float)((double)ff->hdb1[i][j] * hsc);
-        q.hc0 = (float)(-(double)ff->hdb0[i][j] * (double)ff->hdb1[i][j] * hsc);
+        /* pairs without an H-bond entry have hdb1 = 1/0: keep their folded argument finite,
+         * since they run inside warps where another lane's pair is live (hs = 0 kills them) */
+        q.hc1 = live ? (float)((double)ff->hdb1[i][j] * hsc) : 0.0f;
+        q.hc0 = live ? (float)(-(double)ff->hdb0[i][j] * (double)ff->hdb1[i][j] * hsc) : 0.0f;
         q.hs = live ? sqrt_2_pi_m1 * ff->hdb1[i][j] : 0.0f;
         q.hneed = live ? 1.0f : 0.0f;
       }
@@ -566,7 +576,7 @@ int gd_create(const gd_enepara *ff, const gd_complex_desc *cxs, int n_complexes,
     g.pocket[0] = d.pocket_center[0];
     g.pocket[1] = d.pocket_center[1];
     g.pocket[2] = d.pocket_center[2];
-    const int L = d.lna, P = d.pnp, PP = x.pnp_pad;
+    const int L = d.lna, P = d.pnp;
 
     std::vector<float4> lig_pos((size_t)d.n_lig * L);
     std::vector<int2> lig_meta((size_t)d.n_lig * L);
@@ -576,39 +586,65 @@ int gd_create(const gd_enepara *ff, const gd_complex_desc *cxs, int n_complexes,
     }
     std::vector<float> lig_center(d.lig_center, d.lig_center + 3 * d.n_lig);
 
-    /* protein: sort by (type, kind), segments, reference contacts */
-    std::vector<float4> pt_pos((size_t)d.n_prt * PP, make_float4(1e6f, 1e6f, 1e6f, 0.0f));
-    std::vector<float2> pt_aux((size_t)d.n_prt * PP, make_float2(0.0f, bits_as_float(-1)));
+    /* protein: sort by (type, kind) into segments that start on even slots (one padding
+     * slot after an odd-length segment), then write slot pairs */
     std::vector<int4> seg((size_t)d.n_prt * GD_MAX_SEG, make_int4(0, 0, 0, 0));
     std::vector<int> seg_count(d.n_prt, 0);
+    std::vector<std::vector<int>> slot_point(d.n_prt); /* point index per slot, -1: padding */
+    int max_slots = 4;
     for (int pc = 0; pc < d.n_prt; ++pc) {
       const int o = pc * P;
-      std::vector<int> order(P);
-      std::vector<int> key(P);
+      std::vector<int> order(P), key(P);
       for (int p = 0; p < P; ++p) {
         const int kind = (d.prt_hflag[o + p] == 1 ? 1 : 0) | (d.prt_c[o + p] == 2 ? 2 : 0);
         key[p] = d.prt_t[o + p] * 4 + kind;
         order[p] = p;
       }
       std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key[a] < key[b]; });
+      std::vector<int> &sp = slot_point[pc];
       int ns = 0;
       for (int i = 0; i < P; ++i) {
         const int p = order[i];
-        const int kind = key[p] & 3;
-        pt_pos[(size_t)pc * PP + i] =
-            make_float4(d.prt_x[o + p], d.prt_y[o + p], d.prt_z[o + p], d.prt_ele[o + p]);
-        pt_aux[(size_t)pc * PP + i] =
-            make_float2((kind & 1) ? d.prt_hpp[o + p] : 0.0f,
-                        bits_as_float((kind & 2) ? d.prt_seq3r[o + p] : -1));
         if (i == 0 || key[p] != key[order[i - 1]]) {
+          if (sp.size() & 1) sp.push_back(-1);
           if (ns == GD_MAX_SEG) return bail(fail(GD_ERR_CAPACITY, "too many point segments"));
-          seg[(size_t)pc * GD_MAX_SEG + ns] = make_int4(i, i + 1, d.prt_t[o + p], kind);
+          const int s0 = (int)sp.size();
+          seg[(size_t)pc * GD_MAX_SEG + ns] = make_int4(s0, s0 + 1, d.prt_t[o + p], key[p] & 3);
           ++ns;
         } else {
-          seg[(size_t)pc * GD_MAX_SEG + ns - 1].y = i + 1;
+          seg[(size_t)pc * GD_MAX_SEG + ns - 1].y = (int)sp.size() + 1;
         }
+        sp.push_back(p);
       }
       seg_count[pc] = ns;
+      max_slots = std::max(max_slots, (int)sp.size());
+    }
+    const int PP = (max_slots + 3) & ~3;
+    c->info[ci].pnp_pad = PP;
+    g.pnp_pad = PP;
+    const size_t npair = (size_t)PP / 2;
+    std::vector<float4> pt_a((size_t)d.n_prt * npair, make_float4(-1e6f, -1e6f, -1e6f, -1e6f));
+    std::vector<float4> pt_b((size_t)d.n_prt * npair, make_float4(-1e6f, -1e6f, 0.0f, 0.0f));
+    std::vector<float4> pt_x((size_t)d.n_prt * npair,
+                             make_float4(0.0f, 0.0f, bits_as_float(-1), bits_as_float(-1)));
+    for (int pc = 0; pc < d.n_prt; ++pc) {
+      const int o = pc * P;
+      const std::vector<int> &sp = slot_point[pc];
+      for (size_t sidx = 0; sidx < sp.size(); ++sidx) {
+        const int p = sp[sidx];
+        if (p < 0) continue;
+        const int kind = (d.prt_hflag[o + p] == 1 ? 1 : 0) | (d.prt_c[o + p] == 2 ? 2 : 0);
+        float *A = &pt_a[pc * npair + sidx / 2].x;
+        float *B = &pt_b[pc * npair + sidx / 2].x;
+        float *X = &pt_x[pc * npair + sidx / 2].x;
+        const int h = (int)(sidx & 1);
+        A[0 + h] = -d.prt_x[o + p];
+        A[2 + h] = -d.prt_y[o + p];
+        B[0 + h] = -d.prt_z[o + p];
+        B[2 + h] = d.prt_ele[o + p];
+        X[0 + h] = (kind & 1) ? d.prt_hpp[o + p] : 0.0f;
+        X[2 + h] = bits_as_float((kind & 2) ? d.prt_seq3r[o + p] : -1);
+      }
     }
     /* contact reference from (protein 0, ligand 0) at movematrix 0 (InitRefMatrix_d) */
     std::vector<int> ref_start((size_t)d.n_prt * (L + 1));
@@ -655,12 +691,13 @@ int gd_create(const gd_enepara *ff, const gd_complex_desc *cxs, int n_complexes,
     std::vector<float> mb(d.n_tmp);
     for (int t = 0; t < d.n_tmp; ++t) mb[t] = d.temp[t].minus_beta;
 
-    float4 *p_lig_pos; int2 *p_lig_meta; float *p_lig_center; float4 *p_pt_pos; float2 *p_pt_aux;
+    float4 *p_lig_pos; int2 *p_lig_meta; float *p_lig_center; float4 *p_pt_a, *p_pt_b, *p_pt_x;
     int4 *p_seg; int *p_seg_count; float4 *p_kde; float *p_mx, *p_my, *p_mz, *p_mt, *p_psp, *p_mb;
     int *p_ref_start; float4 *p_ref_pts;
     if ((rc = upload(c, &p_lig_pos, lig_pos)) || (rc = upload(c, &p_lig_meta, lig_meta)) ||
-        (rc = upload(c, &p_lig_center, lig_center)) || (rc = upload(c, &p_pt_pos, pt_pos)) ||
-        (rc = upload(c, &p_pt_aux, pt_aux)) || (rc = upload(c, &p_seg, seg)) ||
+        (rc = upload(c, &p_lig_center, lig_center)) || (rc = upload(c, &p_pt_a, pt_a)) ||
+        (rc = upload(c, &p_pt_b, pt_b)) || (rc = upload(c, &p_pt_x, pt_x)) ||
+        (rc = upload(c, &p_seg, seg)) ||
         (rc = upload(c, &p_seg_count, seg_count)) || (rc = upload(c, &p_kde, kde)) ||
         (rc = upload(c, &p_mx, mx)) || (rc = upload(c, &p_my, my)) ||
         (rc = upload(c, &p_mz, mz)) || (rc = upload(c, &p_mt, mt)) ||
@@ -671,7 +708,7 @@ int gd_create(const gd_enepara *ff, const gd_complex_desc *cxs, int n_complexes,
     if (cudaStreamSynchronize(c->stream) != cudaSuccess)
       return bail(fail(GD_ERR_CUDA, "upload failed: %s", cudaGetErrorString(cudaGetLastError())));
     g.lig_pos = p_lig_pos; g.lig_meta = p_lig_meta; g.lig_center = p_lig_center;
-    g.pt_pos = p_pt_pos; g.pt_aux = p_pt_aux; g.seg = p_seg; g.seg_count = p_seg_count;
+    g.pt_a = p_pt_a; g.pt_b = p_pt_b; g.pt_x = p_pt_x; g.seg = p_seg; g.seg_count = p_seg_count;
     g.kde = p_kde; g.mcs_x = p_mx; g.mcs_y = p_my; g.mcs_z = p_mz; g.mcs_tcc = p_mt;
     g.psp = p_psp; g.minus_beta = p_mb; g.ref_start = p_ref_start; g.ref_pts = p_ref_pts;
   }
@@ -868,8 +905,7 @@ int gd_mc_run_fused(gd_ctx *c, int s1, int n_steps, int exchange) {
     if ((rc = upload_tiles(c, 0, c->n_rep - 1, &n))) return rc;
     CK(cudaStreamSynchronize(c->stream));
     const size_t smem = smem_bytes(c);
-    CK(cudaFuncSetAttribute(gd::gd_mc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)smem));
+    if ((rc = set_kernel_attrs(smem))) return rc;
     const int grid = grid_for(c, n, smem);
     cudaGraph_t graph;
     CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));

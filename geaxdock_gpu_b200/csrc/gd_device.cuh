@@ -4,10 +4,12 @@
  * HBM layout (one context, all complexes of a batch):
  *   ligand conformers   float4 (x, y, z, charge) + int2 (type, MCS field) per atom,
  *                       conformer-major; placed coordinates never touch HBM.
- *   protein conformers  points sorted by (point type, kind) per conformer and padded to a
- *                       multiple of 4: float4 (x, y, z, ele) + float2 (hydrophobic hpp or 0,
- *                       PSP column or -1) per point; a segment table (start, end, type, kind)
- *                       per conformer. kind 0: plain, 1: hydrophobic, 2: hydrophobic + PSP.
+ *   protein conformers  points sorted by (point type, kind) per conformer, every segment
+ *                       starting on an even slot, stored as pairs of slots in three float4
+ *                       streams (negated coordinates and ele; hydrophobic hpp or 0 and PSP
+ *                       column) so one 16-byte shared load gives the two-lane register pairs
+ *                       of the FP32x2 pair loop; a segment table (start, end, type, kind) per
+ *                       conformer. kind bit 0: hydrophobic point, bit 1: class-2 (PSP) point.
  *   pair parameters     per (ligand type, protein type) 12 floats, folded for the kernel.
  *   contact reference   per conformer and ligand atom, the list of reference contacts as
  *                       float4 (x, y, z, contact threshold): tp is counted over this sparse
@@ -25,7 +27,8 @@
 #include "../../include/geauxdock_b200.h"
 
 #define GD_MAX_SEG 96          /* (30 point types) x (3 kinds), rounded up */
-#define GD_MAX_TPB 512
+#define GD_MAX_TPB 256         /* threads per CTA: 3 CTAs of 256 fit the register file */
+#define GD_SLOT_BYTES 192      /* shared-memory bytes per replica slot (sizeof gd::Slot) */
 #define GD_MAX_SLOTS 128       /* replicas per CTA */
 #define GD_NQ 12               /* per-lane partial sums handed to the reducer */
 
@@ -49,8 +52,12 @@ struct GdDevComplex {
   const float4 *lig_pos;      /* [n_lig*lna] */
   const int2 *lig_meta;       /* [n_lig*lna] type, MCS index (n + 1) */
   const float *lig_center;    /* [n_lig*3] */
-  const float4 *pt_pos;       /* [n_prt*pnp_pad] */
-  const float2 *pt_aux;       /* [n_prt*pnp_pad] */
+  /* protein points in pairs (slots 2m, 2m+1), [n_prt*pnp_pad/2] each:
+   *   pt_a = (-x0, -x1, -y0, -y1), pt_b = (-z0, -z1, ele0, ele1),
+   *   pt_x = (hpp0 or 0, hpp1 or 0, psp column0 bits, psp column1 bits) */
+  const float4 *pt_a;
+  const float4 *pt_b;
+  const float4 *pt_x;
   const int4 *seg;            /* [n_prt*GD_MAX_SEG] */
   const int *seg_count;       /* [n_prt] */
   const float4 *kde;          /* [pnk] x, y, z, type (exact small integer as float) */

@@ -102,73 +102,128 @@ __device__ __forceinline__ float dist2(float ax, float ay, float az, float px, f
 #define LOG2E_F 1.4426950408889634f
 
 struct Acc {
-  float vdw, ele, pmf, psp, hdb, hsum;
+  float2 vdw, ele, pmf, hdb, hsum;
+  float psp;
   int ncon;
 };
 
-/* Pair loop over points [i0, i1) of one (type, kind) segment held in shared memory.
- * KIND bit 0: hydrophobic point (hpc), bit 1: class-2 point (psp). HDB: some lane of the
- * warp has a live hydrogen-bond pair for this segment's type. */
-template <int KIND, bool HDB>
-__device__ __forceinline__ void pair_range(const float4 *__restrict__ P,
-                                           const float2 *__restrict__ X, int i0, int i1,
-                                           float ax, float ay, float az, const GdPairParam &q,
-                                           const float *__restrict__ psprow,
-                                           const GdForceConst &f, Acc &a) {
-  const float lj1 = f.lj1, el0 = f.el0, el1 = f.el1, a1 = f.a1, b1 = f.b1, iel1 = f.inv_el1;
-  const float cA = -0.5f * LOG2E_F, cB = 6.0f * LOG2E_F;
-#pragma unroll 2
-  for (int i = i0; i < i1; ++i) {
-    const float4 p = P[i];
-    const float d2 = dist2(ax, ay, az, p.x, p.y, p.z);
-    const float ri = rsqrt_a(d2);
-    const float r = d2 * ri;
-    /* vdw: (p1 - p2) / (p1 lj0 (1 + lj1 d2) + 1), p1 = p1a r^-9, p2 = p2a r^-6 */
-    const float r2i = ri * ri;
-    const float r3i = r2i * ri;
-    const float r6i = r3i * r3i;
-    const float num = r6i * __fmaf_rn(q.p1a, r3i, -q.p2a);
-    const float p4 = __fmaf_rn(q.p1l * (r6i * r3i), __fmaf_rn(lj1, d2, 1.0f), 1.0f);
-    a.vdw = __fmaf_rn(num, rcp_a(p4), a.vdw);
-    /* ele: q_l ele_p g(el1 r); q_l applied once per atom */
-    const float s1 = el1 * r;
-    const float gn = __fmaf_rn(s1 * s1, __fmaf_rn(b1, s1, a1), el0);
-    const float gf = ri * iel1;
-    a.ele = __fmaf_rn(p.w, (s1 < 1.0f) ? gn : gf, a.ele);
-    /* pmf: pmf1 / (1 + exp((6 - r/2)(r - pmf0))) */
-    const float ex = ex2_a(__fmaf_rn(cA, r, cB) * (r - q.pmf0));
-    a.pmf = __fmaf_rn(q.pmf1, rcp_a(1.0f + ex), a.pmf);
-    /* contact (mcc, psp): sqrtf(d2) <= pmf0  <=>  d2 <= thr */
-    const bool contact = d2 <= q.thr;
-    a.ncon += contact ? 1 : 0;
-    if (KIND & 2) {
-      const float2 x = X[i];
-      if (contact) a.psp += __ldg(psprow + __float_as_int(x.y));
-    }
-    if (HDB) {
-      const float h = __fmaf_rn(r, q.hc1, q.hc0);
-      a.hdb = __fmaf_rn(q.hs, ex2_a(-(h * h)), a.hdb);
-    }
-    if (KIND & 1) {
-      const float hp = X[i].x;
-      float t = __fmaf_rn(d2, HPC_C4, -HPC_C3);
-      t = __fmaf_rn(d2, t, HPC_C2);
-      t = __fmaf_rn(d2, t, -HPC_C1);
-      const float pl = __fmaf_rn(d2, t, 1.0f);
-      if (d2 <= 81.0f) a.hsum = __fmaf_rn(hp, pl, a.hsum);
-    }
+/* Per-segment pair parameters, splatted over the two lanes of an FP32x2 register pair. */
+struct Pair2 {
+  float2 p1a, mp2a, p1l, mpmf0, pmf1, hc1, hc0, hs;
+  float thr;
+};
+
+__device__ __forceinline__ float2 f2(float v) { return make_float2(v, v); }
+
+/* One pair of protein slots (2m, 2m+1) against the lane's atom. PAIR = false: only the
+ * first slot is a point (the second is segment padding) and nothing of the second is kept. */
+template <int KIND, bool HDB, bool PAIR>
+__device__ __forceinline__ void pair_body(const float4 A, const float4 B,
+                                          const float4 *__restrict__ PX, int m, float2 ax,
+                                          float2 ay, float2 az, const Pair2 &q,
+                                          const float *__restrict__ psprow, const GdForceConst &f,
+                                          Acc &a) {
+  const float2 one = f2(1.0f);
+  /* squared distance, per lane exactly dist2(): a + (-p) == a - p */
+  const float2 dx = __fadd2_rn(ax, make_float2(A.x, A.y));
+  const float2 dy = __fadd2_rn(ay, make_float2(A.z, A.w));
+  const float2 dz = __fadd2_rn(az, make_float2(B.x, B.y));
+  const float2 d2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+  const float2 ri = make_float2(rsqrt_a(d2.x), rsqrt_a(d2.y));
+  const float2 r = __fmul2_rn(d2, ri);
+  /* vdw: (p1 - p2) / (p1 lj0 (1 + lj1 d2) + 1), p1 = p1a r^-9, p2 = p2a r^-6 */
+  const float2 r2i = __fmul2_rn(ri, ri);
+  const float2 r3i = __fmul2_rn(r2i, ri);
+  const float2 r6i = __fmul2_rn(r3i, r3i);
+  const float2 num = __fmul2_rn(r6i, __ffma2_rn(q.p1a, r3i, q.mp2a));
+  const float2 t9 = __fmul2_rn(q.p1l, __fmul2_rn(r6i, r3i));
+  const float2 p4 = __ffma2_rn(t9, __ffma2_rn(f2(f.lj1), d2, one), one);
+  /* ele: q_l ele_p g(el1 r); q_l applied once per atom */
+  const float2 s1 = __fmul2_rn(f2(f.el1), r);
+  const float2 gn = __ffma2_rn(__fmul2_rn(s1, s1), __ffma2_rn(f2(f.b1), s1, f2(f.a1)), f2(f.el0));
+  const float2 gf = __fmul2_rn(ri, f2(f.inv_el1));
+  const float2 g = make_float2(s1.x < 1.0f ? gn.x : gf.x, s1.y < 1.0f ? gn.y : gf.y);
+  const float2 ep = make_float2(B.z, B.w);
+  /* pmf: pmf1 / (1 + exp((6 - r/2)(r - pmf0))), exp as exp2 with log2(e) folded */
+  const float2 tt = __fmul2_rn(__ffma2_rn(f2(-0.5f * LOG2E_F), r, f2(6.0f * LOG2E_F)),
+                               __fadd2_rn(r, q.mpmf0));
+  /* den <= 1 + 2^100 keeps p4 * den finite wherever p4 itself is (p4 is large only at
+   * r << 1 A, where tt < 0); the dropped tail of pmf1 / den is below 1e-30 */
+  const float2 den = __fadd2_rn(one, make_float2(ex2_a(fminf(tt.x, 100.0f)),
+                                                 ex2_a(fminf(tt.y, 100.0f))));
+  /* one reciprocal for both quotients: num / p4 = num den / (p4 den),
+   * pmf1 / den = pmf1 p4 / (p4 den) */
+  const float2 pd = __fmul2_rn(p4, den);
+  const float2 inv = make_float2(rcp_a(pd.x), rcp_a(pd.y));
+  const float2 vn = __fmul2_rn(num, den);
+  const float2 pn = __fmul2_rn(q.pmf1, p4);
+  if constexpr (PAIR) {
+    a.vdw = __ffma2_rn(vn, inv, a.vdw);
+    a.ele = __ffma2_rn(ep, g, a.ele);
+    a.pmf = __ffma2_rn(pn, inv, a.pmf);
+  } else {
+    a.vdw.x = __fmaf_rn(vn.x, inv.x, a.vdw.x);
+    a.ele.x = __fmaf_rn(ep.x, g.x, a.ele.x);
+    a.pmf.x = __fmaf_rn(pn.x, inv.x, a.pmf.x);
+  }
+  /* contacts (mcc, psp): sqrtf(d2) <= pmf0  <=>  d2 <= thr */
+  const bool c0 = d2.x <= q.thr, c1 = PAIR && d2.y <= q.thr;
+  a.ncon += (int)c0 + (int)c1;
+  if (KIND & 2) {
+    const float4 X = PX[m];
+    if (c0) a.psp += __ldg(psprow + __float_as_int(X.z));
+    if (c1) a.psp += __ldg(psprow + __float_as_int(X.w));
+  }
+  if (HDB) {
+    const float2 h = __ffma2_rn(r, q.hc1, q.hc0);
+    const float2 hh = __fmul2_rn(h, h);
+    if constexpr (PAIR)
+      a.hdb = __ffma2_rn(q.hs, make_float2(ex2_a(-hh.x), ex2_a(-hh.y)), a.hdb);
+    else
+      a.hdb.x = __fmaf_rn(q.hs.x, ex2_a(-hh.x), a.hdb.x);
+  }
+  if (KIND & 1) {
+    const float4 X = PX[m];
+    float2 t = __ffma2_rn(d2, f2(HPC_C4), f2(-HPC_C3));
+    t = __ffma2_rn(d2, t, f2(HPC_C2));
+    t = __ffma2_rn(d2, t, f2(-HPC_C1));
+    const float2 pl = __ffma2_rn(d2, t, one);
+    if (d2.x <= 81.0f) a.hsum.x = __fmaf_rn(X.x, pl.x, a.hsum.x);
+    if (PAIR && d2.y <= 81.0f) a.hsum.y = __fmaf_rn(X.y, pl.y, a.hsum.y);
   }
 }
 
+/* Pair loop over slots [i0, i1) of one (type, kind) segment held in shared memory; i0 is
+ * even, an odd i1 leaves one point for a half iteration. KIND bit 0: hydrophobic point (hpc),
+ * bit 1: class-2 point (psp). HDB: some lane of the warp has a live hydrogen-bond pair. */
+template <int KIND, bool HDB>
+__device__ __forceinline__ void pair_range(const float4 *__restrict__ PA,
+                                           const float4 *__restrict__ PB,
+                                           const float4 *__restrict__ PX, int i0, int i1,
+                                           float ax, float ay, float az, const Pair2 &q,
+                                           const float *__restrict__ psprow,
+                                           const GdForceConst &f, Acc &a) {
+  const float2 ax2 = f2(ax), ay2 = f2(ay), az2 = f2(az);
+  const int m0 = i0 >> 1, m1 = i1 >> 1;
+#pragma unroll 2
+  for (int m = m0; m < m1; ++m)
+    pair_body<KIND, HDB, true>(PA[m], PB[m], PX, m, ax2, ay2, az2, q, psprow, f, a);
+  if (i1 & 1) pair_body<KIND, HDB, false>(PA[m1], PB[m1], PX, m1, ax2, ay2, az2, q, psprow, f, a);
+}
+
+/* Per-replica state of the CTA's slots, in shared memory. */
 struct Slot {
   int rep, lig_conf, accept, n_acc;
   int rec_next, pad0;
   float mb, u;
+  float mm_old[6];
   float mm_new[6];
-  float pad1[2];
+  float rot[9];
+  float tx, ty, tz;
   gd_energy e_old;
   gd_replica replica;
 };
+static_assert(sizeof(Slot) == GD_SLOT_BYTES, "slot layout");
 
 /* deterministic warp sum of a double */
 __device__ __forceinline__ double warp_sum(double v) {
@@ -177,29 +232,64 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-#define NQ 10 /* vdw ele pmf psp hdb hpc kde rmsd ncon tp */
+#define NQ 10 /* vdw ele pmf psp hdb hsum->hpc kde rmsd ncon tp */
 
-__global__ void __launch_bounds__(GD_MAX_TPB) gd_mc_kernel(GdMcArgs a, GdForceConst f) {
+/* One segment range of the pair loop, dispatched on (kind, hdb). */
+__device__ __forceinline__ void pair_dispatch(int kind, bool hdb, const float4 *PA,
+                                              const float4 *PB, const float4 *PX, int i0, int i1,
+                                              float ax, float ay, float az, const Pair2 &pq,
+                                              const float *psprow, const GdForceConst &f,
+                                              Acc &acc) {
+  if (hdb) {
+    switch (kind) {
+      case 0: pair_range<0, true>(PA, PB, PX, i0, i1, ax, ay, az, pq, psprow, f, acc); break;
+      case 1: pair_range<1, true>(PA, PB, PX, i0, i1, ax, ay, az, pq, psprow, f, acc); break;
+      case 2: pair_range<2, true>(PA, PB, PX, i0, i1, ax, ay, az, pq, psprow, f, acc); break;
+      default: pair_range<3, true>(PA, PB, PX, i0, i1, ax, ay, az, pq, psprow, f, acc); break;
+    }
+  } else {
+    switch (kind) {
+      case 0: pair_range<0, false>(PA, PB, PX, i0, i1, ax, ay, az, pq, psprow, f, acc); break;
+      case 1: pair_range<1, false>(PA, PB, PX, i0, i1, ax, ay, az, pq, psprow, f, acc); break;
+      case 2: pair_range<2, false>(PA, PB, PX, i0, i1, ax, ay, az, pq, psprow, f, acc); break;
+      default: pair_range<3, false>(PA, PB, PX, i0, i1, ax, ay, az, pq, psprow, f, acc); break;
+    }
+  }
+}
+
+/*
+ * Shared memory: two mbarriers, two protein buffers of D points (float4 + float2), the
+ * placed atoms, NQ FP64 partials per lane, the slots. The protein buffers form a two-stage
+ * ring without CTA barriers: every warp waits on the buffer's "full" mbarrier by itself and,
+ * when done, bumps the buffer's counter; the last warp to finish refills the buffer with the
+ * chunk two ahead. Every wait is bounded (globaltimer); a wait that runs out sets the error
+ * word, the CTA leaves at the next step barrier after letting its copies in flight land.
+ */
+__global__ void __launch_bounds__(GD_MAX_TPB, 3) gd_mc_kernel(GdMcArgs a, GdForceConst f) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int T = blockDim.x, tid = threadIdx.x, D = a.chunk;
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem);
-  float4 *bpos = reinterpret_cast<float4 *>(smem + 16);
-  float2 *baux = reinterpret_cast<float2 *>(bpos + 2 * D);
-  float4 *atoms = reinterpret_cast<float4 *>(baux + 2 * D);
+  /* ring buffers: buffer b holds D slots as D/2 pairs in three float4 streams */
+  float4 *bpa = reinterpret_cast<float4 *>(smem + 16);
+  float4 *bpb = bpa + D;
+  float4 *bpx = bpb + D;
+  float4 *atoms = bpx + D;
   double *part = reinterpret_cast<double *>(atoms + T);
   Slot *slots = reinterpret_cast<Slot *>(part + NQ * T);
-  __shared__ int s_tile;
-  __shared__ int s_abort;
+  __shared__ int s_tile, s_abort;
+  __shared__ int s_done[2];
+  __shared__ unsigned s_issued[2];
 
   if (tid == 0) {
     mbar_init(&bar[0], 1);
     mbar_init(&bar[1], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     s_abort = 0;
+    s_done[0] = s_done[1] = 0;
+    s_issued[0] = s_issued[1] = 0;
   }
   __syncthreads();
-  uint32_t consumed0 = 0, consumed1 = 0; /* completed phases used per buffer */
-  uint32_t issued0 = 0, issued1 = 0;     /* copies issued per buffer (thread 0) */
+  uint32_t consumed0 = 0, consumed1 = 0; /* completed phases waited for, per buffer */
   const int step_first = a.step0 + (a.step_base ? *a.step_base : 0);
   const int warp = tid >> 5, lane = tid & 31, nwarps = T >> 5;
 
@@ -215,7 +305,7 @@ __global__ void __launch_bounds__(GD_MAX_TPB) gd_mc_kernel(GdMcArgs a, GdForceCo
     const int j = active ? tid / L : 0;
     const int l = active ? tid - j * L : 0;
 
-    /* ---- slot set-up ---- */
+    /* ---- slot set-up (one thread per replica) ---- */
     if (tid < k) {
       Slot &s = slots[tid];
       const int id = tile.rep_begin + tid;
@@ -231,144 +321,160 @@ __global__ void __launch_bounds__(GD_MAX_TPB) gd_mc_kernel(GdMcArgs a, GdForceCo
           s.e_old = a.e_old[id];
           s.n_acc = a.n_accept[id];
           s.rec_next = a.rec ? a.rec_next[id] : 0;
+#pragma unroll
+          for (int i = 0; i < 6; ++i) s.mm_old[i] = a.mm_old[(size_t)id * 6 + i];
         } else {
           s.n_acc = 0;
           s.rec_next = 0;
+#pragma unroll
+          for (int i = 0; i < 6; ++i) s.mm_old[i] = 0.0f;
         }
+      }
+    }
+
+    /* ---- protein tile pipeline ---- */
+    const int pc = tile.prt_conf;
+    const size_t pbase = (size_t)pc * (cx.pnp_pad >> 1);
+    const float4 *ga = cx.pt_a + pbase, *gb = cx.pt_b + pbase, *gx = cx.pt_x + pbase;
+    const int P = cx.pnp, pnp_pad = cx.pnp_pad;
+    const int nch = (pnp_pad + D - 1) / D;
+    const bool resident = nch <= 2;
+    const int nsteps = a.mode == 0 ? a.n_steps : 1;
+    const int total_q = resident ? nch : nsteps * nch;
+    if (tid == 0) {
+      s_done[0] = s_done[1] = 0;
+      for (int q = 0; q < min(2, total_q); ++q) {
+        const int b = q & 1, c0 = q * D, n = min(D, pnp_pad - c0);
+        s_issued[b] += 1;
+        mbar_expect_tx(&bar[b], (uint32_t)(n * 24));
+        bulk_g2s(bpa + b * (D >> 1), ga + (c0 >> 1), (uint32_t)(n * 8), &bar[b]);
+        bulk_g2s(bpb + b * (D >> 1), gb + (c0 >> 1), (uint32_t)(n * 8), &bar[b]);
+        bulk_g2s(bpx + b * (D >> 1), gx + (c0 >> 1), (uint32_t)(n * 8), &bar[b]);
       }
     }
     __syncthreads();
 
     /* ---- per-lane constants ---- */
     const int lig_conf = slots[j].lig_conf;
-    const int id = tile.rep_begin + j;
     const float4 orig = cx.lig_pos[lig_conf * L + l];
-    const int2 meta = cx.lig_meta[lig_conf * L + l];
-    const float cxo = cx.lig_center[lig_conf * 3 + 0], cyo = cx.lig_center[lig_conf * 3 + 1],
-                czo = cx.lig_center[lig_conf * 3 + 2];
-    const int tl = meta.x;
+    const int tl = cx.lig_meta[lig_conf * L + l].x;
     const float *psprow = cx.psp + (size_t)tl * cx.psp_ld;
     const GdPairParam *pprow = a.pp + tl * GD_MAXTP1;
-    float mm[6];
-    if (a.mode == 0) {
-#pragma unroll
-      for (int i = 0; i < 6; ++i) mm[i] = a.mm_old[(size_t)id * 6 + i];
-    }
-    const unsigned wmask = __ballot_sync(0xffffffffu, active);
-
-    /* ---- protein tile pipeline ---- */
-    const int pc = tile.prt_conf;
-    const float4 *gpos = cx.pt_pos + (size_t)pc * cx.pnp_pad;
-    const float2 *gaux = cx.pt_aux + (size_t)pc * cx.pnp_pad;
     const int4 *segs = cx.seg + pc * GD_MAX_SEG;
     const int nseg = cx.seg_count[pc];
-    const int P = cx.pnp;
-    const int nch = (P + D - 1) / D;
-    const bool resident = nch <= 2;
-    const int nsteps = a.mode == 0 ? a.n_steps : 1;
-    const int total_q = resident ? nch : nsteps * nch;
-    auto issue = [&](int q) {
-      const int c = q % nch, b = q & 1;
-      const int c0 = c * D;
-      const int n = min(D, cx.pnp_pad - c0);
-      if (b) ++issued1; else ++issued0;
-      mbar_expect_tx(&bar[b], (uint32_t)(n * 24));
-      bulk_g2s(bpos + b * D, gpos + c0, (uint32_t)(n * 16), &bar[b]);
-      bulk_g2s(baux + b * D, gaux + c0, (uint32_t)(n * 8), &bar[b]);
-    };
-    if (tid == 0) {
-      issue(0);
-      if (total_q > 1) issue(1);
-    }
+    const unsigned wmask = __ballot_sync(0xffffffffu, active);
     bool aborted = false;
 
     for (int s = 0; s < nsteps; ++s) {
-      /* ---- Move_d: draw, new pose, placed atom ---- */
-      float mmn[6], u = 0.0f;
-      if (a.mode == 0) {
-        float delta[6];
-        gd_draw_step(a.seed, (uint32_t)cx.stream, (uint32_t)(id - cx.rep_offset),
-                     (uint32_t)(step_first + s), a.move_kind, a.move_scale, delta, &u);
+      /* ---- Move_d: one thread per replica draws the move and builds the rotation ---- */
+      if (tid < k) {
+        Slot &sl = slots[tid];
+        float mmn[6], u = 0.0f;
+        if (a.mode == 0) {
+          float delta[6];
+          gd_draw_step(a.seed, (uint32_t)cx.stream, (uint32_t)(sl.rep - cx.rep_offset),
+                       (uint32_t)(step_first + s), a.move_kind, a.move_scale, delta, &u);
 #pragma unroll
-        for (int i = 0; i < 6; ++i) mmn[i] = GD_ADD(mm[i], delta[i]);
-      } else if (a.mode == 2) {
+          for (int i = 0; i < 6; ++i) mmn[i] = GD_ADD(sl.mm_old[i], delta[i]);
+        } else if (a.mode == 2) {
 #pragma unroll
-        for (int i = 0; i < 6; ++i) mmn[i] = a.mm_in[(size_t)id * 6 + i];
-      } else {
+          for (int i = 0; i < 6; ++i) mmn[i] = a.mm_in[(size_t)sl.rep * 6 + i];
+        } else {
 #pragma unroll
-        for (int i = 0; i < 6; ++i) mmn[i] = 0.0f;
+          for (int i = 0; i < 6; ++i) mmn[i] = 0.0f;
+        }
+        float rot[9];
+        gd_rotation(mmn, rot);
+#pragma unroll
+        for (int i = 0; i < 9; ++i) sl.rot[i] = rot[i];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) sl.mm_new[i] = mmn[i];
+        const float *lc = cx.lig_center + sl.lig_conf * 3;
+        sl.tx = GD_ADD(mmn[0], lc[0]);
+        sl.ty = GD_ADD(mmn[1], lc[1]);
+        sl.tz = GD_ADD(mmn[2], lc[2]);
+        sl.u = u;
       }
-      float rot[9];
-      gd_rotation(mmn, rot);
-      const float tx = GD_ADD(mmn[0], cxo), ty = GD_ADD(mmn[1], cyo), tz = GD_ADD(mmn[2], czo);
-      float ax, ay, az;
-      gd_place_atom(rot, tx, ty, tz, orig.x, orig.y, orig.z, &ax, &ay, &az);
-
-      double dv = 0, de = 0, dp = 0, ds = 0, dh = 0, dhs = 0;
+      __syncthreads();
+      float ax = 0.0f, ay = 0.0f, az = 0.0f;
+      if (active) {
+        const Slot &sl = slots[j];
+        gd_place_atom(sl.rot, sl.tx, sl.ty, sl.tz, orig.x, orig.y, orig.z, &ax, &ay, &az);
+        atoms[tid] = make_float4(ax, ay, az, 0.0f);
+      }
+#pragma unroll
+      for (int qi = 0; qi < NQ; ++qi) part[qi * T + tid] = 0.0;
       int ncon = 0;
 
+      /* ---- CalcEnergy_d pair loop over the protein ring ---- */
       for (int ci = 0; ci < nch; ++ci) {
         const int q = resident ? ci : s * nch + ci;
         const int b = q & 1;
         if (!resident || s == 0) {
-          const uint32_t par = b ? (consumed1 & 1u) : (consumed0 & 1u);
-          const bool ok = mbar_wait_bounded(&bar[b], par, a.timeout_ns);
-          if (ok) { if (b) ++consumed1; else ++consumed0; }
-          if (__syncthreads_or(!ok)) {
-            if (tid == 0) { atomicOr(a.err, GD_DEV_ERR_TIMEOUT); s_abort = 1; }
+          bool ok = !*(volatile int *)&s_abort;
+          if (ok) ok = mbar_wait_bounded(&bar[b], b ? (consumed1 & 1u) : (consumed0 & 1u),
+                                         a.timeout_ns);
+          if (!ok) {
             aborted = true;
+            if (lane == 0) { s_abort = 1; atomicOr(a.err, GD_DEV_ERR_TIMEOUT); }
             break;
           }
+          if (b) ++consumed1; else ++consumed0;
         }
         if (active) {
-          const float4 *P4 = bpos + b * D; /* local index = point index - c0 */
-          const float2 *X2 = baux + b * D;
-          const int c0 = ci * D, c1 = min(P, c0 + D);
+          const float4 *PA = bpa + b * (D >> 1); /* local slot = slot - c0 */
+          const float4 *PB = bpb + b * (D >> 1);
+          const float4 *PX = bpx + b * (D >> 1);
+          const int c0 = ci * D, c1 = min(pnp_pad, c0 + D);
           for (int sg = 0; sg < nseg; ++sg) {
             const int4 g = segs[sg];
             const int i0 = max(g.x, c0) - c0, i1 = min(g.y, c1) - c0;
             if (i0 >= i1) continue;
-            const float4 q0 = __ldg(reinterpret_cast<const float4 *>(pprow + g.z));
-            const float4 q1 = __ldg(reinterpret_cast<const float4 *>(pprow + g.z) + 1);
-            const float4 q2 = __ldg(reinterpret_cast<const float4 *>(pprow + g.z) + 2);
-            GdPairParam pq;
-            pq.p1a = q0.x; pq.p2a = q0.y; pq.p1l = q0.z; pq.thr = q0.w;
-            pq.pmf0 = q1.x; pq.pmf1 = q1.y; pq.hc1 = q1.z; pq.hc0 = q1.w;
-            pq.hs = q2.x; pq.hneed = q2.y;
-            const bool hdb = __any_sync(wmask, pq.hneed != 0.0f);
-            Acc acc = {0, 0, 0, 0, 0, 0, 0};
-            const int kind = g.w;
-            if (hdb) {
-              switch (kind) {
-                case 0: pair_range<0, true>(P4, X2, i0, i1, ax, ay, az, pq, psprow, f, acc); break;
-                case 1: pair_range<1, true>(P4, X2, i0, i1, ax, ay, az, pq, psprow, f, acc); break;
-                case 2: pair_range<2, true>(P4, X2, i0, i1, ax, ay, az, pq, psprow, f, acc); break;
-                default: pair_range<3, true>(P4, X2, i0, i1, ax, ay, az, pq, psprow, f, acc); break;
-              }
-            } else {
-              switch (kind) {
-                case 0: pair_range<0, false>(P4, X2, i0, i1, ax, ay, az, pq, psprow, f, acc); break;
-                case 1: pair_range<1, false>(P4, X2, i0, i1, ax, ay, az, pq, psprow, f, acc); break;
-                case 2: pair_range<2, false>(P4, X2, i0, i1, ax, ay, az, pq, psprow, f, acc); break;
-                default: pair_range<3, false>(P4, X2, i0, i1, ax, ay, az, pq, psprow, f, acc); break;
-              }
-            }
-            dv += acc.vdw; de += acc.ele; dp += acc.pmf; ds += acc.psp; dh += acc.hdb;
-            dhs += acc.hsum;
+            const float4 *pr = reinterpret_cast<const float4 *>(pprow + g.z);
+            const float4 q0 = __ldg(pr), q1 = __ldg(pr + 1), q2 = __ldg(pr + 2);
+            Pair2 pq;
+            pq.p1a = f2(q0.x); pq.mp2a = f2(-q0.y); pq.p1l = f2(q0.z); pq.thr = q0.w;
+            pq.mpmf0 = f2(-q1.x); pq.pmf1 = f2(q1.y); pq.hc1 = f2(q1.z); pq.hc0 = f2(q1.w);
+            pq.hs = f2(q2.x);
+            const bool hdb = __any_sync(wmask, q2.y != 0.0f);
+            const float2 z2 = f2(0.0f);
+            Acc acc = {z2, z2, z2, z2, z2, 0.0f, 0};
+            pair_dispatch(g.w, hdb, PA, PB, PX, i0, i1, ax, ay, az, pq, psprow, f, acc);
+            part[0 * T + tid] += (double)acc.vdw.x + (double)acc.vdw.y;
+            part[1 * T + tid] += (double)acc.ele.x + (double)acc.ele.y;
+            part[2 * T + tid] += (double)acc.pmf.x + (double)acc.pmf.y;
+            part[3 * T + tid] += (double)acc.psp;
+            part[4 * T + tid] += (double)acc.hdb.x + (double)acc.hdb.y;
+            part[5 * T + tid] += (double)acc.hsum.x + (double)acc.hsum.y;
             ncon += acc.ncon;
           }
         }
         if (!resident) {
-          __syncthreads(); /* every lane is done with buffer b */
-          if (tid == 0 && q + 2 < total_q) issue(q + 2);
+          /* the last warp done with buffer b refills it with chunk q + 2 */
+          __syncwarp();
+          if (lane == 0) {
+            __threadfence_block();
+            const int prev = atomicAdd(&s_done[b], 1);
+            if (prev == nwarps - 1) {
+              s_done[b] = 0;
+              if (q + 2 < total_q) {
+                const int c0 = ((q + 2) % nch) * D, n = min(D, pnp_pad - c0);
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                s_issued[b] += 1;
+                mbar_expect_tx(&bar[b], (uint32_t)(n * 24));
+                bulk_g2s(bpa + b * (D >> 1), ga + (c0 >> 1), (uint32_t)(n * 8), &bar[b]);
+                bulk_g2s(bpb + b * (D >> 1), gb + (c0 >> 1), (uint32_t)(n * 8), &bar[b]);
+                bulk_g2s(bpx + b * (D >> 1), gx + (c0 >> 1), (uint32_t)(n * 8), &bar[b]);
+              }
+            }
+          }
         }
       }
-      if (aborted) break;
 
       /* ---- per-atom tail: hpc, kde, rmsd, reference contacts ---- */
-      if (active) {
-        const double hpc2 = (dhs - (double)f.hpl0[tl]) / (double)f.hpl1[tl];
-        const double vhpc = 0.5 * hpc2 * hpc2 - (double)f.hpl2[tl];
+      if (active && !aborted) {
+        const double hpc2 = (part[5 * T + tid] - (double)f.hpl0[tl]) / (double)f.hpl1[tl];
+        part[5 * T + tid] = 0.5 * hpc2 * hpc2 - (double)f.hpl2[tl];
         float ks = 0.0f;
         int kn = 0;
         for (int kk = 0; kk < cx.pnk; ++kk) {
@@ -379,44 +485,38 @@ __global__ void __launch_bounds__(GD_MAX_TPB) gd_mc_kernel(GdMcArgs a, GdForceCo
             ++kn;
           }
         }
-        const double vkde = kn ? (double)ks / (double)kn : 0.0;
-        const float rx = ax - (orig.x + cxo), ry = ay - (orig.y + cyo), rz = az - (orig.z + czo);
-        const double vrms = (double)(rx * rx + ry * ry + rz * rz);
+        part[6 * T + tid] = kn ? (double)ks / (double)kn : 0.0;
+        const Slot &sl = slots[j];
+        const float *lc = cx.lig_center + sl.lig_conf * 3;
+        const float rx = ax - (orig.x + lc[0]), ry = ay - (orig.y + lc[1]),
+                    rz = az - (orig.z + lc[2]);
+        part[7 * T + tid] = (double)(rx * rx + ry * ry + rz * rz);
         int tp = 0;
         const int *rs = cx.ref_start + pc * (L + 1);
         for (int i = rs[l]; i < rs[l + 1]; ++i) {
           const float4 rp = __ldg(cx.ref_pts + i);
           tp += dist2(ax, ay, az, rp.x, rp.y, rp.z) <= rp.w ? 1 : 0;
         }
-        part[0 * T + tid] = dv;
-        part[1 * T + tid] = de * (double)orig.w;
-        part[2 * T + tid] = dp;
-        part[3 * T + tid] = ds;
-        part[4 * T + tid] = dh;
-        part[5 * T + tid] = vhpc;
-        part[6 * T + tid] = vkde;
-        part[7 * T + tid] = vrms;
+        part[1 * T + tid] *= (double)orig.w;
         part[8 * T + tid] = (double)ncon;
         part[9 * T + tid] = (double)tp;
-        atoms[tid] = make_float4(ax, ay, az, 0.0f);
-        if (l == 0) {
-          Slot &sl = slots[j];
-          sl.u = u;
-#pragma unroll
-          for (int i = 0; i < 6; ++i) sl.mm_new[i] = mmn[i];
-        }
       }
-      __syncthreads();
+      if (__syncthreads_or(aborted)) {
+        aborted = true;
+        break;
+      }
 
       /* ---- per-replica epilogue: one warp per slot ---- */
       for (int js = warp; js < k; js += nwarps) {
         Slot &sl = slots[js];
-        double tot[NQ];
-#pragma unroll
+        /* slot totals are written back over the slot's first partial */
+        double *tot = part + js * L;
+#pragma unroll 1
         for (int qi = 0; qi < NQ; ++qi) {
           double v = 0.0;
           for (int i = lane; i < L; i += 32) v += part[qi * T + js * L + i];
-          tot[qi] = warp_sum(v);
+          v = warp_sum(v);
+          if (lane == 0) tot[qi * T] = v;
         }
         /* MCS position restraints */
         double elhm = 0.0;
@@ -443,19 +543,18 @@ __global__ void __launch_bounds__(GD_MAX_TPB) gd_mc_kernel(GdMcArgs a, GdForceCo
         if (lane == 0) {
           const double Ld = (double)L;
           double e[GD_MAXWEI];
-          e[0] = tot[0] / Ld;
-          e[1] = tot[1] / Ld;
-          e[2] = tot[2] / Ld;
-          e[3] = tot[3] / Ld;
-          e[4] = tot[4] / Ld;
-          e[5] = tot[5] / Ld;
-          e[6] = tot[6] / (double)f.kde3 / Ld;
+          e[0] = tot[0 * T] / Ld;
+          e[1] = tot[1 * T] / Ld;
+          e[2] = tot[2 * T] / Ld;
+          e[3] = tot[3 * T] / Ld;
+          e[4] = tot[4 * T] / Ld;
+          e[5] = tot[5 * T] / Ld;
+          e[6] = tot[6 * T] / (double)f.kde3 / Ld;
           e[7] = log(elhm / (double)cx.pos);
           {
-            const float *lc = cx.lig_center + sl.lig_conf * 3;
-            const double dx = (double)GD_ADD(sl.mm_new[0], lc[0]) - (double)cx.pocket[0];
-            const double dy = (double)GD_ADD(sl.mm_new[1], lc[1]) - (double)cx.pocket[1];
-            const double dz = (double)GD_ADD(sl.mm_new[2], lc[2]) - (double)cx.pocket[2];
+            const double dx = (double)sl.tx - (double)cx.pocket[0];
+            const double dy = (double)sl.ty - (double)cx.pocket[1];
+            const double dz = (double)sl.tz - (double)cx.pocket[2];
             e[8] = sqrt(dx * dx + dy * dy + dz * dz);
           }
           double etot = 0.0;
@@ -468,13 +567,13 @@ __global__ void __launch_bounds__(GD_MAX_TPB) gd_mc_kernel(GdMcArgs a, GdForceCo
           }
           en.e[GD_MAXWEI - 1] = (float)etot;
           {
-            const double tp = tot[9], ncn = tot[8];
+            const double tp = tot[9 * T], ncn = tot[8 * T];
             const double fp = ncn - tp, fn = (double)cx.nref_total - tp;
             const double tn = Ld * (double)P - tp - fp - fn;
             const double dv2 = sqrt((tp + fp) * (tp + fn) * (tn + fp) * (tn + fn));
             en.cms = dv2 != 0.0 ? (float)((tp * tn - fp * fn) / dv2) : 0.0f;
           }
-          en.rmsd = (float)sqrt(tot[7] / Ld);
+          en.rmsd = (float)sqrt(tot[7 * T] / Ld);
           const int rid = sl.rep;
           if (a.mode == 2) {
             a.e_out[rid] = en;
@@ -485,6 +584,8 @@ __global__ void __launch_bounds__(GD_MAX_TPB) gd_mc_kernel(GdMcArgs a, GdForceCo
             sl.accept = acc;
             if (acc) {
               sl.e_old = en;
+#pragma unroll
+              for (int i = 0; i < 6; ++i) sl.mm_old[i] = sl.mm_new[i];
               if (a.mode == 0) sl.n_acc += 1;
               if (a.rec) {
                 const int kslot = sl.rec_next;
@@ -512,10 +613,6 @@ __global__ void __launch_bounds__(GD_MAX_TPB) gd_mc_kernel(GdMcArgs a, GdForceCo
         }
       }
       __syncthreads();
-      if (a.mode == 0 && active && slots[j].accept) {
-#pragma unroll
-        for (int i = 0; i < 6; ++i) mm[i] = mmn[i];
-      }
     }
 
     if (aborted) {
@@ -523,26 +620,22 @@ __global__ void __launch_bounds__(GD_MAX_TPB) gd_mc_kernel(GdMcArgs a, GdForceCo
        * the fixed drain limit) before the CTA leaves, then stop */
       if (tid == 0) {
         const long long drain_ns = 2000000000LL;
-        if (issued0 > consumed0) mbar_wait_bounded(&bar[0], consumed0 & 1u, drain_ns);
-        if (issued1 > consumed1) mbar_wait_bounded(&bar[1], consumed1 & 1u, drain_ns);
+        if (s_issued[0]) mbar_wait_bounded(&bar[0], (s_issued[0] - 1u) & 1u, drain_ns);
+        if (s_issued[1]) mbar_wait_bounded(&bar[1], (s_issued[1] - 1u) & 1u, drain_ns);
       }
       __syncthreads();
       break;
     }
 
     /* ---- write back replica state ---- */
-    if (a.mode != 2) {
-      if (tid < k) {
-        const Slot &sl = slots[tid];
-        a.e_old[sl.rep] = sl.e_old;
-        a.etotal[sl.rep] = sl.e_old.e[GD_MAXWEI - 1];
-        a.n_accept[sl.rep] = a.mode == 1 ? 0 : sl.n_acc;
-        if (a.rec) a.rec_next[sl.rep] = sl.rec_next;
-      }
-      if (active && l == 0) {
+    if (a.mode != 2 && tid < k) {
+      const Slot &sl = slots[tid];
+      a.e_old[sl.rep] = sl.e_old;
+      a.etotal[sl.rep] = sl.e_old.e[GD_MAXWEI - 1];
+      a.n_accept[sl.rep] = sl.n_acc;
+      if (a.rec) a.rec_next[sl.rep] = sl.rec_next;
 #pragma unroll
-        for (int i = 0; i < 6; ++i) a.mm_old[(size_t)id * 6 + i] = a.mode == 1 ? 0.0f : mm[i];
-      }
+      for (int i = 0; i < 6; ++i) a.mm_old[(size_t)sl.rep * 6 + i] = sl.mm_old[i];
     }
     __syncthreads();
   }
