@@ -202,8 +202,7 @@ def run_ours(args, rank, world, local_rank):
     # ---------------- device-timed throughput ----------------
     eng = engine.Engine(ff, [cx], params, device=dev)
     if args.tile:
-        k, ch = (int(v) for v in args.tile.split(","))
-        eng.set_tile(k, ch)
+        eng.set_tile(*(int(v) for v in args.tile.split(",")))
     tile_used = eng.tile()
     stream = torch.cuda.ExternalStream(eng.cuda_stream(), device=dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda:%d" % dev)
@@ -331,7 +330,8 @@ def run_ours(args, rank, world, local_rank):
                                   "replicas per GPU, gaussian moves, exchange/10",
                       "step": "10 MC steps + 1 exchange, all replicas",
                       "l2": "flushed between steps (256 MB write)",
-                      "tile": {"replicas_per_cta": tile_used[0], "chunk_points": tile_used[1]},
+                      "tile": {"replicas_per_cta": tile_used[0], "chunk_points": tile_used[1],
+                               "unroll": tile_used[2]},
                       "parallelism": "replica shards, no collective" if world > 1 else "1 GPU"},
            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
            "gpu_launches": 2 * args.steps + args.steps // max(1, intervals_per_dump)}
@@ -346,7 +346,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--tile", default="", help="replicas_per_cta,chunk_points (default: tuned)")
+    ap.add_argument("--tile", default="", help="replicas_per_cta,chunk_points[,unroll] (default: tuned)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

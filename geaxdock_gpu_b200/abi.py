@@ -112,7 +112,7 @@ class McParams(C.Structure):
 
 
 class Tile(C.Structure):
-    _fields_ = [("replicas_per_cta", I), ("chunk_points", I)]
+    _fields_ = [("replicas_per_cta", I), ("chunk_points", I), ("unroll", I)]
 
 
 class ReplicaState(C.Structure):

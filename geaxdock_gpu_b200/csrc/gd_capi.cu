@@ -23,7 +23,11 @@
 #include "gd_numerics.h"
 
 namespace gd {
+template <int UNROLL>
 __global__ void gd_mc_kernel(GdMcArgs a, GdForceConst f);
+extern template __global__ void gd_mc_kernel<1>(GdMcArgs, GdForceConst);
+extern template __global__ void gd_mc_kernel<2>(GdMcArgs, GdForceConst);
+extern template __global__ void gd_mc_kernel<4>(GdMcArgs, GdForceConst);
 __global__ void gd_exchange_kernel(const GdDevComplex *cxs, const int *group_base, int n_complex,
                                    int n_groups, gd_replica *replica, const float *etotal,
                                    int *acs, uint64_t seed, const int *call_base, int call_off,
@@ -88,7 +92,7 @@ struct gd_ctx {
   cudaStream_t stream = nullptr;
   gd_mc_params mc{};
   int n_complex = 0, n_rep = 0, n_groups = 0;
-  int threads = 256, chunk = 512, num_sms = 148;
+  int threads = 256, chunk = 512, unroll = 2, num_sms = 148;
   std::vector<ComplexInfo> info;
   std::vector<void *> allocs;
   GdForceConst fc{};
@@ -262,10 +266,18 @@ int ensure_counters(gd_ctx *c, int n) {
   return GD_OK;
 }
 
+typedef void (*McKernel)(GdMcArgs, GdForceConst);
+
+McKernel mc_kernel(int unroll) {
+  if (unroll >= 4) return gd::gd_mc_kernel<4>;
+  if (unroll >= 2) return gd::gd_mc_kernel<2>;
+  return gd::gd_mc_kernel<1>;
+}
+
 int grid_for(gd_ctx *c, int n_tiles, size_t smem) {
   int nb = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, gd::gd_mc_kernel, c->threads, smem) !=
-          cudaSuccess ||
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, mc_kernel(c->unroll), c->threads,
+                                                    smem) != cudaSuccess ||
       nb < 1)
     nb = 1;
   return std::max(1, std::min(n_tiles, nb * c->num_sms));
@@ -297,10 +309,10 @@ GdMcArgs base_args(gd_ctx *c) {
   return a;
 }
 
-int set_kernel_attrs(size_t smem) {
-  CK(cudaFuncSetAttribute(gd::gd_mc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)smem));
-  CK(cudaFuncSetAttribute(gd::gd_mc_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+int set_kernel_attrs(const gd_ctx *c, size_t smem) {
+  const McKernel k = mc_kernel(c->unroll);
+  CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CK(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
                           cudaSharedmemCarveoutMaxShared));
   return GD_OK;
 }
@@ -308,14 +320,14 @@ int set_kernel_attrs(size_t smem) {
 int launch_mc(gd_ctx *c, GdMcArgs a, const GdTileDesc *d_tiles, int n_tiles, int *counter) {
   if (n_tiles <= 0) return GD_OK;
   const size_t smem = smem_bytes(c);
-  int rc = set_kernel_attrs(smem);
+  int rc = set_kernel_attrs(c, smem);
   if (rc) return rc;
   a.tiles = d_tiles;
   a.n_tiles = n_tiles;
   a.tile_counter = counter;
   CK(cudaMemsetAsync(counter, 0, sizeof(int), c->stream));
   const int grid = grid_for(c, n_tiles, smem);
-  gd::gd_mc_kernel<<<grid, c->threads, smem, c->stream>>>(a, c->fc);
+  mc_kernel(c->unroll)<<<grid, c->threads, smem, c->stream>>>(a, c->fc);
   CK(cudaGetLastError());
   return GD_OK;
 }
@@ -462,6 +474,15 @@ int gd_create(const gd_enepara *ff, const gd_complex_desc *cxs, int n_complexes,
   if (!out) return fail(GD_ERR_INVALID, "null out");
   *out = nullptr;
   if (!ff || !cxs || !mc || n_complexes < 1) return fail(GD_ERR_INVALID, "null argument");
+  if (!(ff->el1 > 0.0f) || !std::isfinite(ff->el1))
+    return fail(GD_ERR_INVALID, "electrostatic scale el1 must be finite and > 0");
+  for (int i = 0; i < GD_MAXTP2; ++i)
+    for (int j = 0; j < GD_MAXTP1; ++j)
+      if (!(ff->pmf0[i][j] > -10.0f) || !(ff->pmf0[i][j] < 1e4f))
+        return fail(GD_ERR_INVALID,
+                    "pmf0[%d][%d] = %g outside (-10, 1e4): the contact-potential exponent "
+                    "would leave FP32 range",
+                    i, j, (double)ff->pmf0[i][j]);
   if (mc->steps_per_exchange < 1 || mc->steps_per_dump < 1)
     return fail(GD_ERR_INVALID, "steps_per_exchange and steps_per_dump must be >= 1");
   if (mc->move_kind != GD_MOVE_UNIFORM && mc->move_kind != GD_MOVE_GAUSSIAN)
@@ -503,6 +524,7 @@ int gd_create(const gd_enepara *ff, const gd_complex_desc *cxs, int n_complexes,
   f.a1 = ff->a1;
   f.b1 = ff->b1;
   f.inv_el1 = 1.0f / ff->el1;
+  f.near2 = f.inv_el1 * f.inv_el1;
   f.kde2 = ff->kde2;
   f.kde3 = ff->kde3;
   for (int i = 0; i < GD_MAXWEI; ++i) {
@@ -538,6 +560,9 @@ int gd_create(const gd_enepara *ff, const gd_complex_desc *cxs, int n_complexes,
         q.hc0 = live ? (float)(-(double)ff->hdb0[i][j] * (double)ff->hdb1[i][j] * hsc) : 0.0f;
         q.hs = live ? sqrt_2_pi_m1 * ff->hdb1[i][j] : 0.0f;
         q.hneed = live ? 1.0f : 0.0f;
+        /* pmf exponent (6 - r/2)(r - pmf0) log2(e) = cA d2 + b2 r + c2 */
+        q.b2 = (float)(1.4426950408889634 * (6.0 + 0.5 * (double)ff->pmf0[i][j]));
+        q.c2 = (float)(-6.0 * 1.4426950408889634 * (double)ff->pmf0[i][j]);
       }
   }
   int rc = upload(c, &c->d_pp, pp);
@@ -592,6 +617,16 @@ int gd_create(const gd_enepara *ff, const gd_complex_desc *cxs, int n_complexes,
     std::vector<int> seg_count(d.n_prt, 0);
     std::vector<std::vector<int>> slot_point(d.n_prt); /* point index per slot, -1: padding */
     int max_slots = 4;
+    /* the hydrogen-bond term runs for a point type when any atom type of this ligand has a
+     * live pair with it: one decision per segment for the whole CTA */
+    bool hdb_live[GD_MAXTP1] = {false};
+    {
+      bool lt_used[GD_MAXTP2] = {false};
+      for (int i = 0; i < d.n_lig * L; ++i) lt_used[d.lig_t[i]] = true;
+      for (int tp = 0; tp < GD_MAXTP1; ++tp)
+        for (int tl = 0; tl < GD_MAXTP2; ++tl)
+          if (lt_used[tl] && ff->hdb0[tl][tp] > 0.1f) hdb_live[tp] = true;
+    }
     for (int pc = 0; pc < d.n_prt; ++pc) {
       const int o = pc * P;
       std::vector<int> order(P), key(P);
@@ -609,7 +644,8 @@ int gd_create(const gd_enepara *ff, const gd_complex_desc *cxs, int n_complexes,
           if (sp.size() & 1) sp.push_back(-1);
           if (ns == GD_MAX_SEG) return bail(fail(GD_ERR_CAPACITY, "too many point segments"));
           const int s0 = (int)sp.size();
-          seg[(size_t)pc * GD_MAX_SEG + ns] = make_int4(s0, s0 + 1, d.prt_t[o + p], key[p] & 3);
+          seg[(size_t)pc * GD_MAX_SEG + ns] = make_int4(
+              s0, s0 + 1, d.prt_t[o + p], (key[p] & 3) | (hdb_live[d.prt_t[o + p]] ? 4 : 0));
           ++ns;
         } else {
           seg[(size_t)pc * GD_MAX_SEG + ns - 1].y = (int)sp.size() + 1;
@@ -641,7 +677,7 @@ int gd_create(const gd_enepara *ff, const gd_complex_desc *cxs, int n_complexes,
         A[0 + h] = -d.prt_x[o + p];
         A[2 + h] = -d.prt_y[o + p];
         B[0 + h] = -d.prt_z[o + p];
-        B[2 + h] = d.prt_ele[o + p];
+        B[2 + h] = d.prt_ele[o + p] * (1.0f / ff->el1); /* ele_p / el1 */
         X[0 + h] = (kind & 1) ? d.prt_hpp[o + p] : 0.0f;
         X[2 + h] = bits_as_float((kind & 2) ? d.prt_seq3r[o + p] : -1);
       }
@@ -774,6 +810,8 @@ int gd_replica_offset(const gd_ctx *c, int k, int *offset) {
 
 int gd_set_tile(gd_ctx *c, int k, const gd_tile *t) {
   if (!c || !t) return fail(GD_ERR_INVALID, "null argument");
+  if (t->unroll != 0 && t->unroll != 1 && t->unroll != 2 && t->unroll != 4)
+    return fail(GD_ERR_INVALID, "unroll must be 1, 2 or 4 (0 keeps the current value)");
   if (t->chunk_points < 4 || (t->chunk_points & 3) || t->chunk_points > 4096)
     return fail(GD_ERR_INVALID, "chunk_points must be a multiple of 4 in 4..4096");
   if (t->replicas_per_cta < 1 || t->replicas_per_cta > GD_MAX_SLOTS)
@@ -789,6 +827,7 @@ int gd_set_tile(gd_ctx *c, int k, const gd_tile *t) {
   c->info = info;
   c->threads = T;
   c->chunk = t->chunk_points;
+  if (t->unroll) c->unroll = t->unroll;
   c->tile_gen += 1;
   build_tiles(c, 0, c->n_rep - 1, c->full_tiles);
   int blocks = 0;
@@ -829,6 +868,7 @@ int gd_get_tile(const gd_ctx *c, int k, gd_tile *t) {
   if (!c || !t || k < 0 || k >= c->n_complex) return fail(GD_ERR_INVALID, "bad argument");
   t->replicas_per_cta = c->info[k].k;
   t->chunk_points = c->chunk;
+  t->unroll = c->unroll;
   return GD_OK;
 }
 
@@ -905,7 +945,7 @@ int gd_mc_run_fused(gd_ctx *c, int s1, int n_steps, int exchange) {
     if ((rc = upload_tiles(c, 0, c->n_rep - 1, &n))) return rc;
     CK(cudaStreamSynchronize(c->stream));
     const size_t smem = smem_bytes(c);
-    if ((rc = set_kernel_attrs(smem))) return rc;
+    if ((rc = set_kernel_attrs(c, smem))) return rc;
     const int grid = grid_for(c, n, smem);
     cudaGraph_t graph;
     CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
@@ -919,7 +959,7 @@ int gd_mc_run_fused(gd_ctx *c, int s1, int n_steps, int exchange) {
       a.tiles = c->d_tiles;
       a.n_tiles = n;
       a.tile_counter = c->d_counters + i;
-      gd::gd_mc_kernel<<<grid, c->threads, smem, c->stream>>>(a, c->fc);
+      mc_kernel(c->unroll)<<<grid, c->threads, smem, c->stream>>>(a, c->fc);
       if (exchange)
         gd::gd_exchange_kernel<<<(c->n_groups + 127) / 128, 128, 0, c->stream>>>(
             c->d_cx, c->d_group_base, c->n_complex, c->n_groups, c->d_replica, c->d_etotal,

@@ -29,6 +29,8 @@
 #define GD_MAX_SEG 96          /* (30 point types) x (3 kinds), rounded up */
 #define GD_MAX_TPB 256         /* threads per CTA: 3 CTAs of 256 fit the register file */
 #define GD_SLOT_BYTES 192      /* shared-memory bytes per replica slot (sizeof gd::Slot) */
+/* resident 256-thread CTAs per SM the register budget is set for, per unroll depth */
+#define GD_MIN_BLOCKS(u) ((u) >= 4 ? 2 : ((u) >= 2 ? 3 : 4))
 #define GD_MAX_SLOTS 128       /* replicas per CTA */
 #define GD_NQ 12               /* per-lane partial sums handed to the reducer */
 
@@ -40,7 +42,8 @@
 struct GdPairParam {
   float p1a, p2a, p1l, thr;    /* LJ numerators; p1a*lj0; contact threshold on d^2 */
   float pmf0, pmf1, hc1, hc0;  /* pmf; hdb argument h = r*hc1 + hc0 (scaled for exp2) */
-  float hs, hneed, pad0, pad1; /* hdb scale (0 when hdb0 <= 0.1); 1 if the hdb term is live */
+  float hs, hneed, b2, c2;     /* hdb scale (0 when hdb0 <= 0.1); 1 if the hdb term is live;
+                                  pmf exponent cA d2 + b2 r + c2 in base 2 */
 };
 
 struct GdDevComplex {
@@ -76,6 +79,7 @@ struct GdTileDesc {
 
 struct GdForceConst {
   float lj1, el0, el1, a1, b1, inv_el1;
+  float near2;                /* (1 / el1)^2: soft-core electrostatics inside */
   float kde2, kde3;
   float a_para[GD_MAXWEI], b_para[GD_MAXWEI], w[GD_MAXWEI];
   float hpl0[GD_MAXTP2], hpl1[GD_MAXTP2], hpl2[GD_MAXTP2];

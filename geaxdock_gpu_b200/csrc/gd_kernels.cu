@@ -109,7 +109,7 @@ struct Acc {
 
 /* Per-segment pair parameters, splatted over the two lanes of an FP32x2 register pair. */
 struct Pair2 {
-  float2 p1a, mp2a, p1l, mpmf0, pmf1, hc1, hc0, hs;
+  float2 p1a, mp2a, p1l, b2, c2, pmf1, hc1, hc0, hs;
   float thr;
 };
 
@@ -138,19 +138,29 @@ __device__ __forceinline__ void pair_body(const float4 A, const float4 B,
   const float2 num = __fmul2_rn(r6i, __ffma2_rn(q.p1a, r3i, q.mp2a));
   const float2 t9 = __fmul2_rn(q.p1l, __fmul2_rn(r6i, r3i));
   const float2 p4 = __ffma2_rn(t9, __ffma2_rn(f2(f.lj1), d2, one), one);
-  /* ele: q_l ele_p g(el1 r); q_l applied once per atom */
-  const float2 s1 = __fmul2_rn(f2(f.el1), r);
-  const float2 gn = __ffma2_rn(__fmul2_rn(s1, s1), __ffma2_rn(f2(f.b1), s1, f2(f.a1)), f2(f.el0));
-  const float2 gf = __fmul2_rn(ri, f2(f.inv_el1));
-  const float2 g = make_float2(s1.x < 1.0f ? gn.x : gf.x, s1.y < 1.0f ? gn.y : gf.y);
+  /* ele: q_l ele_p g(el1 r), q_l applied once per atom. Shared memory holds ele_p / el1, so
+   * the far branch g = 1 / (el1 r) is one FMA with r^-1; inside r < 1 / el1 (d2 < near2,
+   * rare) the soft core adds ele_p (g_near - g_far). g is continuous at el1 r = 1. */
   const float2 ep = make_float2(B.z, B.w);
-  /* pmf: pmf1 / (1 + exp((6 - r/2)(r - pmf0))), exp as exp2 with log2(e) folded */
-  const float2 tt = __fmul2_rn(__ffma2_rn(f2(-0.5f * LOG2E_F), r, f2(6.0f * LOG2E_F)),
-                               __fadd2_rn(r, q.mpmf0));
-  /* den <= 1 + 2^100 keeps p4 * den finite wherever p4 itself is (p4 is large only at
-   * r << 1 A, where tt < 0); the dropped tail of pmf1 / den is below 1e-30 */
-  const float2 den = __fadd2_rn(one, make_float2(ex2_a(fminf(tt.x, 100.0f)),
-                                                 ex2_a(fminf(tt.y, 100.0f))));
+  if constexpr (PAIR) {
+    a.ele = __ffma2_rn(ep, ri, a.ele);
+  } else {
+    a.ele.x = __fmaf_rn(ep.x, ri.x, a.ele.x);
+  }
+  if (d2.x < f.near2 || (PAIR && d2.y < f.near2)) {
+    const float2 s1 = __fmul2_rn(f2(f.el1), r);
+    const float2 gn =
+        __ffma2_rn(__fmul2_rn(s1, s1), __ffma2_rn(f2(f.b1), s1, f2(f.a1)), f2(f.el0));
+    /* ep (el1 gn) - ep ri = ele_p gn - ele_p g_far */
+    if (d2.x < f.near2) a.ele.x += __fmaf_rn(ep.x * f.el1, gn.x, -(ep.x * ri.x));
+    if (PAIR && d2.y < f.near2) a.ele.y += __fmaf_rn(ep.y * f.el1, gn.y, -(ep.y * ri.y));
+  }
+  /* pmf: pmf1 / (1 + exp((6 - r/2)(r - pmf0))) as exp2 of the expanded quadratic
+   * cA d2 + b2 r + c2 (cA = -log2(e)/2, b2 = log2(e)(6 + pmf0/2), c2 = -6 log2(e) pmf0).
+   * Its maximum over r is log2(e) (12 - pmf0)^2 / 8 < 100 for pmf0 > -10 (checked when the
+   * force field is loaded), so den stays finite and p4 den does wherever p4 does. */
+  const float2 tt = __ffma2_rn(q.b2, r, __ffma2_rn(f2(-0.5f * LOG2E_F), d2, q.c2));
+  const float2 den = __fadd2_rn(one, make_float2(ex2_a(tt.x), ex2_a(tt.y)));
   /* one reciprocal for both quotients: num / p4 = num den / (p4 den),
    * pmf1 / den = pmf1 p4 / (p4 den) */
   const float2 pd = __fmul2_rn(p4, den);
@@ -159,11 +169,9 @@ __device__ __forceinline__ void pair_body(const float4 A, const float4 B,
   const float2 pn = __fmul2_rn(q.pmf1, p4);
   if constexpr (PAIR) {
     a.vdw = __ffma2_rn(vn, inv, a.vdw);
-    a.ele = __ffma2_rn(ep, g, a.ele);
     a.pmf = __ffma2_rn(pn, inv, a.pmf);
   } else {
     a.vdw.x = __fmaf_rn(vn.x, inv.x, a.vdw.x);
-    a.ele.x = __fmaf_rn(ep.x, g.x, a.ele.x);
     a.pmf.x = __fmaf_rn(pn.x, inv.x, a.pmf.x);
   }
   /* contacts (mcc, psp): sqrtf(d2) <= pmf0  <=>  d2 <= thr */
@@ -195,8 +203,10 @@ __device__ __forceinline__ void pair_body(const float4 A, const float4 B,
 
 /* Pair loop over slots [i0, i1) of one (type, kind) segment held in shared memory; i0 is
  * even, an odd i1 leaves one point for a half iteration. KIND bit 0: hydrophobic point (hpc),
- * bit 1: class-2 point (psp). HDB: some lane of the warp has a live hydrogen-bond pair. */
-template <int KIND, bool HDB>
+ * bit 1: class-2 point (psp). HDB: the segment's point type has a live hydrogen-bond pair
+ * with some atom type of the ligand (decided per complex on the host, so every warp of the
+ * CTA runs the same code). UNROLL: point pairs in flight per lane. */
+template <int KIND, bool HDB, int UNROLL>
 __device__ __forceinline__ void pair_range(const float4 *__restrict__ PA,
                                            const float4 *__restrict__ PB,
                                            const float4 *__restrict__ PX, int i0, int i1,
@@ -205,7 +215,7 @@ __device__ __forceinline__ void pair_range(const float4 *__restrict__ PA,
                                            const GdForceConst &f, Acc &a) {
   const float2 ax2 = f2(ax), ay2 = f2(ay), az2 = f2(az);
   const int m0 = i0 >> 1, m1 = i1 >> 1;
-#pragma unroll 2
+#pragma unroll UNROLL
   for (int m = m0; m < m1; ++m)
     pair_body<KIND, HDB, true>(PA[m], PB[m], PX, m, ax2, ay2, az2, q, psprow, f, a);
   if (i1 & 1) pair_body<KIND, HDB, false>(PA[m1], PB[m1], PX, m1, ax2, ay2, az2, q, psprow, f, a);
@@ -234,27 +244,26 @@ __device__ __forceinline__ double warp_sum(double v) {
 
 #define NQ 10 /* vdw ele pmf psp hdb hsum->hpc kde rmsd ncon tp */
 
-/* One segment range of the pair loop, dispatched on (kind, hdb). */
-__device__ __forceinline__ void pair_dispatch(int kind, bool hdb, const float4 *PA,
-                                              const float4 *PB, const float4 *PX, int i0, int i1,
-                                              float ax, float ay, float az, const Pair2 &pq,
+/* One segment range of the pair loop, dispatched on the segment kind: bits 0-1 point kind,
+ * bit 2 live hydrogen-bond term. */
+template <int UNROLL>
+__device__ __forceinline__ void pair_dispatch(int kind, const float4 *PA, const float4 *PB,
+                                              const float4 *PX, int i0, int i1, float ax,
+                                              float ay, float az, const Pair2 &pq,
                                               const float *psprow, const GdForceConst &f,
                                               Acc &acc) {
-  if (hdb) {
-    switch (kind) {
-      case 0: pair_range<0, true>(PA, PB, PX, i0, i1, ax, ay, az, pq, psprow, f, acc); break;
-      case 1: pair_range<1, true>(PA, PB, PX, i0, i1, ax, ay, az, pq, psprow, f, acc); break;
-      case 2: pair_range<2, true>(PA, PB, PX, i0, i1, ax, ay, az, pq, psprow, f, acc); break;
-      default: pair_range<3, true>(PA, PB, PX, i0, i1, ax, ay, az, pq, psprow, f, acc); break;
-    }
-  } else {
-    switch (kind) {
-      case 0: pair_range<0, false>(PA, PB, PX, i0, i1, ax, ay, az, pq, psprow, f, acc); break;
-      case 1: pair_range<1, false>(PA, PB, PX, i0, i1, ax, ay, az, pq, psprow, f, acc); break;
-      case 2: pair_range<2, false>(PA, PB, PX, i0, i1, ax, ay, az, pq, psprow, f, acc); break;
-      default: pair_range<3, false>(PA, PB, PX, i0, i1, ax, ay, az, pq, psprow, f, acc); break;
-    }
+#define GD_PR(K, H) pair_range<K, H, UNROLL>(PA, PB, PX, i0, i1, ax, ay, az, pq, psprow, f, acc)
+  switch (kind) {
+    case 0: GD_PR(0, false); break;
+    case 1: GD_PR(1, false); break;
+    case 2: GD_PR(2, false); break;
+    case 3: GD_PR(3, false); break;
+    case 4: GD_PR(0, true); break;
+    case 5: GD_PR(1, true); break;
+    case 6: GD_PR(2, true); break;
+    default: GD_PR(3, true); break;
   }
+#undef GD_PR
 }
 
 /*
@@ -265,7 +274,9 @@ __device__ __forceinline__ void pair_dispatch(int kind, bool hdb, const float4 *
  * chunk two ahead. Every wait is bounded (globaltimer); a wait that runs out sets the error
  * word, the CTA leaves at the next step barrier after letting its copies in flight land.
  */
-__global__ void __launch_bounds__(GD_MAX_TPB, 3) gd_mc_kernel(GdMcArgs a, GdForceConst f) {
+template <int UNROLL>
+__global__ void __launch_bounds__(GD_MAX_TPB, GD_MIN_BLOCKS(UNROLL))
+    gd_mc_kernel(GdMcArgs a, GdForceConst f) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int T = blockDim.x, tid = threadIdx.x, D = a.chunk;
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem);
@@ -362,7 +373,6 @@ __global__ void __launch_bounds__(GD_MAX_TPB, 3) gd_mc_kernel(GdMcArgs a, GdForc
     const GdPairParam *pprow = a.pp + tl * GD_MAXTP1;
     const int4 *segs = cx.seg + pc * GD_MAX_SEG;
     const int nseg = cx.seg_count[pc];
-    const unsigned wmask = __ballot_sync(0xffffffffu, active);
     bool aborted = false;
 
     for (int s = 0; s < nsteps; ++s) {
@@ -434,12 +444,11 @@ __global__ void __launch_bounds__(GD_MAX_TPB, 3) gd_mc_kernel(GdMcArgs a, GdForc
             const float4 q0 = __ldg(pr), q1 = __ldg(pr + 1), q2 = __ldg(pr + 2);
             Pair2 pq;
             pq.p1a = f2(q0.x); pq.mp2a = f2(-q0.y); pq.p1l = f2(q0.z); pq.thr = q0.w;
-            pq.mpmf0 = f2(-q1.x); pq.pmf1 = f2(q1.y); pq.hc1 = f2(q1.z); pq.hc0 = f2(q1.w);
-            pq.hs = f2(q2.x);
-            const bool hdb = __any_sync(wmask, q2.y != 0.0f);
+            pq.pmf1 = f2(q1.y); pq.hc1 = f2(q1.z); pq.hc0 = f2(q1.w);
+            pq.hs = f2(q2.x); pq.b2 = f2(q2.z); pq.c2 = f2(q2.w);
             const float2 z2 = f2(0.0f);
             Acc acc = {z2, z2, z2, z2, z2, 0.0f, 0};
-            pair_dispatch(g.w, hdb, PA, PB, PX, i0, i1, ax, ay, az, pq, psprow, f, acc);
+            pair_dispatch<UNROLL>(g.w, PA, PB, PX, i0, i1, ax, ay, az, pq, psprow, f, acc);
             part[0 * T + tid] += (double)acc.vdw.x + (double)acc.vdw.y;
             part[1 * T + tid] += (double)acc.ele.x + (double)acc.ele.y;
             part[2 * T + tid] += (double)acc.pmf.x + (double)acc.pmf.y;
@@ -640,6 +649,11 @@ __global__ void __launch_bounds__(GD_MAX_TPB, 3) gd_mc_kernel(GdMcArgs a, GdForc
     __syncthreads();
   }
 }
+
+/* the kernel variants the host can launch (point pairs in flight per lane) */
+template __global__ void gd_mc_kernel<1>(GdMcArgs, GdForceConst);
+template __global__ void gd_mc_kernel<2>(GdMcArgs, GdForceConst);
+template __global__ void gd_mc_kernel<4>(GdMcArgs, GdForceConst);
 
 /* ExchangeReplicas_d, one thread per (complex, protein conformer, ligand conformer) group. */
 __global__ void gd_exchange_kernel(const GdDevComplex *cxs, const int *group_base, int n_complex,

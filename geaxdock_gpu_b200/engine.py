@@ -163,9 +163,10 @@ class Engine:
     def sync(self):
         check(lib().gd_sync(self.h))
 
-    def set_tile(self, replicas_per_cta: int, chunk_points: int, complex_index: int = -1):
+    def set_tile(self, replicas_per_cta: int, chunk_points: int, unroll: int = 0,
+                 complex_index: int = -1):
         t = abi.Tile()
-        t.replicas_per_cta, t.chunk_points = replicas_per_cta, chunk_points
+        t.replicas_per_cta, t.chunk_points, t.unroll = replicas_per_cta, chunk_points, unroll
         check(lib().gd_set_tile(self.h, complex_index, C.byref(t)))
 
     def cuda_stream(self) -> int:
@@ -183,7 +184,7 @@ class Engine:
     def tile(self, complex_index=0):
         t = abi.Tile()
         check(lib().gd_get_tile(self.h, complex_index, C.byref(t)))
-        return t.replicas_per_cta, t.chunk_points
+        return t.replicas_per_cta, t.chunk_points, t.unroll
 
     # ---- results ----
     def records(self, r0=0, r1=None):

@@ -164,6 +164,7 @@ typedef struct {
 typedef struct {
   int replicas_per_cta;     /* replicas sharing one protein tile in one CTA */
   int chunk_points;         /* protein points staged per shared-memory buffer */
+  int unroll;               /* protein point pairs in flight per lane: 1, 2 or 4 (0: keep) */
 } gd_tile;
 
 /* Per-replica Monte Carlo state (checkpoint unit). */

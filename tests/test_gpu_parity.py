@@ -69,7 +69,7 @@ def test_chunk_pipeline_gives_same_energies(raw, chunk):
     rm = po.ref_map(ff, cx)
     mm = np.random.default_rng(9).normal(0, 0.5, (16, 6)).astype(np.float32)
     with engine.Engine(ff, [cx], w.params) as eng:
-        k, _ = eng.tile()
+        k = eng.tile()[0]
         eng.set_tile(k, chunk)
         worst = _energy_check(eng, ff, cx, 0, 3, 2, mm, rm)
         assert worst.max() <= TOL
@@ -269,7 +269,7 @@ def test_bounded_wait_times_out_without_fault(raw):
     params = w.params
     params.record = 0
     with engine.Engine(ff, [cx], params) as eng:
-        k, _ = eng.tile()
+        k = eng.tile()[0]
         eng.set_tile(k, 64)  # streaming tiles: many waits
         eng.mc_init()
         eng.sync()
