@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1216,3 +1217,106 @@ int gd_trace_get(gd_ctx *c, float *e_new, int *acc, int *n_steps) {
 }
 
 }  // extern "C"
+
+/* ---------------- pose evaluation without allocation ----------------
+ *
+ * Some callers cannot call cudaMalloc at the moment they need energies: code that runs while
+ * another framework owns all device memory through its own pool, code inside a real-time or
+ * callback context where an allocation (and its implicit synchronisation) is not allowed, or
+ * a host that has already placed its poses and result buffer in device memory it manages.
+ * gd_eval_energy_noalloc serves them: it reads poses from, and writes energies to, device
+ * buffers the caller passes, and keeps the only scratch it needs (the pose work queue, the
+ * tile list and the per-pose conformer index) in the fixed device array below. That array
+ * holds up to GD_NOALLOC_MAX_POSES poses, is allocated once when the library is loaded on a
+ * device and stays there until the process exits, and is shared by every call in the
+ * process: each call rewrites the parts it uses (the queue head is cleared by the fill
+ * kernel), and calls whose kernels overlap on the GPU would race on it. */
+
+namespace {
+
+struct NoallocScratch {
+  GdTileDesc tiles[GD_NOALLOC_MAX_POSES];
+  int lig_conf[GD_NOALLOC_MAX_POSES];
+  int counter;
+};
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoallocScratch)];
+
+/* Writes the tile list, the per-pose conformer index and a cleared queue head into the
+ * scratch array for n poses of one (complex, protein conformer, ligand conformer). */
+__global__ void gd_noalloc_fill(int complex_index, int prt_conf, int lig_conf, int n, int k) {
+  NoallocScratch *s = reinterpret_cast<NoallocScratch *>(g_noalloc_scratch);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) s->counter = 0;
+  if (i < n) {
+    s->lig_conf[i] = lig_conf;
+    if (i % k == 0) {
+      GdTileDesc t;
+      t.complex_index = complex_index;
+      t.prt_conf = prt_conf;
+      t.rep_begin = i;
+      t.count = min(k, n - i);
+      s->tiles[i / k] = t;
+    }
+  }
+}
+
+std::mutex g_noalloc_mu;
+void *g_noalloc_addr[64] = {nullptr};
+
+/* Device address of the scratch array on `device` (the current device), looked up once per
+ * device: host code cannot use the symbol itself as a device address. */
+int noalloc_scratch(int device, NoallocScratch **out) {
+  if (device < 0 || device >= 64) return fail(GD_ERR_NODEVICE, "device %d out of range", device);
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[device]) {
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      return fail(GD_ERR_CUDA, "cudaGetSymbolAddress(scratch) failed: %s", cudaGetErrorString(e));
+    g_noalloc_addr[device] = p;
+  }
+  *out = reinterpret_cast<NoallocScratch *>(g_noalloc_addr[device]);
+  return GD_OK;
+}
+
+}  // namespace
+
+extern "C" int gd_eval_energy_noalloc(gd_ctx *c, int ci, int prt_conf, int lig_conf,
+                                      const float *d_movematrix, int n, gd_energy *d_out) {
+  if (!c || !d_movematrix || !d_out) return fail(GD_ERR_INVALID, "null argument");
+  if (ci < 0 || ci >= c->n_complex) return fail(GD_ERR_INVALID, "bad complex index");
+  const ComplexInfo &x = c->info[ci];
+  if (prt_conf < 0 || prt_conf >= x.n_prt || lig_conf < 0 || lig_conf >= x.n_lig)
+    return fail(GD_ERR_INVALID, "conformer index out of range");
+  if (n < 0 || n > GD_NOALLOC_MAX_POSES)
+    return fail(GD_ERR_CAPACITY,
+                "gd_eval_energy_noalloc: %d poses; the allocation-free path holds at most %d "
+                "(split the batch or use gd_eval_energy)",
+                n, GD_NOALLOC_MAX_POSES);
+  if (n == 0) return GD_OK;
+  CK(cudaSetDevice(c->device));
+  NoallocScratch *s = nullptr;
+  int rc = noalloc_scratch(c->device, &s);
+  if (rc) return rc;
+  const int k = x.k, n_tiles = (n + k - 1) / k;
+  gd_noalloc_fill<<<(n + 255) / 256, 256, 0, c->stream>>>(ci, prt_conf, lig_conf, n, k);
+  CK(cudaGetLastError());
+  GdMcArgs a = base_args(c);
+  a.mode = 2;
+  a.n_steps = 1;
+  a.mm_in = d_movematrix;
+  a.lig_conf_in = s->lig_conf;
+  a.e_out = d_out;
+  a.rec = nullptr;
+  a.trace_e = nullptr;
+  a.tiles = s->tiles;
+  a.n_tiles = n_tiles;
+  a.tile_counter = &s->counter;
+  const size_t smem = smem_bytes(c);
+  if ((rc = set_kernel_attrs(c, smem))) return rc;
+  const int grid = grid_for(c, n_tiles, smem);
+  mc_kernel(c->unroll)<<<grid, c->threads, smem, c->stream>>>(a, c->fc);
+  CK(cudaGetLastError());
+  return GD_OK;
+}
