@@ -201,13 +201,18 @@ def run_ours(args, rank, world, local_rank):
 
     # ---------------- device-timed throughput ----------------
     eng = engine.Engine(ff, [cx], params, device=dev)
+    eng.mc_init()
+    eng.sync()
     if args.tile:
         eng.set_tile(*(int(v) for v in args.tile.split(",")))
+        tile_source = "given"
+    else:
+        from geaxdock_gpu_b200 import autotune
+        tile_source = "autotuned (cached)" if autotune.tune(eng, device=dev)["cached"] \
+            else "autotuned"
     tile_used = eng.tile()
     stream = torch.cuda.ExternalStream(eng.cuda_stream(), device=dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda:%d" % dev)
-    eng.mc_init()
-    eng.sync()
     it = 0
 
     def one_step(ev=None):
@@ -331,7 +336,7 @@ def run_ours(args, rank, world, local_rank):
                       "step": "10 MC steps + 1 exchange, all replicas",
                       "l2": "flushed between steps (256 MB write)",
                       "tile": {"replicas_per_cta": tile_used[0], "chunk_points": tile_used[1],
-                               "unroll": tile_used[2]},
+                               "unroll": tile_used[2], "source": tile_source},
                       "parallelism": "replica shards, no collective" if world > 1 else "1 GPU"},
            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
            "gpu_launches": 2 * args.steps + args.steps // max(1, intervals_per_dump)}

@@ -122,6 +122,21 @@ class ReplicaState(C.Structure):
     ]
 
 
+class SurParams(C.Structure):
+    _fields_ = [
+        ("hidden", I), ("embedding", I), ("lr", F), ("batch", I), ("sample_cap", C.c_longlong),
+        ("fallback_accept", F), ("fallback_window", C.c_longlong), ("seed", C.c_uint64),
+    ]
+
+
+class SurStats(C.Structure):
+    _fields_ = [
+        ("proposed", C.c_longlong), ("passed", C.c_longlong), ("accepted", C.c_longlong),
+        ("plain", C.c_longlong), ("plain_accepted", C.c_longlong), ("rmse", C.c_double),
+        ("n_err", C.c_longlong), ("active", I), ("pad", I),
+    ]
+
+
 assert C.sizeof(Energy) == 48
 assert C.sizeof(Replica) == 16
 assert C.sizeof(RecordStep) == 92

@@ -1,0 +1,88 @@
+"""Tile autotuner with a JSON cache.
+
+The fused kernel's tile is (replicas per CTA, protein points per shared-memory chunk, point
+pairs in flight per lane). `tune(engine)` times a candidate grid with gd_autotune (pose
+evaluation of the chains' current poses, chains untouched), applies the fastest and stores it
+in a JSON cache keyed by (ligand atoms, protein points, replicas, device name); later engines
+with the same key reuse the entry without timing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json
+import os
+from typing import Dict, List, Optional, Sequence, Tuple
+
+from . import abi
+from .engine import Engine, check, lib
+
+DEFAULT_CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tile_cache.json")
+
+
+def candidates(lna: int) -> List[Tuple[int, int, int]]:
+    """Replicas per CTA that fill 128..256 lanes, chunk depths, unroll depths."""
+    ks = sorted({max(1, t // lna) for t in (128, 160, 192, 224, 256)} | {1})
+    ks = [k for k in ks if k * lna <= 256]
+    out = []
+    for k in ks:
+        for chunk in (256, 512, 1024):
+            for unroll in (1, 2):
+                out.append((k, chunk, unroll))
+    return out
+
+
+def _key(eng: Engine, device_name: str) -> str:
+    cx = eng.complexes
+    lna = max(c.lna for c in cx)
+    pnp = max(c.pnp for c in cx)
+    return "lna%d_pnp%d_rep%d_%s" % (lna, pnp, eng.n_rep, device_name.replace(" ", "_"))
+
+
+def _device_name(device: int) -> str:
+    try:
+        import torch
+        return torch.cuda.get_device_name(device)
+    except Exception:
+        return "cuda%d" % device
+
+
+def time_candidates(eng: Engine, cands: Sequence[Tuple[int, int, int]], repeats: int = 2):
+    arr = (abi.Tile * len(cands))()
+    for i, (k, ch, u) in enumerate(cands):
+        arr[i].replicas_per_cta, arr[i].chunk_points, arr[i].unroll = k, ch, u
+    best = abi.Tile()
+    ms = (C.c_float * len(cands))()
+    fn = lib().gd_autotune
+    fn.argtypes = [C.c_void_p, C.POINTER(abi.Tile), C.c_int, C.c_int, C.POINTER(abi.Tile),
+                   C.POINTER(C.c_float)]
+    fn.restype = C.c_int
+    check(fn(eng.h, arr, len(cands), repeats, C.byref(best), ms))
+    return (best.replicas_per_cta, best.chunk_points, best.unroll), list(ms)
+
+
+def tune(eng: Engine, cache_path: Optional[str] = DEFAULT_CACHE, device: int = 0,
+         repeats: int = 2, force: bool = False) -> Dict:
+    name = _device_name(device)
+    key = _key(eng, name)
+    cache = {}
+    if cache_path and os.path.exists(cache_path):
+        try:
+            cache = json.load(open(cache_path))
+        except (OSError, ValueError):
+            cache = {}
+    if key in cache and not force:
+        k, ch, u = cache[key]["tile"]
+        eng.set_tile(k, ch, u)
+        return dict(cache[key], cached=True)
+    lna = max(c.lna for c in eng.complexes)
+    cands = candidates(lna)
+    best, ms = time_candidates(eng, cands, repeats)
+    entry = {"tile": list(best), "ms": {"%d,%d,%d" % c: round(m, 4) for c, m in zip(cands, ms)}}
+    cache[key] = entry
+    if cache_path:
+        try:
+            with open(cache_path, "w") as f:
+                json.dump(cache, f, indent=1, sort_keys=True)
+        except OSError:
+            pass
+    return dict(entry, cached=False)

@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "gd_device.cuh"
+#include "gd_mlp.cuh"
 #include "gd_numerics.h"
 
 namespace gd {
@@ -135,6 +136,8 @@ struct gd_ctx {
   GdTileDesc *d_eval_tiles = nullptr;
   int eval_tiles_cap = 0;
   long long timeout_ns = 2000000000LL;
+  /* surrogate and delayed acceptance (gd_sur_create) */
+  struct DaState *da = nullptr;
 };
 
 namespace {
@@ -364,9 +367,13 @@ int check_range(const gd_ctx *c, int r0, int r1) {
   return GD_OK;
 }
 
+void da_free(gd_ctx *c);        /* delayed-acceptance state, defined with its entry points */
+void da_drop_graphs(gd_ctx *c);
+
 void drop_graphs(gd_ctx *c) {
   for (auto &g : c->graphs) cudaGraphExecDestroy(g.second);
   c->graphs.clear();
+  da_drop_graphs(c);
 }
 
 }  // namespace
@@ -456,6 +463,7 @@ int gd_destroy(gd_ctx *c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   drop_graphs(c);
+  da_free(c);
   for (void *p : c->allocs) cudaFree(p);
   if (c->d_counters) cudaFree(c->d_counters);
   if (c->d_trace_e) cudaFree(c->d_trace_e);
@@ -843,6 +851,91 @@ int gd_set_tile(gd_ctx *c, int k, const gd_tile *t) {
   }
   drop_graphs(c);
   return GD_OK;
+}
+
+int gd_autotune(gd_ctx *c, const gd_tile *cand, int n_cand, int repeats, gd_tile *best,
+                float *ms_out) {
+  if (!c || !cand || n_cand < 1 || repeats < 1 || !best)
+    return fail(GD_ERR_INVALID, "gd_autotune: bad arguments");
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->stream));
+  /* the probe evaluates pose id == replica id: poses are the chains' mm_old, ligand
+   * conformer per pose from the replica table */
+  std::vector<gd_replica> rep(c->n_rep);
+  CK(cudaMemcpy(rep.data(), c->d_replica, sizeof(gd_replica) * c->n_rep, cudaMemcpyDeviceToHost));
+  std::vector<int> lc(c->n_rep);
+  for (int r = 0; r < c->n_rep; ++r) lc[r] = rep[r].idx_lig;
+  int *d_lc = nullptr;
+  gd_energy *d_e = nullptr;
+  CK(cudaMalloc(&d_lc, sizeof(int) * c->n_rep));
+  if (cudaMalloc(&d_e, sizeof(gd_energy) * c->n_rep) != cudaSuccess) {
+    cudaFree(d_lc);
+    return fail(GD_ERR_NOMEM, "gd_autotune: no memory for the probe");
+  }
+  cudaMemcpy(d_lc, lc.data(), sizeof(int) * c->n_rep, cudaMemcpyHostToDevice);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const gd_tile keep_tile = {c->info[0].k, c->chunk, c->unroll};
+  std::vector<int> keep_k;
+  for (auto &x : c->info) keep_k.push_back(x.k);
+  const int keep_threads = c->threads;
+  int best_i = -1, rc = GD_OK;
+  float best_ms = 1e30f;
+  for (int i = 0; i < n_cand && rc == GD_OK; ++i) {
+    if ((rc = gd_set_tile(c, -1, &cand[i])) != GD_OK) {
+      /* a candidate that does not fit this batch is skipped */
+      if (ms_out) ms_out[i] = -1.0f;
+      rc = GD_OK;
+      continue;
+    }
+    int n = 0;
+    if ((rc = upload_tiles(c, 0, c->n_rep - 1, &n))) break;
+    GdMcArgs a = base_args(c);
+    a.mode = 2;
+    a.n_steps = 1;
+    a.mm_in = c->d_mm;
+    a.lig_conf_in = d_lc;
+    a.e_out = d_e;
+    a.rec = nullptr;
+    a.trace_e = nullptr;
+    if ((rc = launch_mc(c, a, c->d_tiles, n, c->d_counters))) break; /* warm-up */
+    cudaEventRecord(e0, c->stream);
+    for (int r = 0; r < repeats && rc == GD_OK; ++r)
+      rc = launch_mc(c, a, c->d_tiles, n, c->d_counters);
+    cudaEventRecord(e1, c->stream);
+    if (cudaEventSynchronize(e1) != cudaSuccess) {
+      rc = fail(GD_ERR_CUDA, "gd_autotune: probe failed");
+      break;
+    }
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    ms /= (float)repeats;
+    if (ms_out) ms_out[i] = ms;
+    if (ms < best_ms) {
+      best_ms = ms;
+      best_i = i;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(d_lc);
+  cudaFree(d_e);
+  if (rc == GD_OK && best_i >= 0) {
+    rc = gd_set_tile(c, -1, &cand[best_i]);
+    *best = cand[best_i];
+    best->unroll = c->unroll;
+  } else {
+    /* restore the tile in use before the probe */
+    for (int i = 0; i < c->n_complex; ++i) c->info[i].k = keep_k[i];
+    c->threads = keep_threads;
+    c->chunk = keep_tile.chunk_points;
+    c->unroll = keep_tile.unroll;
+    c->tile_gen += 1;
+    build_tiles(c, 0, c->n_rep - 1, c->full_tiles);
+    if (rc == GD_OK) rc = fail(GD_ERR_INVALID, "gd_autotune: no candidate fits this batch");
+  }
+  return rc;
 }
 
 int gd_set_rng_stream(gd_ctx *c, int k, int stream) {
@@ -1320,3 +1413,802 @@ extern "C" int gd_eval_energy_noalloc(gd_ctx *c, int ci, int prt_conf, int lig_c
   CK(cudaGetLastError());
   return GD_OK;
 }
+
+/* ======================= surrogate and delayed acceptance ======================= */
+
+struct DaState {
+  gd::Mlp net;
+  gd_sur_params prm{};
+  std::vector<gd::GdGroup> groups;
+  int n_tiles = 0, built_gen = -1;
+  std::vector<void *> allocs;
+  gd::GdGroup *d_groups = nullptr;
+  int *d_rep_cx = nullptr, *d_emb_base = nullptr, *d_active = nullptr;
+  float *d_pocket = nullptr;
+  float *d_mm_prop = nullptr, *d_u1 = nullptr, *d_u2 = nullptr, *d_s_cur = nullptr,
+        *d_s_new = nullptr, *d_pose_mm = nullptr;
+  int *d_pose_rep = nullptr, *d_pose_lc = nullptr, *d_group_cnt = nullptr;
+  gd_energy *d_pose_e = nullptr;
+  GdTileDesc *d_tiles = nullptr;
+  unsigned long long *d_stats = nullptr;
+  double *d_err = nullptr;
+  __nv_bfloat16 *smp_X = nullptr;
+  int *smp_conf = nullptr;
+  float *smp_t = nullptr;
+  long long smp_cap = 0, smp_lo = 0, smp_hi = 0; /* global sample indices written: [lo, hi) */
+  long long norm_hi = -1;                        /* sample set the normalisation was made on */
+  float *d_t = nullptr;
+  double *d_mom = nullptr;
+  float *d_loss_hist = nullptr;
+  int loss_cap = 0;
+  long long train_iter = 0;
+  float *d_pred_mm = nullptr;
+  int pred_cap = 0;
+  float *tr_s = nullptr, *tr_e = nullptr;
+  int *tr_flag = nullptr;
+  int tr_cap = 0, tr_step0 = 0;
+  std::vector<int> active;
+  std::vector<unsigned long long> window0; /* counters at the last controller decision */
+  std::map<long long, cudaGraphExec_t> graphs;
+  int *d_counters = nullptr;
+  int counters_cap = 0;
+};
+
+namespace {
+
+template <class T>
+int da_alloc(DaState *d, T **p, size_t n) {
+  *p = nullptr;
+  void *q = nullptr;
+  cudaError_t e = cudaMalloc(&q, std::max<size_t>(1, n) * sizeof(T));
+  if (e != cudaSuccess)
+    return fail(GD_ERR_NOMEM, "cudaMalloc(%zu) failed: %s", n * sizeof(T), cudaGetErrorString(e));
+  d->allocs.push_back(q);
+  *p = (T *)q;
+  return GD_OK;
+}
+
+void da_free_trace(DaState *d) {
+  if (d->tr_s) cudaFree(d->tr_s);
+  if (d->tr_e) cudaFree(d->tr_e);
+  if (d->tr_flag) cudaFree(d->tr_flag);
+  d->tr_s = d->tr_e = nullptr;
+  d->tr_flag = nullptr;
+  d->tr_cap = 0;
+}
+
+void da_drop_graphs(gd_ctx *c) {
+  if (!c->da) return;
+  for (auto &g : c->da->graphs) cudaGraphExecDestroy(g.second);
+  c->da->graphs.clear();
+}
+
+void da_free(gd_ctx *c) {
+  DaState *d = c->da;
+  if (!d) return;
+  da_drop_graphs(c);
+  gd::mlp_destroy(d->net);
+  for (void *p : d->allocs) cudaFree(p);
+  if (d->d_loss_hist) cudaFree(d->d_loss_hist);
+  if (d->d_pred_mm) cudaFree(d->d_pred_mm);
+  if (d->d_counters) cudaFree(d->d_counters);
+  da_free_trace(d);
+  delete d;
+  c->da = nullptr;
+}
+
+/* groups and their fixed tile positions for the current tile shapes */
+int da_build_groups(gd_ctx *c) {
+  DaState *d = c->da;
+  if (d->built_gen == c->tile_gen && d->d_tiles) return GD_OK;
+  std::vector<gd::GdGroup> g;
+  int tb = 0;
+  for (int ci = 0; ci < c->n_complex; ++ci) {
+    const ComplexInfo &x = c->info[ci];
+    const int block = x.n_tmp * x.n_lig;
+    for (int p = 0; p < x.n_prt; ++p) {
+      gd::GdGroup q;
+      q.ci = ci;
+      q.pc = p;
+      q.b0 = x.rep_offset + p * block;
+      q.n = block;
+      q.k = x.k;
+      q.n_tiles = (block + x.k - 1) / x.k;
+      q.tile_base = tb;
+      q.pad = 0;
+      tb += q.n_tiles;
+      g.push_back(q);
+    }
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  if ((int)g.size() != (int)d->groups.size() || tb > d->n_tiles) {
+    /* sizes only grow with smaller k; reallocate the tile list when needed */
+    if (d->d_tiles) {
+      cudaFree(d->d_tiles);
+      d->allocs.erase(std::remove(d->allocs.begin(), d->allocs.end(), (void *)d->d_tiles),
+                      d->allocs.end());
+      d->d_tiles = nullptr;
+    }
+    int rc = da_alloc(d, &d->d_tiles, tb);
+    if (rc) return rc;
+    if (!d->d_groups) {
+      if ((rc = da_alloc(d, &d->d_groups, g.size()))) return rc;
+      if ((rc = da_alloc(d, &d->d_group_cnt, g.size()))) return rc;
+    }
+  }
+  CK(cudaMemcpy(d->d_groups, g.data(), sizeof(gd::GdGroup) * g.size(), cudaMemcpyHostToDevice));
+  d->groups = g;
+  d->n_tiles = tb;
+  d->built_gen = c->tile_gen;
+  da_drop_graphs(c);
+  return GD_OK;
+}
+
+gd::GdDaDev da_args(gd_ctx *c) {
+  DaState *d = c->da;
+  gd::GdDaDev a;
+  memset(&a, 0, sizeof(a));
+  a.cx = c->d_cx;
+  a.rep_cx = d->d_rep_cx;
+  a.emb_base = d->d_emb_base;
+  a.pocket_feat = d->d_pocket;
+  a.active = d->d_active;
+  a.groups = d->d_groups;
+  a.n_groups = (int)d->groups.size();
+  a.n_rep = c->n_rep;
+  a.replica = c->d_replica;
+  a.mm_old = c->d_mm;
+  a.e_old = c->d_eold;
+  a.etotal = c->d_etotal;
+  a.n_accept = c->d_nacc;
+  a.rec = c->mc.record ? c->d_rec : nullptr;
+  a.rec_next = c->d_rec_next;
+  a.rec_cap = c->rec_cap;
+  a.mm_prop = d->d_mm_prop;
+  a.u1 = d->d_u1;
+  a.u2 = d->d_u2;
+  a.s_cur = d->d_s_cur;
+  a.s_new = d->d_s_new;
+  a.pose_rep = d->d_pose_rep;
+  a.pose_mm = d->d_pose_mm;
+  a.pose_lc = d->d_pose_lc;
+  a.pose_e = d->d_pose_e;
+  a.tiles = d->d_tiles;
+  a.group_cnt = d->d_group_cnt;
+  a.X = d->net.X;
+  a.conf = d->net.conf;
+  a.y = d->net.y;
+  a.mu = d->net.mu;
+  a.sigma = d->net.sigma;
+  a.stats = d->d_stats;
+  a.err = d->d_err;
+  a.smp_X = d->smp_X;
+  a.smp_conf = d->smp_conf;
+  a.smp_t = d->smp_t;
+  a.smp_cap = d->smp_cap;
+  a.tr_s = d->tr_s;
+  a.tr_e = d->tr_e;
+  a.tr_flag = d->tr_flag;
+  a.tr_cap = d->tr_cap;
+  a.tr_step0 = d->tr_step0;
+  a.seed = c->mc.seed;
+  a.move_kind = c->mc.move_kind;
+  for (int i = 0; i < 6; ++i) a.move_scale[i] = c->mc.move_scale[i];
+  a.step_base = c->d_cursor;
+  a.errw = c->d_err;
+  return a;
+}
+
+/* exact energies of the survivors: gd_mc_kernel in pose-evaluation mode over the DA tiles */
+void da_launch_exact(gd_ctx *c, int step, size_t smem, int grid) {
+  DaState *d = c->da;
+  GdMcArgs a = base_args(c);
+  a.mode = 2;
+  a.n_steps = 1;
+  a.rec = nullptr;
+  a.trace_e = nullptr;
+  a.trace_acc = nullptr;
+  a.mm_in = d->d_pose_mm;
+  a.lig_conf_in = d->d_pose_lc;
+  a.e_out = d->d_pose_e;
+  a.tiles = d->d_tiles;
+  a.n_tiles = d->n_tiles;
+  a.tile_counter = d->d_counters + step;
+  mc_kernel(c->unroll)<<<grid, c->threads, smem, c->stream>>>(a, c->fc);
+}
+
+/* the graph of n_steps steps (collect: plain steps that store samples) */
+int da_graph(gd_ctx *c, int n_steps, int exchange, bool collect, cudaGraphExec_t *out) {
+  DaState *d = c->da;
+  const long long key = ((long long)n_steps << 2) | (exchange ? 2 : 0) | (collect ? 1 : 0);
+  auto it = d->graphs.find(key);
+  if (it != d->graphs.end()) {
+    *out = it->second;
+    return GD_OK;
+  }
+  if (n_steps > d->counters_cap) {
+    if (d->d_counters) cudaFree(d->d_counters);
+    d->d_counters = nullptr;
+    d->counters_cap = 0;
+    CK(cudaMalloc(&d->d_counters, sizeof(int) * n_steps));
+    d->counters_cap = n_steps;
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  const size_t smem = smem_bytes(c);
+  int rc = set_kernel_attrs(c, smem);
+  if (rc) return rc;
+  const int grid = grid_for(c, d->n_tiles, smem);
+  const gd::GdDaDev a = da_args(c);
+  const int spe = c->mc.steps_per_exchange;
+  cudaGraph_t graph;
+  CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  cudaMemsetAsync(d->d_counters, 0, sizeof(int) * n_steps, c->stream);
+  if (!collect) {
+    /* surrogate at the current poses under the current network */
+    gd::da_propose(a, 0, true, c->stream);
+    gd::mlp_embed(d->net, c->n_rep, c->stream);
+    gd::mlp_forward(d->net, c->n_rep, c->stream);
+    gd::da_set_current(a, c->stream);
+  }
+  for (int j = 0; j < n_steps; ++j) {
+    gd::da_propose(a, j, false, c->stream);
+    if (!collect) {
+      gd::mlp_embed(d->net, c->n_rep, c->stream);
+      gd::mlp_forward(d->net, c->n_rep, c->stream);
+    }
+    gd::da_stage1(a, j, collect, c->stream);
+    da_launch_exact(c, j, smem, grid);
+    gd::da_stage2(a, j, collect, c->stream);
+    if (exchange && (j + 1) % spe == 0) {
+      const int i = (j + 1) / spe - 1;
+      gd::gd_exchange_kernel<<<(c->n_groups + 127) / 128, 128, 0, c->stream>>>(
+          c->d_cx, c->d_group_base, c->n_complex, c->n_groups, c->d_replica, c->d_etotal,
+          c->d_acs, c->mc.seed, c->d_cursor + 1, i, !(i % 2));
+    }
+  }
+  cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
+  if (ce != cudaSuccess) return fail(GD_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+  cudaGraphExec_t exec;
+  ce = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ce != cudaSuccess) return fail(GD_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ce));
+  d->graphs.emplace(key, exec);
+  *out = exec;
+  return GD_OK;
+}
+
+int da_run_steps(gd_ctx *c, int s1, int n_steps, int exchange, bool collect) {
+  if (!c) return fail(GD_ERR_INVALID, "null context");
+  if (!c->da) return fail(GD_ERR_STATE, "gd_sur_create has not run");
+  if (!c->initialized) return fail(GD_ERR_STATE, "gd_mc_init has not run");
+  const int spe = c->mc.steps_per_exchange;
+  if (n_steps < 1 || (exchange && n_steps % spe))
+    return fail(GD_ERR_INVALID, "n_steps must be >= 1 (a multiple of steps_per_exchange "
+                                "with exchange)");
+  if (s1 < 0) return fail(GD_ERR_INVALID, "s1 must be >= 0");
+  CK(cudaSetDevice(c->device));
+  int rc = da_build_groups(c);
+  if (rc) return rc;
+  cudaGraphExec_t g;
+  if ((rc = da_graph(c, n_steps, exchange, collect, &g))) return rc;
+  CK(cudaStreamSynchronize(c->stream));
+  c->h_cursor[0] = s1;
+  c->h_cursor[1] = c->exchange_calls;
+  CK(cudaMemcpyAsync(c->d_cursor, c->h_cursor, 2 * sizeof(int), cudaMemcpyHostToDevice,
+                     c->stream));
+  CK(cudaGraphLaunch(g, c->stream));
+  if (exchange) c->exchange_calls += n_steps / spe;
+  return GD_OK;
+}
+
+int da_read_stats(gd_ctx *c, std::vector<unsigned long long> &st, std::vector<double> &er) {
+  DaState *d = c->da;
+  st.assign((size_t)c->n_complex * GD_DA_NSTAT, 0);
+  er.assign((size_t)c->n_complex * GD_DA_NERR, 0.0);
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaMemcpy(st.data(), d->d_stats, st.size() * sizeof(unsigned long long),
+                cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(er.data(), d->d_err, er.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  return GD_OK;
+}
+
+int da_upload_active(gd_ctx *c) {
+  DaState *d = c->da;
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaMemcpy(d->d_active, d->active.data(), sizeof(int) * c->n_complex,
+                cudaMemcpyHostToDevice));
+  return GD_OK;
+}
+
+int da_reset_counters(gd_ctx *c) {
+  DaState *d = c->da;
+  CK(cudaMemsetAsync(d->d_stats, 0, sizeof(unsigned long long) * c->n_complex * GD_DA_NSTAT,
+                     c->stream));
+  CK(cudaMemsetAsync(d->d_err, 0, sizeof(double) * c->n_complex * GD_DA_NERR, c->stream));
+  d->window0.assign((size_t)c->n_complex * GD_DA_NSTAT, 0);
+  return GD_OK;
+}
+
+/* target normalisation: mean / std of the samples, then again inside mean +- 4 std */
+int da_normalise(gd_ctx *c, long long start, long long n_valid) {
+  DaState *d = c->da;
+  gd::GdDaDev a = da_args(c);
+  std::vector<double> part(GD_DA_MOM_BLOCKS * 3);
+  double lo = -INFINITY, hi = INFINITY, mean = 0.0, sd = 1.0;
+  for (int pass = 0; pass < 2; ++pass) {
+    gd::da_target_moments(a, start, n_valid, (float)lo, (float)hi, d->d_mom, c->stream);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(c->stream));
+    CK(cudaMemcpy(part.data(), d->d_mom, sizeof(double) * part.size(), cudaMemcpyDeviceToHost));
+    double s0 = 0, s1 = 0, n = 0;
+    for (int b = 0; b < GD_DA_MOM_BLOCKS; ++b) {
+      s0 += part[b * 3];
+      s1 += part[b * 3 + 1];
+      n += part[b * 3 + 2];
+    }
+    if (n < 1) break;
+    mean = s0 / n;
+    sd = std::sqrt(std::max(0.0, s1 / n - mean * mean));
+    lo = mean - 4.0 * sd;
+    hi = mean + 4.0 * sd;
+  }
+  d->net.mu = (float)mean;
+  d->net.sigma = (float)std::max(sd, 1e-3);
+  return GD_OK;
+}
+
+}  // namespace
+
+struct gd_mlp {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  gd::Mlp net;
+  float *d_x = nullptr, *d_t = nullptr;
+  int *d_conf = nullptr;
+  int cap = 0;
+};
+
+namespace {
+
+int mlp_stage_rows(gd_mlp *m, const float *x, const int *conf, int rows) {
+  if (rows > m->cap) {
+    if (m->d_x) cudaFree(m->d_x);
+    if (m->d_t) cudaFree(m->d_t);
+    if (m->d_conf) cudaFree(m->d_conf);
+    m->d_x = m->d_t = nullptr;
+    m->d_conf = nullptr;
+    m->cap = 0;
+    CK(cudaMalloc(&m->d_x, sizeof(float) * GD_MLP_IN * rows));
+    CK(cudaMalloc(&m->d_t, sizeof(float) * rows));
+    CK(cudaMalloc(&m->d_conf, sizeof(int) * rows));
+    m->cap = rows;
+  }
+  if (gd::mlp_reserve(m->net, rows)) return fail(GD_ERR_NOMEM, "network buffers");
+  std::vector<int> cf(rows, -1);
+  if (conf) {
+    for (int i = 0; i < rows; ++i) {
+      if (conf[i] >= m->net.L.n_emb) return fail(GD_ERR_INVALID, "conf %d out of range", conf[i]);
+      cf[i] = m->net.L.n_emb ? conf[i] : -1;
+    }
+  }
+  CK(cudaMemcpyAsync(m->d_x, x, sizeof(float) * GD_MLP_IN * rows, cudaMemcpyHostToDevice,
+                     m->stream));
+  CK(cudaMemcpyAsync(m->d_conf, cf.data(), sizeof(int) * rows, cudaMemcpyHostToDevice,
+                     m->stream));
+  if (gd::mlp_set_rows(m->net, m->d_x, m->d_conf, rows, m->stream))
+    return fail(GD_ERR_CUDA, "row upload failed");
+  if (gd::mlp_embed(m->net, rows, m->stream)) return fail(GD_ERR_CUDA, "embedding failed");
+  CK(cudaStreamSynchronize(m->stream)); /* cf leaves scope */
+  return GD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void gd_sur_default_params(gd_sur_params *p) {
+  if (!p) return;
+  memset(p, 0, sizeof(*p));
+  p->hidden = 256;
+  p->embedding = 1;
+  p->lr = 1e-3f;
+  p->batch = 8192;
+  p->sample_cap = 16LL << 20;
+  p->fallback_accept = 0.1f;
+  p->fallback_window = 20000;
+  p->seed = 7;
+}
+
+int gd_sur_create(gd_ctx *c, const gd_sur_params *p) {
+  if (!c || !p) return fail(GD_ERR_INVALID, "null argument");
+  if (p->hidden < 16 || p->hidden > 1024 || p->hidden % 16)
+    return fail(GD_ERR_INVALID, "hidden must be a multiple of 16 in 16..1024");
+  if (p->batch < 16 || p->sample_cap < 0 || p->lr <= 0.0f)
+    return fail(GD_ERR_INVALID, "bad batch / sample_cap / lr");
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->stream));
+  da_free(c);
+  DaState *d = new DaState();
+  c->da = d;
+  d->prm = *p;
+  int n_emb = 0;
+  std::vector<int> emb_base(c->n_complex), rep_cx(c->n_rep);
+  for (int ci = 0; ci < c->n_complex; ++ci) {
+    const ComplexInfo &x = c->info[ci];
+    emb_base[ci] = n_emb;
+    n_emb += x.n_prt * x.n_lig;
+    for (int r = 0; r < x.n_rep; ++r) rep_cx[x.rep_offset + r] = ci;
+  }
+  int rc = 0;
+#define DA_TRY(x)        \
+  if ((rc = (x))) {      \
+    da_free(c);          \
+    return rc;           \
+  }
+  if (gd::mlp_create(d->net, p->hidden, p->embedding ? n_emb : 0, p->seed, c->stream)) {
+    da_free(c);
+    return fail(GD_ERR_NOMEM, "network allocation failed");
+  }
+  const int rows = std::max(c->n_rep, p->batch);
+  if (gd::mlp_reserve(d->net, rows)) {
+    da_free(c);
+    return fail(GD_ERR_NOMEM, "network work buffers (%d rows)", rows);
+  }
+  if (!p->embedding) std::fill(emb_base.begin(), emb_base.end(), -(1 << 30));
+  /* pocket features: sizes and the pocket centre, scaled to O(1) */
+  std::vector<GdDevComplex> hcx(c->n_complex);
+  CK(cudaMemcpy(hcx.data(), c->d_cx, sizeof(GdDevComplex) * c->n_complex,
+                cudaMemcpyDeviceToHost));
+  std::vector<float> pf((size_t)c->n_complex * GD_MLP_POCKET, 0.0f);
+  for (int ci = 0; ci < c->n_complex; ++ci) {
+    const ComplexInfo &x = c->info[ci];
+    float *f = pf.data() + (size_t)ci * GD_MLP_POCKET;
+    f[0] = x.pnp / 1000.0f;
+    f[1] = x.pnk / 40.0f;
+    f[2] = x.lna / 40.0f;
+    f[3] = x.n_lig / 10.0f;
+    f[4] = x.n_prt / 10.0f;
+    f[5] = x.pos / 8.0f;
+    f[6] = x.n_tmp / 20.0f;
+    f[7] = hcx[ci].pocket[0] / 10.0f;
+    f[8] = hcx[ci].pocket[1] / 10.0f;
+    f[9] = hcx[ci].pocket[2] / 10.0f;
+    f[10] = 1.0f;
+  }
+  const size_t R = c->n_rep;
+  DA_TRY(da_alloc(d, &d->d_rep_cx, R));
+  DA_TRY(da_alloc(d, &d->d_emb_base, c->n_complex));
+  DA_TRY(da_alloc(d, &d->d_active, c->n_complex));
+  DA_TRY(da_alloc(d, &d->d_pocket, pf.size()));
+  DA_TRY(da_alloc(d, &d->d_mm_prop, R * 6));
+  DA_TRY(da_alloc(d, &d->d_u1, R));
+  DA_TRY(da_alloc(d, &d->d_u2, R));
+  DA_TRY(da_alloc(d, &d->d_s_cur, R));
+  DA_TRY(da_alloc(d, &d->d_s_new, R));
+  DA_TRY(da_alloc(d, &d->d_pose_mm, R * 6));
+  DA_TRY(da_alloc(d, &d->d_pose_rep, R));
+  DA_TRY(da_alloc(d, &d->d_pose_lc, R));
+  DA_TRY(da_alloc(d, &d->d_pose_e, R));
+  DA_TRY(da_alloc(d, &d->d_stats, (size_t)c->n_complex * GD_DA_NSTAT));
+  DA_TRY(da_alloc(d, &d->d_err, (size_t)c->n_complex * GD_DA_NERR));
+  DA_TRY(da_alloc(d, &d->d_t, (size_t)rows));
+  DA_TRY(da_alloc(d, &d->d_mom, (size_t)GD_DA_MOM_BLOCKS * 3));
+  d->smp_cap = p->sample_cap;
+  if (d->smp_cap > 0) {
+    DA_TRY(da_alloc(d, &d->smp_X, (size_t)d->smp_cap * GD_MLP_IN));
+    DA_TRY(da_alloc(d, &d->smp_conf, (size_t)d->smp_cap));
+    DA_TRY(da_alloc(d, &d->smp_t, (size_t)d->smp_cap));
+  }
+#undef DA_TRY
+  d->active.assign(c->n_complex, 0); /* off until trained */
+  CK(cudaMemcpy(d->d_rep_cx, rep_cx.data(), sizeof(int) * R, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d->d_emb_base, emb_base.data(), sizeof(int) * c->n_complex,
+                cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d->d_pocket, pf.data(), sizeof(float) * pf.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemset(d->d_s_cur, 0, sizeof(float) * R));
+  CK(cudaMemset(d->d_s_new, 0, sizeof(float) * R));
+  rc = da_upload_active(c);
+  if (!rc) rc = da_reset_counters(c);
+  if (!rc) rc = da_build_groups(c);
+  if (rc) {
+    da_free(c);
+    return rc;
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  return GD_OK;
+}
+
+int gd_sur_collect(gd_ctx *c, int s1, int n_steps, int exchange) {
+  if (!c || !c->da) return fail(GD_ERR_STATE, "gd_sur_create has not run");
+  DaState *d = c->da;
+  if (d->smp_cap <= 0) return fail(GD_ERR_CAPACITY, "sample_cap is 0");
+  const long long g0 = (long long)s1 * c->n_rep;
+  int rc = da_run_steps(c, s1, n_steps, exchange, true);
+  if (rc) return rc;
+  if (d->smp_hi != g0) d->smp_lo = g0; /* not contiguous with the earlier samples */
+  d->smp_hi = g0 + (long long)n_steps * c->n_rep;
+  return GD_OK;
+}
+
+int gd_sur_train(gd_ctx *c, int iterations, float *losses) {
+  if (!c || !c->da) return fail(GD_ERR_STATE, "gd_sur_create has not run");
+  if (iterations < 0) return fail(GD_ERR_INVALID, "iterations < 0");
+  DaState *d = c->da;
+  const long long vlo = std::max(d->smp_lo, d->smp_hi - d->smp_cap);
+  const long long n_valid = d->smp_hi - vlo;
+  if (n_valid <= 0) return fail(GD_ERR_STATE, "no samples (gd_sur_collect)");
+  CK(cudaSetDevice(c->device));
+  const long long start = vlo % d->smp_cap;
+  int rc;
+  if (d->norm_hi != d->smp_hi) {
+    if ((rc = da_normalise(c, start, n_valid))) return rc;
+    d->norm_hi = d->smp_hi;
+  }
+  if (iterations > d->loss_cap) {
+    if (d->d_loss_hist) cudaFree(d->d_loss_hist);
+    d->d_loss_hist = nullptr;
+    d->loss_cap = 0;
+    CK(cudaMalloc(&d->d_loss_hist, sizeof(float) * iterations));
+    d->loss_cap = iterations;
+  }
+  gd::GdDaDev a = da_args(c);
+  const int B = d->prm.batch;
+  for (int it = 0; it < iterations; ++it) {
+    gd::da_gather(a, start, n_valid, B, (int)(d->train_iter++), d->d_t, c->stream);
+    if (gd::mlp_embed(d->net, B, c->stream) || gd::mlp_loss_backward(d->net, B, d->d_t, c->stream))
+      return fail(GD_ERR_CUDA, "training step failed: %s", cudaGetErrorString(cudaGetLastError()));
+    CK(cudaMemcpyAsync(d->d_loss_hist + it, d->net.loss, sizeof(float), cudaMemcpyDeviceToDevice,
+                       c->stream));
+    if (gd::mlp_adam(d->net, d->prm.lr, c->stream))
+      return fail(GD_ERR_CUDA, "Adam step failed");
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaGetLastError());
+  if (losses && iterations)
+    CK(cudaMemcpy(losses, d->d_loss_hist, sizeof(float) * iterations, cudaMemcpyDeviceToHost));
+  /* the new network (and normalisation) replaces the old one in every later graph */
+  da_drop_graphs(c);
+  d->active.assign(c->n_complex, 1);
+  if ((rc = da_upload_active(c))) return rc;
+  return da_reset_counters(c);
+}
+
+int gd_da_run(gd_ctx *c, int s1, int n_steps, int exchange) {
+  int rc = da_run_steps(c, s1, n_steps, exchange, false);
+  if (rc) return rc;
+  DaState *d = c->da;
+  if (d->prm.fallback_accept <= 0.0f) return GD_OK;
+  std::vector<unsigned long long> st;
+  std::vector<double> er;
+  if ((rc = da_read_stats(c, st, er))) return rc;
+  bool changed = false;
+  for (int ci = 0; ci < c->n_complex; ++ci) {
+    if (!d->active[ci]) continue;
+    const unsigned long long *s = st.data() + (size_t)ci * GD_DA_NSTAT;
+    unsigned long long *w = d->window0.data() + (size_t)ci * GD_DA_NSTAT;
+    const unsigned long long passed = s[GD_DA_PASSED] - w[GD_DA_PASSED];
+    if ((long long)passed < std::max(1LL, d->prm.fallback_window)) continue;
+    const double acc = (double)(s[GD_DA_ACCEPTED] - w[GD_DA_ACCEPTED]) / (double)passed;
+    if (acc < d->prm.fallback_accept) {
+      d->active[ci] = 0;
+      changed = true;
+    }
+    for (int k = 0; k < GD_DA_NSTAT; ++k) w[k] = s[k];
+  }
+  if (changed) return da_upload_active(c);
+  return GD_OK;
+}
+
+int gd_sur_get_stats(gd_ctx *c, gd_sur_stats *out) {
+  if (!c || !c->da || !out) return fail(GD_ERR_STATE, "gd_sur_create has not run");
+  std::vector<unsigned long long> st;
+  std::vector<double> er;
+  int rc = da_read_stats(c, st, er);
+  if (rc) return rc;
+  for (int ci = 0; ci < c->n_complex; ++ci) {
+    const unsigned long long *s = st.data() + (size_t)ci * GD_DA_NSTAT;
+    gd_sur_stats &o = out[ci];
+    memset(&o, 0, sizeof(o));
+    o.proposed = (long long)s[GD_DA_PROPOSED];
+    o.passed = (long long)s[GD_DA_PASSED];
+    o.accepted = (long long)s[GD_DA_ACCEPTED];
+    o.plain = (long long)s[GD_DA_PLAIN];
+    o.plain_accepted = (long long)s[GD_DA_PLAIN_ACC];
+    const double n = er[(size_t)ci * GD_DA_NERR + 1];
+    o.n_err = (long long)n;
+    o.rmse = n > 0 ? std::sqrt(er[(size_t)ci * GD_DA_NERR] / n) : 0.0;
+    o.active = c->da->active[ci];
+  }
+  return GD_OK;
+}
+
+int gd_sur_set_active(gd_ctx *c, int ci, int on) {
+  if (!c || !c->da) return fail(GD_ERR_STATE, "gd_sur_create has not run");
+  if (ci < 0 || ci >= c->n_complex) return fail(GD_ERR_INVALID, "bad complex index");
+  c->da->active[ci] = on ? 1 : 0;
+  for (int k = 0; k < GD_DA_NSTAT; ++k) c->da->window0[(size_t)ci * GD_DA_NSTAT + k] = 0;
+  /* restart this complex's controller window from the current counters */
+  std::vector<unsigned long long> st;
+  std::vector<double> er;
+  int rc = da_read_stats(c, st, er);
+  if (rc) return rc;
+  for (int k = 0; k < GD_DA_NSTAT; ++k)
+    c->da->window0[(size_t)ci * GD_DA_NSTAT + k] = st[(size_t)ci * GD_DA_NSTAT + k];
+  return da_upload_active(c);
+}
+
+int gd_sur_predict(gd_ctx *c, int ci, int prt_conf, int lig_conf, const float *mm, int n,
+                   float *energy) {
+  if (!c || !c->da) return fail(GD_ERR_STATE, "gd_sur_create has not run");
+  if (!mm || !energy) return fail(GD_ERR_INVALID, "null argument");
+  if (ci < 0 || ci >= c->n_complex) return fail(GD_ERR_INVALID, "bad complex index");
+  const ComplexInfo &x = c->info[ci];
+  if (prt_conf < 0 || prt_conf >= x.n_prt || lig_conf < 0 || lig_conf >= x.n_lig)
+    return fail(GD_ERR_INVALID, "conformer index out of range");
+  if (n < 1) return GD_OK;
+  DaState *d = c->da;
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->stream));
+  if (gd::mlp_reserve(d->net, n)) return fail(GD_ERR_NOMEM, "network work buffers");
+  if (n > d->pred_cap) {
+    if (d->d_pred_mm) cudaFree(d->d_pred_mm);
+    d->d_pred_mm = nullptr;
+    d->pred_cap = 0;
+    CK(cudaMalloc(&d->d_pred_mm, sizeof(float) * 6 * n));
+    d->pred_cap = n;
+  }
+  /* the work buffers may have moved: graphs that point at them are stale */
+  da_drop_graphs(c);
+  CK(cudaMemcpy(d->d_pred_mm, mm, sizeof(float) * 6 * n, cudaMemcpyHostToDevice));
+  gd::GdDaDev a = da_args(c);
+  gd::da_pose_features(a, ci, prt_conf, lig_conf, d->d_pred_mm, n, c->stream);
+  if (gd::mlp_embed(d->net, n, c->stream) || gd::mlp_forward(d->net, n, c->stream))
+    return fail(GD_ERR_CUDA, "forward failed");
+  CK(cudaStreamSynchronize(c->stream));
+  std::vector<float> y(n);
+  CK(cudaMemcpy(y.data(), d->net.y, sizeof(float) * n, cudaMemcpyDeviceToHost));
+  for (int i = 0; i < n; ++i) energy[i] = fmaf(y[i], d->net.sigma, d->net.mu);
+  return GD_OK;
+}
+
+int gd_sur_info(gd_ctx *c, float *mu, float *sigma, long long *n_samples) {
+  if (!c || !c->da) return fail(GD_ERR_STATE, "gd_sur_create has not run");
+  DaState *d = c->da;
+  if (mu) *mu = d->net.mu;
+  if (sigma) *sigma = d->net.sigma;
+  if (n_samples) *n_samples = d->smp_hi - std::max(d->smp_lo, d->smp_hi - d->smp_cap);
+  return GD_OK;
+}
+
+int gd_da_trace_enable(gd_ctx *c, int step0, int max_steps) {
+  if (!c || !c->da) return fail(GD_ERR_STATE, "gd_sur_create has not run");
+  if (max_steps < 0 || step0 < 0) return fail(GD_ERR_INVALID, "bad argument");
+  DaState *d = c->da;
+  CK(cudaStreamSynchronize(c->stream));
+  da_free_trace(d);
+  da_drop_graphs(c);
+  d->tr_step0 = step0;
+  if (max_steps == 0) return GD_OK;
+  const size_t n = (size_t)c->n_rep * max_steps;
+  CK(cudaMalloc(&d->tr_s, sizeof(float) * n));
+  CK(cudaMalloc(&d->tr_e, sizeof(float) * n));
+  CK(cudaMalloc(&d->tr_flag, sizeof(int) * n));
+  CK(cudaMemset(d->tr_flag, 0xff, sizeof(int) * n));
+  d->tr_cap = max_steps;
+  return GD_OK;
+}
+
+int gd_da_trace_get(gd_ctx *c, float *s_new, float *e_new, int *outcome) {
+  if (!c || !c->da) return fail(GD_ERR_STATE, "gd_sur_create has not run");
+  DaState *d = c->da;
+  if (!d->tr_cap) return fail(GD_ERR_STATE, "trace not enabled");
+  CK(cudaStreamSynchronize(c->stream));
+  const size_t n = (size_t)c->n_rep * d->tr_cap;
+  if (s_new) CK(cudaMemcpy(s_new, d->tr_s, sizeof(float) * n, cudaMemcpyDeviceToHost));
+  if (e_new) CK(cudaMemcpy(e_new, d->tr_e, sizeof(float) * n, cudaMemcpyDeviceToHost));
+  if (outcome) CK(cudaMemcpy(outcome, d->tr_flag, sizeof(int) * n, cudaMemcpyDeviceToHost));
+  return GD_OK;
+}
+
+/* ---- the network alone ---- */
+
+int gd_mlp_create(int device, int hidden, int n_emb, uint64_t seed, gd_mlp **out) {
+  if (!out) return fail(GD_ERR_INVALID, "null argument");
+  *out = nullptr;
+  if (hidden < 16 || hidden > 1024 || hidden % 16 || n_emb < 0)
+    return fail(GD_ERR_INVALID, "hidden must be a multiple of 16 in 16..1024, n_emb >= 0");
+  CK(cudaSetDevice(device));
+  gd_mlp *m = new gd_mlp();
+  m->device = device;
+  cudaError_t e = cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete m;
+    return fail(GD_ERR_CUDA, "stream: %s", cudaGetErrorString(e));
+  }
+  if (gd::mlp_create(m->net, hidden, n_emb, seed, m->stream)) {
+    gd::mlp_destroy(m->net);
+    cudaStreamDestroy(m->stream);
+    delete m;
+    return fail(GD_ERR_NOMEM, "network allocation failed");
+  }
+  *out = m;
+  CK(cudaStreamSynchronize(m->stream));
+  return GD_OK;
+}
+
+int gd_mlp_destroy(gd_mlp *m) {
+  if (!m) return GD_OK;
+  cudaSetDevice(m->device);
+  cudaStreamSynchronize(m->stream);
+  gd::mlp_destroy(m->net);
+  if (m->d_x) cudaFree(m->d_x);
+  if (m->d_t) cudaFree(m->d_t);
+  if (m->d_conf) cudaFree(m->d_conf);
+  cudaStreamDestroy(m->stream);
+  delete m;
+  return GD_OK;
+}
+
+int gd_mlp_num_params(gd_mlp *m, long long *n) {
+  if (!m || !n) return fail(GD_ERR_INVALID, "null argument");
+  *n = (long long)m->net.L.total;
+  return GD_OK;
+}
+
+int gd_mlp_get_params(gd_mlp *m, float *theta, long long n) {
+  if (!m || !theta) return fail(GD_ERR_INVALID, "null argument");
+  if (n != (long long)m->net.L.total) return fail(GD_ERR_INVALID, "parameter count mismatch");
+  CK(cudaSetDevice(m->device));
+  CK(cudaStreamSynchronize(m->stream));
+  CK(cudaMemcpy(theta, m->net.theta, sizeof(float) * n, cudaMemcpyDeviceToHost));
+  return GD_OK;
+}
+
+int gd_mlp_set_params(gd_mlp *m, const float *theta, long long n) {
+  if (!m || !theta) return fail(GD_ERR_INVALID, "null argument");
+  if (n != (long long)m->net.L.total) return fail(GD_ERR_INVALID, "parameter count mismatch");
+  CK(cudaSetDevice(m->device));
+  CK(cudaStreamSynchronize(m->stream));
+  CK(cudaMemcpy(m->net.theta, theta, sizeof(float) * n, cudaMemcpyHostToDevice));
+  if (gd::mlp_refresh_bf16(m->net, m->stream)) return fail(GD_ERR_CUDA, "bf16 refresh failed");
+  CK(cudaStreamSynchronize(m->stream));
+  return GD_OK;
+}
+
+int gd_mlp_forward(gd_mlp *m, const float *x, const int *conf, int rows, float *y) {
+  if (!m || !x || !y || rows < 0) return fail(GD_ERR_INVALID, "bad argument");
+  if (rows == 0) return GD_OK;
+  CK(cudaSetDevice(m->device));
+  int rc = mlp_stage_rows(m, x, conf, rows);
+  if (rc) return rc;
+  if (gd::mlp_forward(m->net, rows, m->stream)) return fail(GD_ERR_CUDA, "forward failed");
+  CK(cudaStreamSynchronize(m->stream));
+  CK(cudaMemcpy(y, m->net.y, sizeof(float) * rows, cudaMemcpyDeviceToHost));
+  return GD_OK;
+}
+
+int gd_mlp_backward(gd_mlp *m, const float *x, const int *conf, const float *t, int rows,
+                    float *loss, float *grad) {
+  if (!m || !x || !t || rows < 1) return fail(GD_ERR_INVALID, "bad argument");
+  CK(cudaSetDevice(m->device));
+  int rc = mlp_stage_rows(m, x, conf, rows);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(m->d_t, t, sizeof(float) * rows, cudaMemcpyHostToDevice, m->stream));
+  if (gd::mlp_loss_backward(m->net, rows, m->d_t, m->stream))
+    return fail(GD_ERR_CUDA, "backward failed");
+  CK(cudaStreamSynchronize(m->stream));
+  if (loss) CK(cudaMemcpy(loss, m->net.loss, sizeof(float), cudaMemcpyDeviceToHost));
+  if (grad)
+    CK(cudaMemcpy(grad, m->net.grad, sizeof(float) * m->net.L.total, cudaMemcpyDeviceToHost));
+  return GD_OK;
+}
+
+int gd_mlp_adam(gd_mlp *m, float lr) {
+  if (!m || !(lr > 0.0f)) return fail(GD_ERR_INVALID, "bad argument");
+  CK(cudaSetDevice(m->device));
+  if (gd::mlp_adam(m->net, lr, m->stream)) return fail(GD_ERR_CUDA, "Adam step failed");
+  CK(cudaStreamSynchronize(m->stream));
+  return GD_OK;
+}
+
+}  // extern "C"

@@ -310,6 +310,12 @@ __global__ void __launch_bounds__(GD_MAX_TPB, GD_MIN_BLOCKS(UNROLL))
     const int t = s_tile;
     if (t >= a.n_tiles || s_abort) break;
     const GdTileDesc tile = a.tiles[t];
+    if (tile.count <= 0) {
+      /* an empty tile (a delayed-acceptance block with fewer survivors than tiles): no copy
+       * issued, nothing to wait for; the barrier keeps s_tile until every thread read it */
+      __syncthreads();
+      continue;
+    }
     const GdDevComplex &cx = a.cx[tile.complex_index];
     const int L = cx.lna, k = tile.count;
     const bool active = tid < k * L;

@@ -1,0 +1,343 @@
+/*
+ * gd_mlp.cu -- forward, backward and Adam kernels of the energy surrogate (gd_mlp.cuh).
+ *
+ * Matrix products run on the tensor cores as BF16 x BF16 -> FP32 warp-level MMA tiles
+ * (16 x 16 x 16 fragments); every product the network needs is one kernel template:
+ *   forward        Z = X W            (A row-major, B row-major)
+ *   weight grad    dW = X^T dZ        (A read transposed from X, reduction over the batch)
+ *   input grad     dX = dZ W^T        (B read transposed from W)
+ * Bias, SiLU and its derivative, the 256 -> 1 output layer, the loss, column sums for the
+ * bias gradients, the embedding gradient (atomic scatter) and Adam are elementwise kernels.
+ * Master parameters, gradients and Adam moments are FP32; W1..W3 are mirrored in BF16 after
+ * every update.
+ */
+#include <mma.h>
+
+#include <cmath>
+
+#include "gd_mlp.cuh"
+#include "gd_numerics.h"
+
+namespace gd {
+
+using bf16 = __nv_bfloat16;
+
+namespace {
+
+__device__ __forceinline__ float silu(float z) { return z / (1.0f + expf(-z)); }
+__device__ __forceinline__ float silu_grad(float z) {
+  const float s = 1.0f / (1.0f + expf(-z));
+  return s * (1.0f + z * (1.0f - s));
+}
+
+/* C[M,N] (fp32, row-major, ldc) = op(A)[M,K] op(B)[K,N]; M, N, K multiples of 16.
+ * A_T: element (m, k) of A is A[k * lda + m]; otherwise A[m * lda + k].
+ * B_T: element (k, n) of B is B[n * ldb + k]; otherwise B[k * ldb + n]. */
+template <bool A_T, bool B_T>
+__global__ void wmma_gemm(const bf16 *__restrict__ A, int lda, const bf16 *__restrict__ B,
+                          int ldb, float *__restrict__ C, int ldc, int M, int N, int K) {
+  using namespace nvcuda;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int tiles_n = N >> 4;
+  const int tm = warp / tiles_n, tn = warp - tm * tiles_n;
+  if (tm * 16 >= M) return;
+  wmma::fragment<wmma::accumulator, 16, 16, 16, float> acc;
+  wmma::fill_fragment(acc, 0.0f);
+  using LA = typename std::conditional<A_T, wmma::col_major, wmma::row_major>::type;
+  using LB = typename std::conditional<B_T, wmma::col_major, wmma::row_major>::type;
+  for (int k = 0; k < K; k += 16) {
+    wmma::fragment<wmma::matrix_a, 16, 16, 16, bf16, LA> a;
+    wmma::fragment<wmma::matrix_b, 16, 16, 16, bf16, LB> b;
+    wmma::load_matrix_sync(a, A_T ? A + (size_t)k * lda + tm * 16 : A + (size_t)tm * 16 * lda + k,
+                           lda);
+    wmma::load_matrix_sync(b, B_T ? B + (size_t)tn * 16 * ldb + k : B + (size_t)k * ldb + tn * 16,
+                           ldb);
+    wmma::mma_sync(acc, a, b, acc);
+  }
+  wmma::store_matrix_sync(C + (size_t)tm * 16 * ldc + tn * 16, acc, ldc, wmma::mem_row_major);
+}
+
+template <bool A_T, bool B_T>
+void gemm(const bf16 *A, int lda, const bf16 *B, int ldb, float *C, int ldc, int M, int N, int K,
+          cudaStream_t s) {
+  const int warps = (M / 16) * (N / 16);
+  wmma_gemm<A_T, B_T><<<(warps + 3) / 4, 128, 0, s>>>(A, lda, B, ldb, C, ldc, M, N, K);
+}
+
+/* Z = C + b (kept for the backward pass when Z != null), A = bf16(SiLU(Z)) */
+__global__ void bias_silu(const float *__restrict__ C, const float *__restrict__ b, float *Z,
+                          bf16 *__restrict__ A, int rows, int n) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (size_t)rows * n) return;
+  const float z = C[i] + b[i % n];
+  if (Z) Z[i] = z;
+  A[i] = __float2bfloat16_rn(silu(z));
+}
+
+/* y[r] = A3[r] . w4 + b4, one warp per row */
+__global__ void out_layer(const bf16 *__restrict__ A3, const float *__restrict__ w4,
+                          const float *__restrict__ b4, float *__restrict__ y, int rows, int h) {
+  const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (r >= rows) return;
+  float s = 0.0f;
+  for (int j = lane; j < h; j += 32) s += __bfloat162float(A3[(size_t)r * h + j]) * w4[j];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if (lane == 0) y[r] = s + b4[0];
+}
+
+/* dy = 2 (y - t) / rows; squared errors to e2 */
+__global__ void mse_grad(const float *__restrict__ y, const float *__restrict__ t,
+                         float *__restrict__ dy, float *__restrict__ e2, int rows) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= rows) return;
+  const float d = y[r] - t[r];
+  dy[r] = 2.0f * d / (float)rows;
+  e2[r] = d * d;
+}
+
+/* deterministic mean of e2 into out[0] (one block) */
+__global__ void mean_reduce(const float *__restrict__ e2, int rows, float *out) {
+  __shared__ double sh[256];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < rows; i += 256) s += e2[i];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[0] = (float)(sh[0] / (double)rows);
+}
+
+/* dZ3 = (dy w4^T) * SiLU'(Z3) -> bf16 */
+__global__ void out_backward(const float *__restrict__ dy, const float *__restrict__ w4,
+                             const float *__restrict__ Z3, bf16 *__restrict__ D, int rows, int h) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (size_t)rows * h) return;
+  const int r = (int)(i / h), j = (int)(i % h);
+  D[i] = __float2bfloat16_rn(dy[r] * w4[j] * silu_grad(Z3[i]));
+}
+
+/* dZ = dX * SiLU'(Z) -> bf16 */
+__global__ void act_backward(const float *__restrict__ dX, const float *__restrict__ Z,
+                             bf16 *__restrict__ D, size_t n) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  D[i] = __float2bfloat16_rn(dX[i] * silu_grad(Z[i]));
+}
+
+/* g[j] += sum_r D[r][j] (bias gradient), one thread per column */
+__global__ void colsum_bf16(const bf16 *__restrict__ D, int rows, int n, float *__restrict__ g) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  float s = 0.0f;
+  for (int r = 0; r < rows; ++r) s += __bfloat162float(D[(size_t)r * n + j]);
+  g[j] += s;
+}
+
+/* dw4[j] = sum_r A3[r][j] dy[r]; db4 = sum_r dy[r] */
+__global__ void out_weight_grad(const bf16 *__restrict__ A3, const float *__restrict__ dy,
+                                int rows, int h, float *__restrict__ gw4,
+                                float *__restrict__ gb4) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j > h) return;
+  float s = 0.0f;
+  if (j < h) {
+    for (int r = 0; r < rows; ++r) s += __bfloat162float(A3[(size_t)r * h + j]) * dy[r];
+    gw4[j] += s;
+  } else {
+    for (int r = 0; r < rows; ++r) s += dy[r];
+    gb4[0] += s;
+  }
+}
+
+/* embedding gradient: columns [7, 39) of dX1 scattered to the rows' conformer entries */
+__global__ void emb_grad(const float *__restrict__ dX, const int *__restrict__ conf, int rows,
+                         float *__restrict__ gemb) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= rows * GD_MLP_EMB) return;
+  const int r = i / GD_MLP_EMB, c = i - r * GD_MLP_EMB;
+  const int e = conf[r];
+  if (e >= 0) atomicAdd(gemb + (size_t)e * GD_MLP_EMB + c, dX[(size_t)r * GD_MLP_IN + GD_MLP_EMB_OFF + c]);
+}
+
+/* embedding columns of X from theta (rows with conf < 0 keep their columns) */
+__global__ void emb_fill(bf16 *__restrict__ X, const float *__restrict__ emb,
+                         const int *__restrict__ conf, int rows) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= rows * GD_MLP_EMB) return;
+  const int r = i / GD_MLP_EMB, c = i - r * GD_MLP_EMB;
+  const int e = conf[r];
+  if (e >= 0)
+    X[(size_t)r * GD_MLP_IN + GD_MLP_EMB_OFF + c] = __float2bfloat16_rn(emb[(size_t)e * GD_MLP_EMB + c]);
+}
+
+__global__ void adam_kernel(float *__restrict__ th, const float *__restrict__ g,
+                            float *__restrict__ m, float *__restrict__ v, size_t n, float lr,
+                            float b1, float b2, float eps, float c1, float c2) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float gi = g[i];
+  const float mi = b1 * m[i] + (1.0f - b1) * gi;
+  const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  th[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+__global__ void to_bf16(const float *__restrict__ a, bf16 *__restrict__ b, size_t n) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) b[i] = __float2bfloat16_rn(a[i]);
+}
+
+/* uniform(-scale, scale) from Philox, keyed by (seed, tensor id) */
+__global__ void init_uniform(float *p, size_t n, float scale, uint32_t tensor, uint64_t seed) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const gd_u32x4 r = gd_philox4x32_10((uint32_t)i, tensor, 0x5EEDu, 7u, (uint32_t)seed,
+                                      (uint32_t)(seed >> 32));
+  p[i] = scale * gd_sym11(r.v[0]);
+}
+
+inline int blocks(size_t n, int t = 256) { return (int)((n + t - 1) / t); }
+
+}  // namespace
+
+int mlp_refresh_bf16(Mlp &n, cudaStream_t s) {
+  const size_t nw = n.L.b4; /* W1..w4 region; biases converted too, unused */
+  to_bf16<<<blocks(nw), 256, 0, s>>>(n.theta, n.wh, nw);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+int mlp_create(Mlp &n, int hidden, int n_emb, uint64_t seed, cudaStream_t s) {
+  if (hidden % 16 || hidden < 16) return -1;
+  n.L.set(hidden, n_emb);
+  const size_t T = n.L.total;
+  if (cudaMalloc(&n.theta, T * 4) || cudaMalloc(&n.grad, T * 4) || cudaMalloc(&n.m, T * 4) ||
+      cudaMalloc(&n.v, T * 4) || cudaMalloc(&n.wh, n.L.b4 * 2) || cudaMalloc(&n.loss, 16))
+    return -3;
+  cudaMemsetAsync(n.theta, 0, T * 4, s);
+  cudaMemsetAsync(n.m, 0, T * 4, s);
+  cudaMemsetAsync(n.v, 0, T * 4, s);
+  const int H = hidden;
+  init_uniform<<<blocks((size_t)GD_MLP_IN * H), 256, 0, s>>>(n.theta + n.L.w1, (size_t)GD_MLP_IN * H,
+                                                             1.0f / sqrtf((float)GD_MLP_IN), 1, seed);
+  init_uniform<<<blocks((size_t)H * H), 256, 0, s>>>(n.theta + n.L.w2, (size_t)H * H,
+                                                     1.0f / sqrtf((float)H), 2, seed);
+  init_uniform<<<blocks((size_t)H * H), 256, 0, s>>>(n.theta + n.L.w3, (size_t)H * H,
+                                                     1.0f / sqrtf((float)H), 3, seed);
+  init_uniform<<<blocks(H), 256, 0, s>>>(n.theta + n.L.w4, H, 1.0f / sqrtf((float)H), 4, seed);
+  if (n_emb)
+    init_uniform<<<blocks((size_t)n_emb * GD_MLP_EMB), 256, 0, s>>>(
+        n.theta + n.L.emb, (size_t)n_emb * GD_MLP_EMB, 0.3f, 5, seed);
+  n.adam_t = 0;
+  return mlp_refresh_bf16(n, s);
+}
+
+void mlp_destroy(Mlp &n) {
+  void *ps[] = {n.theta, n.grad, n.m, n.v, n.wh, n.loss, n.X, n.A1, n.A2, n.A3, n.D,
+                n.Z1, n.Z2, n.Z3, n.C, n.y, n.dy, n.conf};
+  for (void *p : ps)
+    if (p) cudaFree(p);
+  n = Mlp();
+}
+
+int mlp_reserve(Mlp &n, int rows) {
+  rows = (rows + 15) & ~15;
+  if (rows <= n.cap) return 0;
+  void *ps[] = {n.X, n.A1, n.A2, n.A3, n.D, n.Z1, n.Z2, n.Z3, n.C, n.y, n.dy, n.conf};
+  for (void *p : ps)
+    if (p) cudaFree(p);
+  const size_t H = n.L.hidden, R = rows;
+  if (cudaMalloc(&n.X, R * GD_MLP_IN * 2) || cudaMalloc(&n.A1, R * H * 2) ||
+      cudaMalloc(&n.A2, R * H * 2) || cudaMalloc(&n.A3, R * H * 2) ||
+      cudaMalloc(&n.D, R * H * 2) || cudaMalloc(&n.Z1, R * H * 4) ||
+      cudaMalloc(&n.Z2, R * H * 4) || cudaMalloc(&n.Z3, R * H * 4) ||
+      cudaMalloc(&n.C, R * (H > GD_MLP_IN ? H : GD_MLP_IN) * 4) || cudaMalloc(&n.y, R * 4) ||
+      cudaMalloc(&n.dy, R * 4) || cudaMalloc(&n.conf, R * 4))
+    return -3;
+  cudaMemset(n.X, 0, R * GD_MLP_IN * 2);
+  cudaMemset(n.conf, 0xff, R * 4);
+  n.cap = (int)R;
+  return 0;
+}
+
+int mlp_set_rows(Mlp &n, const float *x, const int *conf, int rows, cudaStream_t s) {
+  if (rows > n.cap) return -4;
+  to_bf16<<<blocks((size_t)rows * GD_MLP_IN), 256, 0, s>>>(x, n.X, (size_t)rows * GD_MLP_IN);
+  cudaMemcpyAsync(n.conf, conf, sizeof(int) * rows, cudaMemcpyDeviceToDevice, s);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+int mlp_embed(Mlp &n, int rows, cudaStream_t s) {
+  if (!n.L.n_emb) return 0;
+  emb_fill<<<blocks((size_t)rows * GD_MLP_EMB), 256, 0, s>>>(n.X, n.theta + n.L.emb, n.conf, rows);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+/* forward over `rows` rows of n.X; keeps Z1..Z3 when `keep` for the backward pass */
+static int forward_impl(Mlp &n, int rows, bool keep, cudaStream_t s) {
+  const int M = (rows + 15) & ~15, H = n.L.hidden;
+  if (M > n.cap) return -4;
+  const bf16 *W1 = n.wh + n.L.w1, *W2 = n.wh + n.L.w2, *W3 = n.wh + n.L.w3;
+  gemm<false, false>(n.X, GD_MLP_IN, W1, H, n.C, H, M, H, GD_MLP_IN, s);
+  bias_silu<<<blocks((size_t)M * H), 256, 0, s>>>(n.C, n.theta + n.L.b1, keep ? n.Z1 : nullptr,
+                                                  n.A1, M, H);
+  gemm<false, false>(n.A1, H, W2, H, n.C, H, M, H, H, s);
+  bias_silu<<<blocks((size_t)M * H), 256, 0, s>>>(n.C, n.theta + n.L.b2, keep ? n.Z2 : nullptr,
+                                                  n.A2, M, H);
+  gemm<false, false>(n.A2, H, W3, H, n.C, H, M, H, H, s);
+  bias_silu<<<blocks((size_t)M * H), 256, 0, s>>>(n.C, n.theta + n.L.b3, keep ? n.Z3 : nullptr,
+                                                  n.A3, M, H);
+  out_layer<<<blocks((size_t)rows * 32), 256, 0, s>>>(n.A3, n.theta + n.L.w4, n.theta + n.L.b4,
+                                                      n.y, rows, H);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+int mlp_forward(Mlp &n, int rows, cudaStream_t s) { return forward_impl(n, rows, false, s); }
+
+int mlp_loss_backward(Mlp &n, int rows, const float *t, cudaStream_t s) {
+  const int M = (rows + 15) & ~15, H = n.L.hidden;
+  int rc = forward_impl(n, rows, true, s);
+  if (rc) return rc;
+  cudaMemsetAsync(n.grad, 0, n.L.total * 4, s);
+  /* padded rows (rows..M) carry zero gradient */
+  cudaMemsetAsync(n.dy, 0, (size_t)M * 4, s);
+  mse_grad<<<blocks(rows), 256, 0, s>>>(n.y, t, n.dy, n.C, rows);
+  mean_reduce<<<1, 256, 0, s>>>(n.C, rows, n.loss);
+  /* output layer */
+  out_weight_grad<<<blocks(H + 1), 256, 0, s>>>(n.A3, n.dy, M, H, n.grad + n.L.w4,
+                                                 n.grad + n.L.b4);
+  out_backward<<<blocks((size_t)M * H), 256, 0, s>>>(n.dy, n.theta + n.L.w4, n.Z3, n.D, M, H);
+  /* layer 3: dW3 = A2^T dZ3, db3, dA2 = dZ3 W3^T */
+  gemm<true, false>(n.A2, H, n.D, H, n.grad + n.L.w3, H, H, H, M, s);
+  colsum_bf16<<<blocks(H), 256, 0, s>>>(n.D, M, H, n.grad + n.L.b3);
+  gemm<false, true>(n.D, H, n.wh + n.L.w3, H, n.C, H, M, H, H, s);
+  act_backward<<<blocks((size_t)M * H), 256, 0, s>>>(n.C, n.Z2, n.D, (size_t)M * H);
+  /* layer 2 */
+  gemm<true, false>(n.A1, H, n.D, H, n.grad + n.L.w2, H, H, H, M, s);
+  colsum_bf16<<<blocks(H), 256, 0, s>>>(n.D, M, H, n.grad + n.L.b2);
+  gemm<false, true>(n.D, H, n.wh + n.L.w2, H, n.C, H, M, H, H, s);
+  act_backward<<<blocks((size_t)M * H), 256, 0, s>>>(n.C, n.Z1, n.D, (size_t)M * H);
+  /* layer 1: dW1 = X^T dZ1 (64 x H), db1; dX1 = dZ1 W1^T for the embedding */
+  gemm<true, false>(n.X, GD_MLP_IN, n.D, H, n.grad + n.L.w1, H, GD_MLP_IN, H, M, s);
+  colsum_bf16<<<blocks(H), 256, 0, s>>>(n.D, M, H, n.grad + n.L.b1);
+  if (n.L.n_emb) {
+    gemm<false, true>(n.D, H, n.wh + n.L.w1, H, n.C, GD_MLP_IN, M, GD_MLP_IN, H, s);
+    emb_grad<<<blocks((size_t)rows * GD_MLP_EMB), 256, 0, s>>>(n.C, n.conf, rows,
+                                                             n.grad + n.L.emb);
+  }
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+int mlp_adam(Mlp &n, float lr, cudaStream_t s) {
+  const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+  n.adam_t += 1;
+  const float c1 = 1.0f - powf(b1, (float)n.adam_t), c2 = 1.0f - powf(b2, (float)n.adam_t);
+  adam_kernel<<<blocks(n.L.total), 256, 0, s>>>(n.theta, n.grad, n.m, n.v, n.L.total, lr, b1, b2,
+                                               eps, c1, c2);
+  return mlp_refresh_bf16(n, s);
+}
+
+}  // namespace gd

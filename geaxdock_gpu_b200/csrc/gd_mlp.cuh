@@ -1,0 +1,177 @@
+/*
+ * gd_mlp.cuh -- the energy surrogate: a 64 -> H -> H -> H -> 1 SiLU MLP with a learned
+ * conformer embedding, BF16 weights and activations on the tensor cores, FP32 accumulation,
+ * FP32 master parameters and Adam moments. Internal C++ interface shared by gd_mlp.cu (the
+ * kernels) and gd_capi.cu (delayed acceptance).
+ *
+ * Input row (64 features): [0,3) ligand centre minus pocket centre / 4 A, [3,7) unit
+ * quaternion of the pose rotation (w >= 0), [7,39) conformer embedding (32, learned, one row
+ * per (complex, protein conformer, ligand conformer)), [39,55) pocket features (16), [55,61)
+ * the first two columns of the rotation matrix (a continuous rotation code), [61] distance
+ * to the pocket centre / 8 A, [62,64) zero. The network predicts (E - mu) / sigma; mu, sigma
+ * are set from the training samples.
+ */
+#ifndef GD_MLP_CUH
+#define GD_MLP_CUH
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "gd_device.cuh"
+
+#define GD_MLP_IN 64
+#define GD_MLP_EMB 32
+#define GD_MLP_EMB_OFF 7
+#define GD_MLP_POCKET 16
+#define GD_MLP_POCKET_OFF 39
+
+namespace gd {
+
+struct MlpLayout {
+  int hidden = 256, n_emb = 0;
+  size_t w1, b1, w2, b2, w3, b3, w4, b4, emb, total;
+  void set(int h, int ne) {
+    hidden = h;
+    n_emb = ne;
+    size_t o = 0;
+    w1 = o; o += (size_t)GD_MLP_IN * h;
+    b1 = o; o += h;
+    w2 = o; o += (size_t)h * h;
+    b2 = o; o += h;
+    w3 = o; o += (size_t)h * h;
+    b3 = o; o += h;
+    w4 = o; o += h;
+    b4 = o; o += 4; /* keep the embedding 16-byte aligned */
+    emb = o; o += (size_t)ne * GD_MLP_EMB;
+    total = o;
+  }
+};
+
+/* One network and its training buffers on one device. */
+struct Mlp {
+  MlpLayout L;
+  float *theta = nullptr, *grad = nullptr, *m = nullptr, *v = nullptr; /* [L.total] */
+  __nv_bfloat16 *wh = nullptr;        /* BF16 copies of W1, W2, W3 (same offsets as theta) */
+  float mu = 0.0f, sigma = 1.0f;      /* target normalisation */
+  int adam_t = 0;
+  int cap = 0;                        /* rows of the work buffers */
+  __nv_bfloat16 *X = nullptr, *A1 = nullptr, *A2 = nullptr, *A3 = nullptr, *D = nullptr;
+  float *Z1 = nullptr, *Z2 = nullptr, *Z3 = nullptr, *C = nullptr, *y = nullptr, *dy = nullptr;
+  float *loss = nullptr;              /* [1] */
+  int *conf = nullptr;                /* [cap] embedding row per input row */
+};
+
+int mlp_create(Mlp &n, int hidden, int n_emb, uint64_t seed, cudaStream_t s);
+void mlp_destroy(Mlp &n);
+int mlp_reserve(Mlp &n, int rows);
+/* rows of X (bf16, 64 wide, embedding columns filled by the caller or by mlp_embed) -> y */
+int mlp_forward(Mlp &n, int rows, cudaStream_t s);
+/* rows of X from device FP32 rows (rounded to BF16) and their conformer ids */
+int mlp_set_rows(Mlp &n, const float *x, const int *conf, int rows, cudaStream_t s);
+/* fills the embedding columns of X from theta for the rows' conformer ids (n.conf >= 0) */
+int mlp_embed(Mlp &n, int rows, cudaStream_t s);
+/* forward + MSE loss against t (normalised targets) + backward into n.grad (zeroed first) */
+int mlp_loss_backward(Mlp &n, int rows, const float *t, cudaStream_t s);
+int mlp_adam(Mlp &n, float lr, cudaStream_t s);
+/* BF16 copies of the weight matrices from theta */
+int mlp_refresh_bf16(Mlp &n, cudaStream_t s);
+
+/* ---------------- delayed acceptance (gd_da.cu) ---------------- */
+
+/* One (complex, protein conformer) block of replicas: the unit of survivor compaction. Its
+ * tiles occupy the fixed positions [tile_base, tile_base + n_tiles) of the stage-2 tile list;
+ * tiles past the survivors get count 0. */
+struct GdGroup {
+  int ci, pc, b0, n;          /* complex, protein conformer, first replica, replicas */
+  int tile_base, n_tiles, k, pad;
+};
+
+/* per-complex counters (unsigned long long): */
+#define GD_DA_PROPOSED 0      /* proposals seen with the surrogate stage on */
+#define GD_DA_PASSED 1        /* ... that passed the surrogate stage */
+#define GD_DA_ACCEPTED 2      /* ... that the exact energy then accepted */
+#define GD_DA_PLAIN 3         /* proposals handled as plain Metropolis (stage off) */
+#define GD_DA_PLAIN_ACC 4     /* ... accepted */
+#define GD_DA_NSTAT 8
+/* per-complex double sums: squared surrogate error and its count over exact evaluations */
+#define GD_DA_NERR 2
+
+struct GdDaDev {
+  const GdDevComplex *cx;
+  const int *rep_cx;          /* [n_rep] complex of each replica */
+  const int *emb_base;        /* [n_complex] first embedding row of the complex */
+  const float *pocket_feat;   /* [n_complex*16] */
+  const int *active;          /* [n_complex] 1: surrogate stage on */
+  const GdGroup *groups;
+  int n_groups, n_rep;
+  /* replica state (the plain engine's arrays) */
+  gd_replica *replica;
+  float *mm_old;
+  gd_energy *e_old;
+  float *etotal;
+  int *n_accept;
+  gd_record_step *rec;
+  int *rec_next;
+  int rec_cap;
+  /* per step */
+  float *mm_prop;             /* [n_rep*6] proposed movematrix */
+  float *u2;                  /* [n_rep] final accept uniform (the plain step's) */
+  float *u1;                  /* [n_rep] surrogate-stage uniform */
+  float *s_cur, *s_new;       /* [n_rep] surrogate energy at the current / proposed pose */
+  int *pose_rep;              /* [n_rep] survivors, compacted per group */
+  float *pose_mm;             /* [n_rep*6] */
+  int *pose_lc;               /* [n_rep] */
+  gd_energy *pose_e;          /* [n_rep] exact energies of the survivors */
+  GdTileDesc *tiles;          /* [sum n_tiles] */
+  int *group_cnt;             /* [n_groups] survivors */
+  /* network rows */
+  __nv_bfloat16 *X;           /* [>= n_rep rows * 64] */
+  int *conf;
+  const float *y;
+  float mu, sigma;
+  unsigned long long *stats;  /* [n_complex*GD_DA_NSTAT] */
+  double *err;                /* [n_complex*GD_DA_NERR] */
+  /* training samples (collect mode), ring of smp_cap rows */
+  __nv_bfloat16 *smp_X;
+  int *smp_conf;
+  float *smp_t;
+  long long smp_cap;
+  /* decision trace (replay checks), [n_rep*tr_cap] */
+  float *tr_s, *tr_e;
+  int *tr_flag;
+  int tr_cap, tr_step0;
+  /* proposals */
+  uint64_t seed;
+  int move_kind;
+  float move_scale[6];
+  const int *step_base;       /* device step cursor */
+  unsigned *errw;             /* device error word */
+};
+
+/* proposal (or, with current = true, the current pose) of every replica -> mm_prop, u1, u2,
+ * and its feature row in X / conf */
+void da_propose(const GdDaDev &d, int step0, bool current, cudaStream_t s);
+/* feature rows 0..n-1 of X / conf for n poses of one (complex, protein, ligand conformer) */
+void da_pose_features(const GdDaDev &d, int ci, int pc, int lc, const float *mm, int n,
+                      cudaStream_t s);
+/* s_cur = surrogate of the rows (after a forward over the current poses) */
+void da_set_current(const GdDaDev &d, cudaStream_t s);
+/* surrogate stage and survivor compaction; collect: every proposal passes (plain step) */
+void da_stage1(const GdDaDev &d, int step0, bool collect, cudaStream_t s);
+/* exact stage on the survivors' energies, state update, records, samples when collect */
+void da_stage2(const GdDaDev &d, int step0, bool collect, cudaStream_t s);
+/* training batch: rows drawn from the sample ring into X / conf / t (normalised, clipped) */
+void da_gather(const GdDaDev &d, long long start, long long n_valid, int rows, int iter,
+               float *t, cudaStream_t s);
+/* per-block sum, sum of squares and count of the sample targets inside [lo, hi]:
+ * GD_DA_MOM_BLOCKS x 3 doubles into part (summed on the host in block order) */
+#define GD_DA_MOM_BLOCKS 256
+void da_target_moments(const GdDaDev &d, long long start, long long n_valid, float lo, float hi,
+                       double *part, cudaStream_t s);
+
+}  // namespace gd
+
+#endif

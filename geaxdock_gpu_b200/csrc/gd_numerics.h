@@ -72,9 +72,11 @@ GD_UNROLL
 
 /* Stream purposes (last counter word). */
 #define GD_RNG_MOVE 0u      /* word 0..3: move dims 0..3 */
-#define GD_RNG_MOVE2 1u     /* word 0..1: move dims 4..5, word 2: accept, word 3: spare */
+#define GD_RNG_MOVE2 1u     /* word 0..1: move dims 4..5, word 2: accept, word 3: surrogate
+                               stage of delayed acceptance */
 #define GD_RNG_EXCHANGE 2u  /* word 0: exchange uniform */
 #define GD_RNG_INIT 3u
+#define GD_RNG_TRAIN 4u     /* surrogate training: batch row picks */
 
 /* [0, 1): 24 random bits, exact in float. */
 GD_HD float gd_u01(uint32_t x) { return (float)(x >> 8) * 5.9604644775390625e-08f; }
@@ -187,6 +189,15 @@ GD_HD void gd_draw_step(uint64_t seed, uint32_t stream, uint32_t replica, uint32
   *u_accept = gd_u01(b.v[2]);
 }
 
+/* Uniform of the surrogate (first) stage of a delayed-acceptance step: the spare word of the
+ * proposal's second Philox block, so the move and the final accept uniform stay those of the
+ * plain step. */
+GD_HD float gd_draw_stage1(uint64_t seed, uint32_t stream, uint32_t replica, uint32_t step) {
+  const gd_u32x4 b = gd_philox4x32_10(replica, step, stream, GD_RNG_MOVE2, (uint32_t)seed,
+                                      (uint32_t)(seed >> 32));
+  return gd_u01(b.v[3]);
+}
+
 /* Exchange uniform for (stream, complex-local group p*n_lig + l, exchange call, pair). */
 GD_HD float gd_draw_exchange(uint64_t seed, uint32_t stream, uint32_t group,
                              uint32_t exchange_call, uint32_t pair) {
@@ -227,6 +238,16 @@ GD_HD void gd_place_atom(const float rot[9], float tx, float ty, float tz, float
  * accept iff u < exp((E_new - E_old) * minus_beta). */
 GD_HD int gd_metropolis(float e_new, float e_old, float minus_beta, float u) {
   const float d = GD_MUL(GD_SUB(e_new, e_old), minus_beta);
+  return u < gd_expf(d);
+}
+
+/* Second stage of delayed acceptance (Christen & Fox, J. Comput. Graph. Stat. 14, 2005):
+ * accept iff u < exp(((E_new - E_old) - (S_new - S_old)) * minus_beta), S the surrogate
+ * energy that admitted the proposal in the first stage. With S_new == S_old the difference is
+ * +0 and the decision is bit-identical to gd_metropolis. */
+GD_HD int gd_da_stage2(float e_new, float e_old, float s_new, float s_old, float minus_beta,
+                       float u) {
+  const float d = GD_MUL(GD_SUB(GD_SUB(e_new, e_old), GD_SUB(s_new, s_old)), minus_beta);
   return u < gd_expf(d);
 }
 

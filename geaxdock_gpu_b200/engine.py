@@ -70,11 +70,32 @@ def lib() -> C.CDLL:
         "gd_get_stream": [vp, C.POINTER(vp)],
         "gd_set_rng_stream": [vp, C.c_int, C.c_int],
         "gd_set_wait_timeout": [vp, C.c_longlong],
+        "gd_sur_create": [vp, C.POINTER(abi.SurParams)],
+        "gd_sur_collect": [vp, C.c_int, C.c_int, C.c_int],
+        "gd_sur_train": [vp, C.c_int, fp],
+        "gd_da_run": [vp, C.c_int, C.c_int, C.c_int],
+        "gd_sur_get_stats": [vp, C.POINTER(abi.SurStats)],
+        "gd_sur_set_active": [vp, C.c_int, C.c_int],
+        "gd_sur_predict": [vp, C.c_int, C.c_int, C.c_int, fp, C.c_int, fp],
+        "gd_sur_info": [vp, C.POINTER(C.c_float), C.POINTER(C.c_float),
+                        C.POINTER(C.c_longlong)],
+        "gd_da_trace_enable": [vp, C.c_int, C.c_int],
+        "gd_da_trace_get": [vp, fp, fp, ip],
+        "gd_mlp_create": [C.c_int, C.c_int, C.c_int, C.c_uint64, C.POINTER(vp)],
+        "gd_mlp_destroy": [vp],
+        "gd_mlp_num_params": [vp, C.POINTER(C.c_longlong)],
+        "gd_mlp_get_params": [vp, fp, C.c_longlong],
+        "gd_mlp_set_params": [vp, fp, C.c_longlong],
+        "gd_mlp_forward": [vp, fp, ip, C.c_int, fp],
+        "gd_mlp_backward": [vp, fp, ip, fp, C.c_int, fp, fp],
+        "gd_mlp_adam": [vp, C.c_float],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
         fn.argtypes = args
         fn.restype = C.c_int
+    L.gd_sur_default_params.argtypes = [C.POINTER(abi.SurParams)]
+    L.gd_sur_default_params.restype = None
     L.gd_last_error_string.restype = C.c_char_p
     L.gd_version.restype = C.c_char_p
     _lib = L
@@ -276,3 +297,128 @@ class Engine:
             s1 += spd
         self.steps_total = s1
         return out
+
+
+def sur_default_params(**kw) -> abi.SurParams:
+    p = abi.SurParams()
+    lib().gd_sur_default_params(C.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+class Surrogate:
+    """The learned energy surrogate of an Engine and its delayed-acceptance steps
+    (gd_sur_* / gd_da_* of the C ABI)."""
+
+    def __init__(self, eng: Engine, params: abi.SurParams = None, **kw):
+        self.eng = eng
+        self.params = params if params is not None else sur_default_params(**kw)
+        check(lib().gd_sur_create(eng.h, C.byref(self.params)))
+        self._tr_cap = 0
+
+    def collect(self, s1: int, n_steps: int, exchange: bool = True):
+        check(lib().gd_sur_collect(self.eng.h, s1, n_steps, int(bool(exchange))))
+
+    def train(self, iterations: int) -> np.ndarray:
+        losses = np.zeros(max(1, iterations), np.float32)
+        check(lib().gd_sur_train(self.eng.h, iterations, abi.fptr(losses)))
+        return losses[:iterations]
+
+    def run(self, s1: int, n_steps: int, exchange: bool = True):
+        check(lib().gd_da_run(self.eng.h, s1, n_steps, int(bool(exchange))))
+
+    def stats(self) -> List[Dict]:
+        n = len(self.eng.complexes)
+        arr = (abi.SurStats * n)()
+        check(lib().gd_sur_get_stats(self.eng.h, arr))
+        return [{f: getattr(s, f) for f, _ in abi.SurStats._fields_ if f != "pad"} for s in arr]
+
+    def set_active(self, complex_index: int, active: bool):
+        check(lib().gd_sur_set_active(self.eng.h, complex_index, int(bool(active))))
+
+    def predict(self, complex_index: int, prt_conf: int, lig_conf: int,
+                movematrix: np.ndarray) -> np.ndarray:
+        mm = np.ascontiguousarray(movematrix, np.float32).reshape(-1, 6)
+        out = np.zeros(mm.shape[0], np.float32)
+        check(lib().gd_sur_predict(self.eng.h, complex_index, prt_conf, lig_conf, abi.fptr(mm),
+                                   mm.shape[0], abi.fptr(out)))
+        return out
+
+    def info(self) -> Dict:
+        mu, sg, n = C.c_float(), C.c_float(), C.c_longlong()
+        check(lib().gd_sur_info(self.eng.h, C.byref(mu), C.byref(sg), C.byref(n)))
+        return {"mu": mu.value, "sigma": sg.value, "n_samples": n.value}
+
+    def trace_enable(self, step0: int, max_steps: int):
+        check(lib().gd_da_trace_enable(self.eng.h, step0, max_steps))
+        self._tr_cap = max_steps
+
+    def trace(self):
+        shp = (self.eng.n_rep, self._tr_cap)
+        s = np.zeros(shp, np.float32)
+        e = np.zeros(shp, np.float32)
+        f = np.zeros(shp, np.int32)
+        check(lib().gd_da_trace_get(self.eng.h, abi.fptr(s), abi.fptr(e),
+                                    f.ctypes.data_as(C.POINTER(C.c_int))))
+        return s, e, f
+
+
+class Mlp:
+    """The surrogate network alone (gd_mlp_*): FP32 rows in, FP32 outputs/gradients out."""
+
+    def __init__(self, hidden: int = 256, n_embedding: int = 0, seed: int = 1, device: int = 0):
+        h = C.c_void_p()
+        check(lib().gd_mlp_create(device, hidden, n_embedding, seed, C.byref(h)))
+        self.h = h
+        self.hidden, self.n_embedding = hidden, n_embedding
+        n = C.c_longlong()
+        check(lib().gd_mlp_num_params(self.h, C.byref(n)))
+        self.n_params = n.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().gd_mlp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def params(self) -> np.ndarray:
+        th = np.zeros(self.n_params, np.float32)
+        check(lib().gd_mlp_get_params(self.h, abi.fptr(th), self.n_params))
+        return th
+
+    def set_params(self, th: np.ndarray):
+        th = np.ascontiguousarray(th, np.float32)
+        check(lib().gd_mlp_set_params(self.h, abi.fptr(th), th.size))
+
+    @staticmethod
+    def _rows(x, conf):
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, 64)
+        cp = None
+        if conf is not None:
+            conf = np.ascontiguousarray(conf, np.int32)
+            cp = conf.ctypes.data_as(C.POINTER(C.c_int))
+        return x, conf, cp
+
+    def forward(self, x: np.ndarray, conf: np.ndarray = None) -> np.ndarray:
+        x, conf, cp = self._rows(x, conf)
+        y = np.zeros(x.shape[0], np.float32)
+        check(lib().gd_mlp_forward(self.h, abi.fptr(x), cp, x.shape[0], abi.fptr(y)))
+        return y
+
+    def backward(self, x: np.ndarray, t: np.ndarray, conf: np.ndarray = None):
+        x, conf, cp = self._rows(x, conf)
+        t = np.ascontiguousarray(t, np.float32)
+        loss = np.zeros(1, np.float32)
+        g = np.zeros(self.n_params, np.float32)
+        check(lib().gd_mlp_backward(self.h, abi.fptr(x), cp, abi.fptr(t), x.shape[0],
+                                    abi.fptr(loss), abi.fptr(g)))
+        return float(loss[0]), g
+
+    def adam(self, lr: float = 1e-3):
+        check(lib().gd_mlp_adam(self.h, lr))

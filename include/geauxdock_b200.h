@@ -200,6 +200,12 @@ int gd_replica_offset(const gd_ctx *ctx, int complex_index, int *offset);
 /* Tile of the fused kernel for one complex (-1: all); one CTA size per context. */
 int gd_set_tile(gd_ctx *ctx, int complex_index, const gd_tile *tile);
 int gd_get_tile(const gd_ctx *ctx, int complex_index, gd_tile *tile);
+/* Autotuner: times each candidate tile by evaluating the energies of the replicas' current
+ * poses (the pair loop of gd_mc_run, without touching the chains), `repeats` launches each,
+ * applies the fastest to every complex and returns it with its mean launch time (ms) in
+ * ms_out[i] per candidate (may be null). */
+int gd_autotune(gd_ctx *ctx, const gd_tile *candidates, int n_candidates, int repeats,
+                gd_tile *best, float *ms_out);
 /* RNG stream id of a complex (default: its index in the batch). Draws depend only on
  * (seed, stream, complex-local replica, step), so a complex run alone with the stream id it
  * has in a batch reproduces its batched trajectory. */
@@ -270,6 +276,80 @@ int gd_eval_energy_noalloc(gd_ctx *ctx, int complex_index, int prt_conf, int lig
  * step the proposal's total energy and the accept flag; trace[(r * max_steps) + s]. */
 int gd_trace_enable(gd_ctx *ctx, int max_steps);
 int gd_trace_get(gd_ctx *ctx, float *e_new_total, int *accepted, int *n_steps);
+
+/* ---- learned energy surrogate and delayed acceptance (no reference counterpart) ----
+ *
+ * A 64 -> H -> H -> H -> 1 SiLU MLP of the total energy (pose translation and rotation, a
+ * learned embedding per (complex, protein conformer, ligand conformer), per-pocket features)
+ * with BF16 weights/activations on the tensor cores and FP32 accumulation, FP32 master
+ * weights and Adam. It is the first stage of a delayed-acceptance Metropolis step; the exact
+ * energy judges every surviving proposal with the corrected ratio, so the stationary
+ * distribution is the plain method's. */
+
+typedef struct {
+  int hidden;               /* hidden width, multiple of 16 (default 256) */
+  int embedding;            /* 1: learned conformer embedding (32 wide) */
+  float lr;                 /* Adam learning rate (default 1e-3) */
+  int batch;                /* training rows per Adam step (default 8192) */
+  long long sample_cap;     /* training samples kept (ring; default 16M) */
+  float fallback_accept;    /* a complex whose stage-2 acceptance over the last window falls
+                               below this reverts to plain MC (0: never) */
+  long long fallback_window;/* surviving proposals per complex between decisions */
+  uint64_t seed;            /* weight init and batch draws */
+} gd_sur_params;
+
+/* per-complex counters since gd_sur_create / the last gd_sur_train */
+typedef struct {
+  long long proposed;       /* proposals with the surrogate stage on */
+  long long passed;         /* ... surviving the surrogate stage (exact evaluations) */
+  long long accepted;       /* ... accepted by the exact stage */
+  long long plain;          /* proposals handled as plain Metropolis (stage off) */
+  long long plain_accepted;
+  double rmse;              /* surrogate error against the exact energy over evaluations */
+  long long n_err;
+  int active;               /* surrogate stage currently on */
+  int pad;
+} gd_sur_stats;
+
+void gd_sur_default_params(gd_sur_params *p);
+int gd_sur_create(gd_ctx *ctx, const gd_sur_params *p);
+/* n_steps plain Monte Carlo steps from step s1 (the trajectory of gd_mc_run_fused with the
+ * same arguments), each proposal's features and exact energy appended to the sample ring */
+int gd_sur_collect(gd_ctx *ctx, int s1, int n_steps, int exchange);
+/* iterations Adam steps on batches drawn from the samples; losses[i] (normalised MSE) when
+ * not null; re-activates the surrogate stage of every complex */
+int gd_sur_train(gd_ctx *ctx, int iterations, float *losses);
+/* delayed-acceptance steps (the loop of gd_mc_run_fused, graph-captured); afterwards the
+ * fallback controller switches off the stage of complexes below fallback_accept */
+int gd_da_run(gd_ctx *ctx, int s1, int n_steps, int exchange);
+int gd_sur_get_stats(gd_ctx *ctx, gd_sur_stats *per_complex);
+int gd_sur_set_active(gd_ctx *ctx, int complex_index, int active);
+/* surrogate energies of n poses (movematrix[6] each) of one conformer pair */
+int gd_sur_predict(gd_ctx *ctx, int complex_index, int prt_conf, int lig_conf,
+                   const float *movematrix, int n_poses, float *energy);
+/* normalisation of the targets (E = mu + sigma * network output), valid samples */
+int gd_sur_info(gd_ctx *ctx, float *mu, float *sigma, long long *n_samples);
+/* decision trace of gd_da_run: per replica and step the surrogate energy of the proposal,
+ * its exact energy (NaN when the surrogate stage rejected it) and the outcome
+ * (0 stage-1 reject, 1 stage-2 reject, 2 accept); index r * max_steps + (step - step0) */
+int gd_da_trace_enable(gd_ctx *ctx, int step0, int max_steps);
+int gd_da_trace_get(gd_ctx *ctx, float *s_new, float *e_new, int *outcome);
+
+/* The network alone (gradient checks, offline training). x: rows x 64 features (row-major;
+ * the embedding columns 7..38 are taken from the table for rows with conf >= 0). */
+typedef struct gd_mlp gd_mlp;
+int gd_mlp_create(int device, int hidden, int n_embedding, uint64_t seed, gd_mlp **out);
+int gd_mlp_destroy(gd_mlp *net);
+int gd_mlp_num_params(gd_mlp *net, long long *n);
+/* flat parameter vector: W1 [64][H], b1, W2 [H][H], b2, W3 [H][H], b3, w4 [H], b4 (+3 pad),
+ * embedding [n_embedding][32] */
+int gd_mlp_get_params(gd_mlp *net, float *theta, long long n);
+int gd_mlp_set_params(gd_mlp *net, const float *theta, long long n);
+int gd_mlp_forward(gd_mlp *net, const float *x, const int *conf, int rows, float *y);
+/* forward + mean squared error against t + backward; loss and the gradient (may be null) */
+int gd_mlp_backward(gd_mlp *net, const float *x, const int *conf, const float *t, int rows,
+                    float *loss, float *grad);
+int gd_mlp_adam(gd_mlp *net, float lr);
 
 const char *gd_last_error_string(void);
 const char *gd_version(void);

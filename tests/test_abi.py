@@ -18,7 +18,7 @@ HEADER = os.path.join(ROOT, "include", "geauxdock_b200.h")
 
 def declared_symbols():
     text = open(HEADER).read()
-    return sorted(set(re.findall(r"^(?:int|const char \*)\s*(gd_\w+)\s*\(", text, re.M)))
+    return sorted(set(re.findall(r"^(?:int|void|const char \*)\s*(gd_\w+)\s*\(", text, re.M)))
 
 
 def test_library_exports_every_declared_symbol():

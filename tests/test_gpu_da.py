@@ -1,0 +1,213 @@
+"""Delayed acceptance on the GPU: exactness against the plain Monte Carlo path.
+
+* collect mode (every proposal passes, samples stored) is the plain trajectory, bit for bit;
+* with the surrogate stage switched off, the delayed-acceptance step is the plain step, bit
+  for bit (S_new = S_cur, same proposal and final uniform);
+* with the stage on, every decision is replayed on the CPU from the Philox draws, the traced
+  surrogate energies and the exact energies (checked against the FP64 oracle): stage 1 is
+  u1 < exp(mb (S_new - S_cur)), stage 2 is u2 < exp(mb ((E_new - E_old) - (S_new - S_cur)));
+* per-temperature energy distributions of delayed acceptance and plain Monte Carlo from the
+  same equilibrated start are indistinguishable (two-sample KS, p > 0.01);
+* the fallback controller switches a complex whose stage-2 acceptance is below the threshold
+  back to plain Monte Carlo.
+"""
+import numpy as np
+import pytest
+
+from geaxdock_gpu_b200 import abi, engine, system
+from oracle import pyoracle as po
+from tests.conftest import have_gpu
+from tests.golden.fixtures import load_ref
+from tests.tolerance import scales
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not have_gpu(), reason="needs a B200")]
+
+
+@pytest.fixture(scope="module")
+def raw():
+    z, _, _ = load_ref("1a07C1")
+    return abi.enepara_raw_from_array(z["enepara_raw"])
+
+
+def _small(raw, **kw):
+    w = system.config(0, raw)
+    p = w.params
+    p.steps_per_dump = 400
+    for k, v in kw.items():
+        if k == "move_scale":
+            for i in range(6):
+                p.move_scale[i] = v[i]
+        else:
+            setattr(p, k, v)
+    return w
+
+
+def _same_records(a, b):
+    ra, na = a.records()
+    rb, nb = b.records()
+    assert np.array_equal(na, nb)
+    for r in range(na.size):
+        assert ra[r, :na[r]].tobytes() == rb[r, :nb[r]].tobytes(), r
+
+
+def test_collect_is_the_plain_trajectory(raw):
+    w = _small(raw)
+    cx, ff, params = w.complexes[0], w.ff, w.params
+    with engine.Engine(ff, [cx], params) as a, engine.Engine(ff, [cx], params) as b:
+        a.mc_init()
+        b.mc_init()
+        a.run_fused(0, 60, exchange=True)
+        sur = engine.Surrogate(b, hidden=64, batch=256, sample_cap=1 << 16)
+        sur.collect(0, 60, exchange=True)
+        a.sync()
+        b.sync()
+        assert a.state().tobytes() == b.state().tobytes()
+        _same_records(a, b)
+        assert sur.info()["n_samples"] == 60 * cx.n_rep
+        st = sur.stats()[0]
+        assert st["plain"] == 60 * cx.n_rep and st["proposed"] == 0
+        assert st["plain_accepted"] == int(b.state()["n_accept"].sum())
+
+
+def test_stage_off_is_the_plain_step(raw):
+    w = _small(raw)
+    cx, ff, params = w.complexes[0], w.ff, w.params
+    with engine.Engine(ff, [cx], params) as a, engine.Engine(ff, [cx], params) as b:
+        a.mc_init()
+        b.mc_init()
+        a.run_fused(0, 60, exchange=True)
+        sur = engine.Surrogate(b, hidden=64, batch=256, sample_cap=1 << 16, fallback_accept=0.0)
+        sur.collect(0, 60, exchange=True)
+        sur.train(20)
+        assert sur.stats()[0]["active"] == 1
+        sur.set_active(0, False)
+        a.run_fused(60, 60, exchange=True)
+        sur.run(60, 60, exchange=True)
+        a.sync()
+        b.sync()
+        assert a.state().tobytes() == b.state().tobytes()
+        _same_records(a, b)
+
+
+def _stage1_uniform(seed, stream, replica, step):
+    w = po.philox(int(replica), int(step), int(stream), 1, seed & 0xFFFFFFFF, seed >> 32)[3]
+    return np.float32((w >> 8) * 2.0 ** -24)
+
+
+def test_decisions_replay(raw):
+    scale = (0.6, 0.6, 0.6, 0.3, 0.3, 0.3)  # larger moves: both stages reject
+    w = _small(raw, move_scale=scale)
+    cx, ff, params = w.complexes[0], w.ff, w.params
+    s0, n = 100, 30
+    with engine.Engine(ff, [cx], params) as eng:
+        eng.mc_init()
+        sur = engine.Surrogate(eng, hidden=128, batch=512, sample_cap=1 << 16,
+                               fallback_accept=0.0)
+        sur.collect(0, s0, exchange=True)
+        losses = sur.train(150)
+        assert losses[-1] < losses[0]
+        st0 = eng.state()
+        sur.trace_enable(s0, n)
+        sur.run(s0, n, exchange=False)
+        eng.sync()
+        s_tr, e_tr, f_tr = sur.trace()
+        st1 = eng.state()
+    assert set(np.unique(f_tr)) <= {0, 1, 2}
+    assert (f_tr == 0).any() and (f_tr == 1).any() and (f_tr == 2).any()
+    refmap = po.ref_map(ff, cx)
+    mm = st0["movematrix_old"].copy()
+    e_old = st0["energy_old"]["e"][:, 9].copy()
+    s_cur = np.full(cx.n_rep, np.nan, np.float32)  # known once a replica accepted a move
+    idx_tmp = st0["replica"]["idx_tmp"]
+    mbs = np.asarray(cx.temp["minus_beta"], np.float32)
+    checked_e = 0
+    worst = np.zeros(10)
+    for k in range(n):
+        step = s0 + k
+        reps = np.arange(cx.n_rep, dtype=np.uint32)
+        delta, u2 = po.draw_steps(params.seed, params.move_kind, list(params.move_scale), reps,
+                                  np.full(cx.n_rep, step, np.uint32))
+        for r in range(cx.n_rep):
+            mb = mbs[idx_tmp[r]]
+            mmn = (mm[r] + delta[r]).astype(np.float32)
+            f = f_tr[r, k]
+            sn = s_tr[r, k]
+            if not np.isnan(s_cur[r]):
+                u1 = _stage1_uniform(params.seed, 0, r, step)
+                d1 = np.float32(np.float32(sn - s_cur[r]) * mb)
+                assert (f > 0) == bool(u1 < po.expf(d1)), (r, k)
+            if f == 0:
+                assert np.isnan(e_tr[r, k])
+                continue
+            en = np.float32(e_tr[r, k])
+            if r % 9 == 0:
+                p, l = r // (cx.n_tmp * cx.n_lig), r % cx.n_lig
+                o = po.pose_energy(ff, cx, int(p), int(l), mmn, refmap, 64)
+                worst[9] = max(worst[9], abs(float(en) - o["e"][9]) / scales(o, ff)[9])
+                checked_e += 1
+            sc = s_cur[r] if not np.isnan(s_cur[r]) else sn
+            d2 = np.float32(np.float32(np.float32(en - e_old[r]) - np.float32(sn - sc)) * mb)
+            acc = bool(u2[r] < po.expf(d2))
+            if not np.isnan(s_cur[r]):
+                assert acc == (f == 2), (r, k)
+            if f == 2:
+                mm[r] = mmn
+                e_old[r] = en
+                s_cur[r] = sn
+    assert checked_e > 20
+    assert worst[9] < 1e-5, worst[9]
+    assert np.array_equal(st1["movematrix_old"].view(np.uint32), mm.view(np.uint32))
+    assert np.array_equal(st1["energy_old"]["e"][:, 9], e_old)
+    assert np.array_equal(st1["n_accept"] - st0["n_accept"], (f_tr == 2).sum(axis=1))
+
+
+def test_energy_distributions_match_plain(raw):
+    """Config-1 system, configured moves: 2,000 plain burn-in steps (the surrogate's training
+    samples), then plain and delayed-acceptance runs of 1,000 steps each from the same state.
+    The 341 (protein, ligand conformer) chains at one temperature are independent, so the
+    final snapshot gives independent samples per temperature."""
+    from scipy import stats
+    w = system.config(1, raw)
+    cx, ff, params = w.complexes[0], w.ff, w.params
+    params.record = 0
+    burn, span = 2000, 1000
+    with engine.Engine(ff, [cx], params) as a, engine.Engine(ff, [cx], params) as b:
+        b.mc_init()
+        sur = engine.Surrogate(b, sample_cap=16 << 20, fallback_accept=0.0)
+        sur.collect(0, burn, exchange=True)
+        losses = sur.train(1000)
+        assert losses[-50:].mean() < 0.05 * losses[:10].mean()
+        b.sync()
+        a.mc_init()
+        a.set_state(b.state())
+        a.run_fused(burn, span, exchange=True)
+        sur.run(burn, span, exchange=True)
+        sa, sb = a.state(), b.state()
+        st = sur.stats()[0]
+    assert st["proposed"] == span * cx.n_rep and st["active"] == 1
+    assert st["rmse"] < 0.5
+    ea, eb = sa["energy_old"]["e"][:, 9], sb["energy_old"]["e"][:, 9]
+    ta, tb = sa["replica"]["idx_tmp"], sb["replica"]["idx_tmp"]
+    for t in range(cx.n_tmp):
+        p = stats.ks_2samp(ea[ta == t], eb[tb == t]).pvalue
+        assert p > 0.01, (t, p)
+
+
+def test_fallback_to_plain(raw):
+    w = _small(raw)
+    cx, ff, params = w.complexes[0], w.ff, w.params
+    with engine.Engine(ff, [cx], params) as eng:
+        eng.mc_init()
+        sur = engine.Surrogate(eng, hidden=32, batch=64, sample_cap=1 << 14,
+                               fallback_accept=0.999, fallback_window=500)
+        sur.collect(0, 20, exchange=True)
+        sur.train(1)  # barely trained: stage-2 acceptance below 0.999
+        sur.run(20, 20, exchange=True)
+        st = sur.stats()[0]
+        assert st["active"] == 0
+        assert st["proposed"] == 20 * cx.n_rep
+        sur.run(40, 20, exchange=True)
+        st2 = sur.stats()[0]
+        assert st2["proposed"] == st["proposed"]
+        assert st2["plain"] == st["plain"] + 20 * cx.n_rep
+        assert st["rmse"] > 0 and st["n_err"] == st["passed"]

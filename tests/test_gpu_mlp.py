@@ -1,0 +1,77 @@
+"""Surrogate network on the GPU (BF16 tensor-core GEMMs, FP32 accumulation) against the FP64
+CPU oracle that rounds the same values to BF16: forward, gradient, Adam, and training."""
+import numpy as np
+import pytest
+
+from oracle import mlp as mo
+from tests.conftest import have_gpu
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not have_gpu(), reason="needs a B200")]
+
+
+def _setup(hidden=64, n_emb=5, rows=40, seed=3):
+    from geaxdock_gpu_b200 import engine
+    net = engine.Mlp(hidden=hidden, n_embedding=n_emb, seed=seed)
+    rng = np.random.default_rng(seed)
+    x = rng.normal(0, 1, (rows, 64)).astype(np.float32)
+    conf = rng.integers(-1, n_emb, rows).astype(np.int32)
+    t = rng.normal(0, 1, rows).astype(np.float32)
+    orc = mo.MlpOracle(net.params(), hidden, n_emb, bf16_mode=True)
+    return net, orc, x, conf, t
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(np.asarray(a, np.float64) - b) / max(np.linalg.norm(b), 1e-30))
+
+
+def test_forward_matches_oracle():
+    net, orc, x, conf, t = _setup()
+    y = net.forward(x, conf)
+    yo = orc.forward(x, conf)
+    # FP32 accumulation vs FP64, BF16 rounding boundaries: 1e-2 of the output scale
+    assert np.max(np.abs(y - yo)) <= 1e-2 * max(1.0, np.max(np.abs(yo))), np.max(np.abs(y - yo))
+    y64 = mo.MlpOracle(net.params(), 64, 5, bf16_mode=False).forward(x, conf)
+    assert _rel(y, y64) < 0.05  # what BF16 costs against the exact network
+
+
+@pytest.mark.parametrize("hidden,rows", [(64, 40), (256, 333)])
+def test_gradient_matches_oracle(hidden, rows):
+    net, orc, x, conf, t = _setup(hidden=hidden, rows=rows)
+    loss, g = net.backward(x, t, conf)
+    lo, go = orc.backward(x, t, conf)
+    assert abs(loss - lo) <= 1e-3 * max(1.0, lo)
+    for name in ("w1", "b1", "w2", "b2", "w3", "b3", "w4", "emb"):
+        off, size = orc.L[name]
+        r = _rel(g[off:off + size], go[off:off + size])
+        assert r < 2e-2, (name, r)
+    off, _ = orc.L["b4"]
+    assert abs(g[off] - go[off]) <= 1e-4 * max(1.0, abs(go[off]))
+
+
+def test_adam_step_matches_oracle():
+    net, orc, x, conf, t = _setup()
+    th0 = net.params().astype(np.float64)
+    _, g = net.backward(x, t, conf)
+    net.adam(1e-3)
+    th1 = net.params()
+    m = np.zeros_like(th0)
+    v = np.zeros_like(th0)
+    ref = th0.copy()
+    mo.MlpOracle.adam(ref, g.astype(np.float64), m, v, 1, 1e-3)
+    assert np.max(np.abs(th1 - ref)) <= 2e-6
+
+
+def test_training_reduces_loss():
+    from geaxdock_gpu_b200 import engine
+    net = engine.Mlp(hidden=128, n_embedding=4, seed=11)
+    rng = np.random.default_rng(5)
+    x = rng.normal(0, 1, (2048, 64)).astype(np.float32)
+    x[:, 7:39] = 0.0
+    conf = rng.integers(0, 4, 2048).astype(np.int32)
+    t = (np.sin(x[:, 0]) + 0.5 * x[:, 1] * x[:, 2] + 0.3 * conf).astype(np.float32)
+    first = net.backward(x, t, conf)[0]
+    for _ in range(300):
+        net.backward(x, t, conf)
+        net.adam(3e-3)
+    last = net.backward(x, t, conf)[0]
+    assert last < 0.1 * first, (first, last)

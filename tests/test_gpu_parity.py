@@ -283,3 +283,26 @@ def test_bounded_wait_times_out_without_fault(raw):
         eng.mc_run(0, 0)
         eng.sync()
         assert np.all(np.isfinite(eng.etotal()))
+
+
+def test_autotune_picks_a_tile_and_keeps_the_chains(raw, tmp_path):
+    from geaxdock_gpu_b200 import autotune
+    w = system.config(0, raw)
+    cx, ff = w.complexes[0], w.ff
+    with engine.Engine(ff, [cx], w.params) as eng:
+        eng.mc_init()
+        eng.mc_run(0, 0)
+        eng.sync()
+        before = eng.state()
+        res = autotune.tune(eng, cache_path=str(tmp_path / "cache.json"), repeats=1)
+        assert not res["cached"]
+        k, ch, u = eng.tile()
+        assert [k, ch, u] == res["tile"]
+        assert all(m > 0 or m == -1 for m in res["ms"].values())
+        after = eng.state()
+        assert np.array_equal(before.view(np.uint8), after.view(np.uint8))
+        # the chains continue under the new tile exactly as a fresh run would
+        eng.mc_run(0, 10)
+        eng.sync()
+        again = autotune.tune(eng, cache_path=str(tmp_path / "cache.json"))
+        assert again["cached"] and again["tile"] == res["tile"]
