@@ -253,9 +253,8 @@ def run_ours(args, rank, world, local_rank):
     mc_ms = [a.elapsed_time(b) for a, b, c in evs]
     tot_ms = sum(step_ms)
     if dist:
-        t = torch.tensor([tot_ms], dtype=torch.float64, device="cuda:%d" % dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tot_ms = float(t.item())
+        from geaxdock_gpu_b200.shard import max_over_ranks
+        tot_ms = max_over_ranks(tot_ms, dist)
     rs_per_step = cx.n_rep * spe
     value = world * rs_per_step * args.steps / (tot_ms * 1e-3)
     flops_rs = algorithmic_flops_per_replica_step(eng, w) if rank == 0 else 0.0

@@ -1,0 +1,91 @@
+"""Replica shards on two ranks (gloo, CPU): the partition is agreed by every rank, covers each
+complex exactly once with its batch index as RNG stream id, splits by whole exchange groups,
+and the timing reduction is the max over ranks."""
+import os
+import socket
+
+import pytest
+import torch.multiprocessing as mp
+
+from geaxdock_gpu_b200 import shard
+
+
+def test_assign_complexes_balances_and_covers():
+    costs = [50, 10, 40, 30, 20, 60, 5]
+    parts = shard.assign_complexes(costs, 3)
+    flat = sorted(i for p in parts for i in p)
+    assert flat == list(range(len(costs)))
+    loads = [sum(costs[i] for i in p) for p in parts]
+    assert max(loads) - min(loads) <= max(costs)
+    assert shard.assign_complexes(costs, 3) == parts  # deterministic
+
+
+def test_protein_conformer_split_is_group_aligned():
+    for n_prt in (1, 4, 11):
+        for world in (1, 2, 3, 8):
+            cuts = [shard.split_protein_conformers(n_prt, world, r) for r in range(world)]
+            assert cuts[0][0] == 0 and cuts[-1][1] == n_prt
+            for (a0, a1), (b0, b1) in zip(cuts, cuts[1:]):
+                assert a1 == b0 and a0 <= a1
+            sizes = [b - a for a, b in cuts]
+            assert max(sizes) - min(sizes) <= 1
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _worker(rank, world, port, costs, q):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    import datetime
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        parts = shard.assign_complexes(costs, world)
+        mine = parts[rank]
+        gathered = [None] * world
+        dist.all_gather_object(gathered, mine)
+        t = shard.max_over_ranks(1.5 + rank, dist)
+        q.put((rank, mine, gathered, t))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_agree_on_shards_and_max_time():
+    costs = [7, 3, 9, 1, 4, 4, 8]
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, world, port, costs, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = [q.get(timeout=120) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    out.sort()
+    all_idx = sorted(i for _, mine, _, _ in out for i in mine)
+    assert all_idx == list(range(len(costs)))
+    for rank, mine, gathered, t in out:
+        assert gathered == [o[1] for o in out]
+        assert t == 1.5 + (world - 1)
+
+
+def test_shard_batch_keeps_batch_index_as_stream():
+    class Cx:
+        def __init__(self, n_rep, lna, pnp):
+            self.n_rep, self.lna, self.pnp = n_rep, lna, pnp
+    batch = [Cx(512, 10 + i, 1200 + 100 * i) for i in range(6)]
+    seen = []
+    for rank in range(2):
+        cxs, streams = shard.shard_batch(batch, 2, rank)
+        assert [batch[s] for s in streams] == cxs
+        seen += streams
+    assert sorted(seen) == list(range(6))
