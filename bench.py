@@ -17,6 +17,10 @@ reference: the reference's path restated on the host cores (the reference's own 
            a bounded sample per step, all host threads, same metric.
 Multi-GPU (torchrun): every rank runs its own config-1 system (own RNG stream), no data-path
 collective (replicas shard without exchange across shards): weak scaling.
+delayed_acceptance (N = 1): the config-3 workload on the config-1 system (2,000 burn-in steps of
+           training samples, one epoch of Adam, then K intervals of delayed-acceptance and of
+           plain steps from the same state, device-timed), at the configured moves and at 20x
+           larger moves; surrogate RMSE, stage acceptances, per-temperature KS p-values.
 """
 from __future__ import annotations
 
@@ -34,7 +38,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "MC replica-steps/s (plain batched REMC)"
+METRIC = "MC replica-steps/s (plain batched REMC; delayed acceptance under delayed_acceptance)"
 UNIT = "replica-steps/s"
 
 
@@ -158,7 +162,7 @@ def run_reference(args, rank, world):
     t0 = time.perf_counter()
     mc.run_range(0, nt, 0, 0, 1, nt)
     per_batch = max(time.perf_counter() - t0, 1e-3)  # one step of nt replicas
-    n_rep = int(min(cx.n_rep, max(nt, nt * int(2.0 / (10 * per_batch)))))
+    n_rep = int(min(cx.n_rep, max(nt, nt * int(0.8 / (10 * per_batch)))))
     s2 = 0
     for _ in range(args.warmup):
         mc.run_range(0, n_rep, 0, s2, 10, nt)
@@ -183,6 +187,94 @@ def run_reference(args, rank, world):
            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
+
+
+def delayed_acceptance(w, dev, tile, scale_mult, intervals, burn=2000, iters=1665):
+    """Config-3 workload: the config-1 system, 2,000 plain burn-in steps whose proposals train
+    the surrogate (13.64 M samples), one epoch of Adam (batch 8,192, lr 1e-3), then `intervals`
+    exchange intervals of delayed-acceptance steps and, from the same state, of plain steps,
+    alternately, each bracketed by CUDA events on its engine's stream (L2 flushed between).
+    Per-temperature KS test on the final states of the two runs."""
+    import ctypes as C
+    import torch
+    from scipy import stats
+    from geaxdock_gpu_b200 import engine
+    cx, ff = w.complexes[0], w.ff
+    p = type(w.params).from_buffer_copy(w.params)
+    p.record = 0
+    for i in range(6):
+        p.move_scale[i] = w.params.move_scale[i] * scale_mult
+    spe = p.steps_per_exchange
+    with engine.Engine(ff, [cx], p, device=dev) as b, engine.Engine(ff, [cx], p, device=dev) as a:
+        b.set_tile(*tile)
+        a.set_tile(*tile)
+        b.mc_init()
+        sur = engine.Surrogate(b)
+        t0 = time.perf_counter()
+        sur.collect(0, burn, exchange=True)
+        b.sync()
+        collect_s = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        losses = sur.train(iters)
+        train_s = time.perf_counter() - t0
+        info = sur.info()
+        a.mc_init()
+        a.set_state(b.state())
+        a.sync()
+        sa = torch.cuda.ExternalStream(a.cuda_stream(), device=dev)
+        sb = torch.cuda.ExternalStream(b.cuda_stream(), device=dev)
+        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda:%d" % dev)
+        s = burn
+        a.run_fused(s, spe, exchange=True)  # graph capture + warm-up
+        sur.run(s, spe, exchange=True)
+        a.sync()
+        b.sync()
+        s += spe
+        ev = []
+        for _ in range(intervals):
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+            e[0].record(sa)
+            a.run_fused(s, spe, exchange=True)
+            e[1].record(sa)
+            with torch.cuda.stream(sa):
+                flush.add_(1.0)
+            a.sync()
+            e[2].record(sb)
+            sur.run(s, spe, exchange=True)
+            e[3].record(sb)
+            with torch.cuda.stream(sb):
+                flush.add_(1.0)
+            b.sync()
+            ev.append(e)
+            s += spe
+        torch.cuda.synchronize(dev)
+        plain_ms = sum(x[0].elapsed_time(x[1]) for x in ev)
+        da_ms = sum(x[2].elapsed_time(x[3]) for x in ev)
+        st = sur.stats()[0]
+        fa, fb = a.state(), b.state()
+        del flush
+    ea, eb = fa["energy_old"]["e"][:, 9], fb["energy_old"]["e"][:, 9]
+    ta, tb = fa["replica"]["idx_tmp"], fb["replica"]["idx_tmp"]
+    ks = [float(stats.ks_2samp(ea[ta == t], eb[tb == t]).pvalue) for t in range(cx.n_tmp)]
+    rs = cx.n_rep * spe * intervals
+    passed = max(1, st["passed"])
+    return {"metric": "MC replica-steps/s (surrogate delayed acceptance)",
+            "value": rs / (da_ms * 1e-3), "unit": UNIT,
+            "plain_same_state": rs / (plain_ms * 1e-3),
+            "speedup_vs_plain": plain_ms / da_ms,
+            "move_scale": [p.move_scale[i] for i in range(6)],
+            "stage1_pass": st["passed"] / max(1, st["proposed"]),
+            "stage2_accept": st["accepted"] / passed,
+            "accept": st["accepted"] / max(1, st["proposed"]),
+            "surrogate_rmse": st["rmse"], "target_mu_sigma": [info["mu"], info["sigma"]],
+            "surrogate_active": st["active"],
+            "ks_min_p": min(ks), "ks_p_per_temperature": ks,
+            "collect_steps": burn, "collect_s": collect_s, "samples": info["n_samples"],
+            "train_iterations": iters, "train_batch": 8192, "train_s": train_s,
+            "train_loss_first_last": [float(losses[0]), float(losses[-1])],
+            "intervals": intervals, "ms_per_interval": da_ms / intervals,
+            "gpu_launches_per_interval": 3 + 5 * spe + 1,
+            "timing": "CUDA events on each engine's stream, L2 flushed between intervals"}
 
 
 def run_ours(args, rank, world, local_rank):
@@ -322,6 +414,11 @@ def run_ours(args, rank, world, local_rank):
                "scope": "gd_create + gd_mc_init + K x (gd_mc_run + gd_exchange + gd_get_etotal)"
                         " + gd_get_records_raw + gd_destroy, host wall clock"}
 
+    da = None
+    if world == 1 and not args.no_da:
+        da = {"configured_moves": delayed_acceptance(w, dev, tile_used, 1.0, args.steps),
+              "moves_x20": delayed_acceptance(w, dev, tile_used, 20.0, args.steps)}
+
     cpu = None
     if world == 1 and not args.no_cpu:
         cpu = cpu_baseline_sample(w)
@@ -338,7 +435,8 @@ def run_ours(args, rank, world, local_rank):
                                "unroll": tile_used[2], "source": tile_source},
                       "parallelism": "replica shards, no collective" if world > 1 else "1 GPU"},
            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
-           "gpu_launches": 2 * args.steps + args.steps // max(1, intervals_per_dump)}
+           "gpu_launches": 2 * args.steps + args.steps // max(1, intervals_per_dump),
+           "delayed_acceptance": da}
     print(json.dumps(out), flush=True)
 
 
@@ -350,6 +448,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-da", action="store_true", help="skip the delayed-acceptance runs")
     ap.add_argument("--tile", default="", help="replicas_per_cta,chunk_points[,unroll] (default: tuned)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))

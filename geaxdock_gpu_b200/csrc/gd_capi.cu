@@ -1646,16 +1646,12 @@ int da_graph(gd_ctx *c, int n_steps, int exchange, bool collect, cudaGraphExec_t
   if (!collect) {
     /* surrogate at the current poses under the current network */
     gd::da_propose(a, 0, true, c->stream);
-    gd::mlp_embed(d->net, c->n_rep, c->stream);
     gd::mlp_forward(d->net, c->n_rep, c->stream);
     gd::da_set_current(a, c->stream);
   }
   for (int j = 0; j < n_steps; ++j) {
     gd::da_propose(a, j, false, c->stream);
-    if (!collect) {
-      gd::mlp_embed(d->net, c->n_rep, c->stream);
-      gd::mlp_forward(d->net, c->n_rep, c->stream);
-    }
+    if (!collect) gd::mlp_forward(d->net, c->n_rep, c->stream);
     gd::da_stage1(a, j, collect, c->stream);
     da_launch_exact(c, j, smem, grid);
     gd::da_stage2(a, j, collect, c->stream);
@@ -2062,7 +2058,7 @@ int gd_sur_predict(gd_ctx *c, int ci, int prt_conf, int lig_conf, const float *m
   CK(cudaMemcpy(d->d_pred_mm, mm, sizeof(float) * 6 * n, cudaMemcpyHostToDevice));
   gd::GdDaDev a = da_args(c);
   gd::da_pose_features(a, ci, prt_conf, lig_conf, d->d_pred_mm, n, c->stream);
-  if (gd::mlp_embed(d->net, n, c->stream) || gd::mlp_forward(d->net, n, c->stream))
+  if (gd::mlp_forward(d->net, n, c->stream))
     return fail(GD_ERR_CUDA, "forward failed");
   CK(cudaStreamSynchronize(c->stream));
   std::vector<float> y(n);

@@ -127,29 +127,70 @@ __global__ void act_backward(const float *__restrict__ dX, const float *__restri
   D[i] = __float2bfloat16_rn(dX[i] * silu_grad(Z[i]));
 }
 
-/* g[j] += sum_r D[r][j] (bias gradient), one thread per column */
-__global__ void colsum_bf16(const bf16 *__restrict__ D, int rows, int n, float *__restrict__ g) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= n) return;
+/* Reductions over the batch are split into chunks of SPLIT_ROWS rows: each chunk writes a
+ * partial result, reduce_partials adds the chunks in a fixed order (deterministic). */
+constexpr int SPLIT_ROWS = 256;
+
+/* partial column sums of a [rows][n] BF16 matrix, optionally weighted per row by w; with
+ * w != null an extra column n holds sum_r w[r]. Block: 32 columns x 8 row lanes; grid
+ * (columns / 32, chunks). part[chunk][ncol], ncol = n + (w != null). */
+__global__ void __launch_bounds__(256) colsum_split(const bf16 *__restrict__ A, const float *__restrict__ w,
+                                                    int rows, int n, float *__restrict__ part) {
+  __shared__ float sh[8][33];
+  const int cx = threadIdx.x & 31, ry = threadIdx.x >> 5;
+  const int col = blockIdx.x * 32 + cx, chunk = blockIdx.y;
+  const int ncol = n + (w ? 1 : 0);
+  const int r0 = chunk * SPLIT_ROWS, r1 = min(rows, r0 + SPLIT_ROWS);
   float s = 0.0f;
-  for (int r = 0; r < rows; ++r) s += __bfloat162float(D[(size_t)r * n + j]);
-  g[j] += s;
+  if (col < ncol) {
+    for (int r = r0 + ry; r < r1; r += 8) {
+      const float a = col < n ? __bfloat162float(A[(size_t)r * n + col]) : 1.0f;
+      s += w ? a * w[r] : a;
+    }
+  }
+  sh[ry][cx] = s;
+  __syncthreads();
+  if (ry == 0 && col < ncol) {
+    float t = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) t += sh[k][cx];
+    part[(size_t)chunk * ncol + col] = t;
+  }
 }
 
-/* dw4[j] = sum_r A3[r][j] dy[r]; db4 = sum_r dy[r] */
-__global__ void out_weight_grad(const bf16 *__restrict__ A3, const float *__restrict__ dy,
-                                int rows, int h, float *__restrict__ gw4,
-                                float *__restrict__ gb4) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j > h) return;
+/* out[i] += sum_c part[c * count + i] */
+__global__ void reduce_partials(const float *__restrict__ part, int chunks, size_t count,
+                                float *__restrict__ out) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
   float s = 0.0f;
-  if (j < h) {
-    for (int r = 0; r < rows; ++r) s += __bfloat162float(A3[(size_t)r * h + j]) * dy[r];
-    gw4[j] += s;
-  } else {
-    for (int r = 0; r < rows; ++r) s += dy[r];
-    gb4[0] += s;
+  for (int c = 0; c < chunks; ++c) s += part[(size_t)c * count + i];
+  out[i] += s;
+}
+
+/* part[chunk] = A[chunk rows]^T D[chunk rows]: A [rows][K] row-major, D [rows][N] row-major,
+ * one warp per 16 x 16 tile of the [K][N] result and chunk of SPLIT_ROWS rows */
+__global__ void wmma_tn_split(const bf16 *__restrict__ A, int K, const bf16 *__restrict__ D, int N,
+                              int rows, float *__restrict__ part) {
+  using namespace nvcuda;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int tiles_n = N >> 4, tiles = (K >> 4) * tiles_n;
+  const int chunk = warp / tiles, t = warp - chunk * tiles;
+  const int r0 = chunk * SPLIT_ROWS;
+  if (r0 >= rows) return;
+  const int r1 = min(rows, r0 + SPLIT_ROWS);
+  const int tm = t / tiles_n, tn = t - tm * tiles_n;
+  wmma::fragment<wmma::accumulator, 16, 16, 16, float> acc;
+  wmma::fill_fragment(acc, 0.0f);
+  for (int k = r0; k < r1; k += 16) {
+    wmma::fragment<wmma::matrix_a, 16, 16, 16, bf16, wmma::col_major> a;
+    wmma::fragment<wmma::matrix_b, 16, 16, 16, bf16, wmma::row_major> b;
+    wmma::load_matrix_sync(a, A + (size_t)k * K + tm * 16, K);
+    wmma::load_matrix_sync(b, D + (size_t)k * N + tn * 16, N);
+    wmma::mma_sync(acc, a, b, acc);
   }
+  wmma::store_matrix_sync(part + (size_t)chunk * K * N + (size_t)tm * 16 * N + tn * 16, acc, N,
+                          wmma::mem_row_major);
 }
 
 /* embedding gradient: columns [7, 39) of dX1 scattered to the rows' conformer entries */
@@ -200,6 +241,104 @@ __global__ void init_uniform(float *p, size_t n, float scale, uint32_t tensor, u
   p[i] = scale * gd_sym11(r.v[0]);
 }
 
+/* The whole forward pass of FR rows in one CTA of 8 warps: the rows (embedding columns filled
+ * from the FP32 table) in shared memory, three BF16 tensor-core layers whose FP32 accumulators
+ * are staged through shared memory for bias + SiLU, and the output dot product. Weight
+ * fragments come straight from global memory (L2-resident). Per output element the MMA
+ * sequence, the bias/SiLU arithmetic and the output reduction order are those of the layered
+ * path (wmma_gemm, bias_silu, out_layer), so both paths give the same bits. */
+constexpr int FR = 64;
+
+template <int NT> /* 16-column tiles per warp: H = 128 * NT */
+struct FusedDims {
+  static constexpr int H = 128 * NT, LDX = GD_MLP_IN + 8, LDA = H + 8, LDS = H + 4;
+  static constexpr size_t smem = (size_t)FR * LDX * 2 + (size_t)FR * LDA * 2 + (size_t)FR * LDS * 4;
+};
+
+template <int NT>
+__device__ __forceinline__ void fused_layer(const bf16 *A, int lda, int K, const bf16 *__restrict__ W,
+                                            const float *__restrict__ bias, bf16 *act, float *stg,
+                                            int warp, int tid) {
+  using namespace nvcuda;
+  using D = FusedDims<NT>;
+  wmma::fragment<wmma::accumulator, 16, 16, 16, float> acc[4][NT];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < NT; ++j) wmma::fill_fragment(acc[i][j], 0.0f);
+  for (int k = 0; k < K; k += 16) {
+    wmma::fragment<wmma::matrix_b, 16, 16, 16, bf16, wmma::row_major> b[NT];
+#pragma unroll
+    for (int j = 0; j < NT; ++j)
+      wmma::load_matrix_sync(b[j], W + (size_t)k * D::H + (warp * NT + j) * 16, D::H);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      wmma::fragment<wmma::matrix_a, 16, 16, 16, bf16, wmma::row_major> a;
+      wmma::load_matrix_sync(a, A + i * 16 * lda + k, lda);
+#pragma unroll
+      for (int j = 0; j < NT; ++j) wmma::mma_sync(acc[i][j], a, b[j], acc[i][j]);
+    }
+  }
+  __syncthreads(); /* every warp is done reading A before act is rewritten below */
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < NT; ++j)
+      wmma::store_matrix_sync(stg + i * 16 * D::LDS + (warp * NT + j) * 16, acc[i][j], D::LDS,
+                              wmma::mem_row_major);
+  __syncthreads();
+  for (int e = tid; e < FR * D::H; e += 256) {
+    const int r = e / D::H, c = e - r * D::H;
+    act[r * D::LDA + c] = __float2bfloat16_rn(silu(stg[r * D::LDS + c] + bias[c]));
+  }
+  __syncthreads();
+}
+
+template <int NT>
+__global__ void __launch_bounds__(256) fused_forward(const bf16 *__restrict__ X,
+                                                     const int *__restrict__ conf,
+                                                     const float *__restrict__ theta,
+                                                     const bf16 *__restrict__ wh, MlpLayout L,
+                                                     int rows, float *__restrict__ y) {
+  using D = FusedDims<NT>;
+  extern __shared__ __align__(128) unsigned char fsm[];
+  bf16 *xs = reinterpret_cast<bf16 *>(fsm);
+  bf16 *act = xs + FR * D::LDX;
+  float *stg = reinterpret_cast<float *>(act + FR * D::LDA);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int row0 = blockIdx.x * FR;
+  for (int i = tid; i < FR * 8; i += 256) {
+    const int r = i >> 3, c = i & 7;
+    uint4 v = make_uint4(0u, 0u, 0u, 0u);
+    if (row0 + r < rows) v = reinterpret_cast<const uint4 *>(X + (size_t)(row0 + r) * GD_MLP_IN)[c];
+    *reinterpret_cast<uint4 *>(xs + r * D::LDX + c * 8) = v;
+  }
+  __syncthreads();
+  if (L.n_emb) {
+    for (int i = tid; i < FR * GD_MLP_EMB; i += 256) {
+      const int r = i / GD_MLP_EMB, c = i - r * GD_MLP_EMB;
+      if (row0 + r < rows) {
+        const int e = conf[row0 + r];
+        if (e >= 0)
+          xs[r * D::LDX + GD_MLP_EMB_OFF + c] =
+              __float2bfloat16_rn(theta[L.emb + (size_t)e * GD_MLP_EMB + c]);
+      }
+    }
+    __syncthreads();
+  }
+  fused_layer<NT>(xs, D::LDX, GD_MLP_IN, wh + L.w1, theta + L.b1, act, stg, warp, tid);
+  fused_layer<NT>(act, D::LDA, D::H, wh + L.w2, theta + L.b2, act, stg, warp, tid);
+  fused_layer<NT>(act, D::LDA, D::H, wh + L.w3, theta + L.b3, act, stg, warp, tid);
+  const float *w4 = theta + L.w4;
+  for (int r = warp; r < FR; r += 8) {
+    float s = 0.0f;
+    for (int j = lane; j < D::H; j += 32) s += __bfloat162float(act[r * D::LDA + j]) * w4[j];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0 && row0 + r < rows) y[row0 + r] = s + theta[L.b4];
+  }
+}
+
 inline int blocks(size_t n, int t = 256) { return (int)((n + t - 1) / t); }
 
 }  // namespace
@@ -232,12 +371,17 @@ int mlp_create(Mlp &n, int hidden, int n_emb, uint64_t seed, cudaStream_t s) {
     init_uniform<<<blocks((size_t)n_emb * GD_MLP_EMB), 256, 0, s>>>(
         n.theta + n.L.emb, (size_t)n_emb * GD_MLP_EMB, 0.3f, 5, seed);
   n.adam_t = 0;
+  if (cudaFuncSetAttribute(fused_forward<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)FusedDims<1>::smem) != cudaSuccess ||
+      cudaFuncSetAttribute(fused_forward<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)FusedDims<2>::smem) != cudaSuccess)
+    return -2;
   return mlp_refresh_bf16(n, s);
 }
 
 void mlp_destroy(Mlp &n) {
   void *ps[] = {n.theta, n.grad, n.m, n.v, n.wh, n.loss, n.X, n.A1, n.A2, n.A3, n.D,
-                n.Z1, n.Z2, n.Z3, n.C, n.y, n.dy, n.conf};
+                n.Z1, n.Z2, n.Z3, n.C, n.y, n.dy, n.conf, n.P};
   for (void *p : ps)
     if (p) cudaFree(p);
   n = Mlp();
@@ -295,7 +439,23 @@ static int forward_impl(Mlp &n, int rows, bool keep, cudaStream_t s) {
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
-int mlp_forward(Mlp &n, int rows, cudaStream_t s) { return forward_impl(n, rows, false, s); }
+int mlp_forward(Mlp &n, int rows, cudaStream_t s) {
+  const int H = n.L.hidden;
+  if (rows > n.cap) return -4;
+  if (rows < 1) return 0;
+  if (H == 128) {
+    fused_forward<1><<<(rows + FR - 1) / FR, 256, FusedDims<1>::smem, s>>>(
+        n.X, n.conf, n.theta, n.wh, n.L, rows, n.y);
+  } else if (H == 256) {
+    fused_forward<2><<<(rows + FR - 1) / FR, 256, FusedDims<2>::smem, s>>>(
+        n.X, n.conf, n.theta, n.wh, n.L, rows, n.y);
+  } else {
+    int rc = mlp_embed(n, rows, s);
+    if (rc) return rc;
+    return forward_impl(n, rows, false, s);
+  }
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
 
 int mlp_loss_backward(Mlp &n, int rows, const float *t, cudaStream_t s) {
   const int M = (rows + 15) & ~15, H = n.L.hidden;
@@ -306,23 +466,42 @@ int mlp_loss_backward(Mlp &n, int rows, const float *t, cudaStream_t s) {
   cudaMemsetAsync(n.dy, 0, (size_t)M * 4, s);
   mse_grad<<<blocks(rows), 256, 0, s>>>(n.y, t, n.dy, n.C, rows);
   mean_reduce<<<1, 256, 0, s>>>(n.C, rows, n.loss);
-  /* output layer */
-  out_weight_grad<<<blocks(H + 1), 256, 0, s>>>(n.A3, n.dy, M, H, n.grad + n.L.w4,
-                                                 n.grad + n.L.b4);
+  /* batch reductions in chunks of SPLIT_ROWS rows, partials added in a fixed order */
+  const int S = (M + SPLIT_ROWS - 1) / SPLIT_ROWS;
+  const size_t need = (size_t)S * (size_t)H * (size_t)(H > GD_MLP_IN ? H : GD_MLP_IN) + S;
+  if (need > n.p_cap) {
+    if (n.P) cudaFree(n.P);
+    n.P = nullptr;
+    n.p_cap = 0;
+    if (cudaMalloc(&n.P, need * sizeof(float)) != cudaSuccess) return -3;
+    n.p_cap = need;
+  }
+  auto colsum = [&](const bf16 *A, const float *w, float *g) {
+    const int ncol = H + (w ? 1 : 0);
+    colsum_split<<<dim3((ncol + 31) / 32, S), 256, 0, s>>>(A, w, M, H, n.P);
+    reduce_partials<<<blocks(ncol), 256, 0, s>>>(n.P, S, (size_t)ncol, g);
+  };
+  auto weight_grad = [&](const bf16 *A, int K, float *g) {
+    const int warps = S * (K / 16) * (H / 16);
+    wmma_tn_split<<<(warps + 7) / 8, 256, 0, s>>>(A, K, n.D, H, M, n.P);
+    reduce_partials<<<blocks((size_t)K * H), 256, 0, s>>>(n.P, S, (size_t)K * H, g);
+  };
+  /* output layer: dw4 = A3^T dy and db4 = sum dy (b4 follows w4 in theta) */
+  colsum(n.A3, n.dy, n.grad + n.L.w4);
   out_backward<<<blocks((size_t)M * H), 256, 0, s>>>(n.dy, n.theta + n.L.w4, n.Z3, n.D, M, H);
   /* layer 3: dW3 = A2^T dZ3, db3, dA2 = dZ3 W3^T */
-  gemm<true, false>(n.A2, H, n.D, H, n.grad + n.L.w3, H, H, H, M, s);
-  colsum_bf16<<<blocks(H), 256, 0, s>>>(n.D, M, H, n.grad + n.L.b3);
+  weight_grad(n.A2, H, n.grad + n.L.w3);
+  colsum(n.D, nullptr, n.grad + n.L.b3);
   gemm<false, true>(n.D, H, n.wh + n.L.w3, H, n.C, H, M, H, H, s);
   act_backward<<<blocks((size_t)M * H), 256, 0, s>>>(n.C, n.Z2, n.D, (size_t)M * H);
   /* layer 2 */
-  gemm<true, false>(n.A1, H, n.D, H, n.grad + n.L.w2, H, H, H, M, s);
-  colsum_bf16<<<blocks(H), 256, 0, s>>>(n.D, M, H, n.grad + n.L.b2);
+  weight_grad(n.A1, H, n.grad + n.L.w2);
+  colsum(n.D, nullptr, n.grad + n.L.b2);
   gemm<false, true>(n.D, H, n.wh + n.L.w2, H, n.C, H, M, H, H, s);
   act_backward<<<blocks((size_t)M * H), 256, 0, s>>>(n.C, n.Z1, n.D, (size_t)M * H);
   /* layer 1: dW1 = X^T dZ1 (64 x H), db1; dX1 = dZ1 W1^T for the embedding */
-  gemm<true, false>(n.X, GD_MLP_IN, n.D, H, n.grad + n.L.w1, H, GD_MLP_IN, H, M, s);
-  colsum_bf16<<<blocks(H), 256, 0, s>>>(n.D, M, H, n.grad + n.L.b1);
+  weight_grad(n.X, GD_MLP_IN, n.grad + n.L.w1);
+  colsum(n.D, nullptr, n.grad + n.L.b1);
   if (n.L.n_emb) {
     gemm<false, true>(n.D, H, n.wh + n.L.w1, H, n.C, GD_MLP_IN, M, GD_MLP_IN, H, s);
     emb_grad<<<blocks((size_t)rows * GD_MLP_EMB), 256, 0, s>>>(n.C, n.conf, rows,

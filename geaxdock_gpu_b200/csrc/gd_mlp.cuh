@@ -62,12 +62,15 @@ struct Mlp {
   float *Z1 = nullptr, *Z2 = nullptr, *Z3 = nullptr, *C = nullptr, *y = nullptr, *dy = nullptr;
   float *loss = nullptr;              /* [1] */
   int *conf = nullptr;                /* [cap] embedding row per input row */
+  float *P = nullptr;                 /* per-chunk partials of the batch reductions */
+  size_t p_cap = 0;
 };
 
 int mlp_create(Mlp &n, int hidden, int n_emb, uint64_t seed, cudaStream_t s);
 void mlp_destroy(Mlp &n);
 int mlp_reserve(Mlp &n, int rows);
-/* rows of X (bf16, 64 wide, embedding columns filled by the caller or by mlp_embed) -> y */
+/* rows of X (bf16, 64 wide) -> y; the embedding columns of rows with conf >= 0 are taken from
+ * the table (one fused kernel for H = 128 and 256, layer by layer otherwise) */
 int mlp_forward(Mlp &n, int rows, cudaStream_t s);
 /* rows of X from device FP32 rows (rounded to BF16) and their conformer ids */
 int mlp_set_rows(Mlp &n, const float *x, const int *conf, int rows, cudaStream_t s);
