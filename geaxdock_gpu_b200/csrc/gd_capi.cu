@@ -31,9 +31,9 @@ extern template __global__ void gd_mc_kernel<1>(GdMcArgs, GdForceConst);
 extern template __global__ void gd_mc_kernel<2>(GdMcArgs, GdForceConst);
 extern template __global__ void gd_mc_kernel<4>(GdMcArgs, GdForceConst);
 __global__ void gd_exchange_kernel(const GdDevComplex *cxs, const int *group_base, int n_complex,
-                                   int n_groups, gd_replica *replica, const float *etotal,
-                                   int *acs, uint64_t seed, const int *call_base, int call_off,
-                                   int mode_t);
+                                   int g_begin, int g_end, gd_replica *replica,
+                                   const float *etotal, int *acs, uint64_t seed,
+                                   const int *call_base, int call_off, int mode_t);
 __global__ void gd_reset_records_kernel(int *rec_next, int r0, int r1);
 }  // namespace gd
 
@@ -87,6 +87,16 @@ struct ComplexInfo {
   int stream;
 };
 
+/* One chain of the fused loops: a contiguous range of (complex, protein conformer) blocks,
+ * their replicas, exchange groups and tiles. Chains share nothing, so the graph runs them on
+ * separate streams and one chain's kernels fill the other's tail. */
+struct Chain {
+  int g0, g1;    /* blocks [g0, g1) in (complex, protein conformer) order */
+  int r0, r1;    /* replicas */
+  int xg0, xg1;  /* exchange groups */
+  int t_off, t_cnt; /* plain tiles in the chain tile list */
+};
+
 }  // namespace
 
 struct gd_ctx {
@@ -138,6 +148,15 @@ struct gd_ctx {
   long long timeout_ns = 2000000000LL;
   /* surrogate and delayed acceptance (gd_sur_create) */
   struct DaState *da = nullptr;
+  /* concurrent chains of the fused loops: plain (gd_mc_run_fused) and delayed acceptance */
+  int chains = 1, chains_da = 3;
+  std::vector<cudaStream_t> aux;             /* streams of chains 1.. */
+  cudaEvent_t ev_fork = nullptr;
+  std::vector<cudaEvent_t> ev_join;
+  std::vector<Chain> chain;
+  int chain_gen = -1;
+  GdTileDesc *d_chain_tiles = nullptr;
+  int chain_tiles_cap = 0;
 };
 
 namespace {
@@ -367,6 +386,112 @@ int check_range(const gd_ctx *c, int r0, int r1) {
   return GD_OK;
 }
 
+/* Partition of the batch into `want` contiguous block ranges of about equal pair work; with
+ * `tiles`, each chain's plain tile list (longest first within the chain) appended to it. */
+void build_chains(gd_ctx *c, int want, std::vector<Chain> &ch, std::vector<GdTileDesc> *tiles) {
+  int n_blocks = 0;
+  for (const auto &x : c->info) n_blocks += x.n_prt;
+  want = std::max(1, std::min(want, n_blocks));
+  struct Blk { int r0, r1, xg0, xg1; double cost; };
+  std::vector<Blk> blk;
+  int xg = 0;
+  double total = 0.0;
+  for (int ci = 0; ci < c->n_complex; ++ci) {
+    const ComplexInfo &x = c->info[ci];
+    const int block = x.n_tmp * x.n_lig;
+    for (int p = 0; p < x.n_prt; ++p) {
+      Blk b;
+      b.r0 = x.rep_offset + p * block;
+      b.r1 = b.r0 + block;
+      b.xg0 = xg + p * x.n_lig;
+      b.xg1 = b.xg0 + x.n_lig;
+      b.cost = (double)block * x.lna * x.pnp_pad;
+      total += b.cost;
+      blk.push_back(b);
+    }
+    xg += x.n_prt * x.n_lig;
+  }
+  ch.clear();
+  int g = 0;
+  double acc = 0.0;
+  for (int k = 0; k < want; ++k) {
+    Chain cc;
+    cc.g0 = g;
+    const double target = total * (k + 1) / want;
+    /* at least one block, and one left for every later chain */
+    do {
+      acc += blk[g].cost;
+      ++g;
+    } while (g < n_blocks - (want - 1 - k) && acc + 0.5 * blk[g].cost <= target);
+    if (k == want - 1) g = n_blocks;
+    cc.g1 = g;
+    cc.r0 = blk[cc.g0].r0;
+    cc.r1 = blk[cc.g1 - 1].r1;
+    cc.xg0 = blk[cc.g0].xg0;
+    cc.xg1 = blk[cc.g1 - 1].xg1;
+    cc.t_off = cc.t_cnt = 0;
+    if (tiles) {
+      std::vector<GdTileDesc> t;
+      build_tiles(c, cc.r0, cc.r1 - 1, t);
+      cc.t_off = (int)tiles->size();
+      cc.t_cnt = (int)t.size();
+      tiles->insert(tiles->end(), t.begin(), t.end());
+    }
+    ch.push_back(cc);
+  }
+}
+
+/* streams and events for n chains (chain 0 runs on the context's stream) */
+int ensure_chain_streams(gd_ctx *c, int n) {
+  while ((int)c->aux.size() < n - 1) {
+    cudaStream_t st;
+    CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    c->aux.push_back(st);
+    cudaEvent_t ev;
+    CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    c->ev_join.push_back(ev);
+  }
+  if (!c->ev_fork) CK(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+  return GD_OK;
+}
+
+/* the plain fused loop's chains and their tile lists on the device */
+int ensure_chains(gd_ctx *c) {
+  if (c->chain_gen == c->tile_gen && !c->chain.empty()) return GD_OK;
+  std::vector<Chain> ch;
+  std::vector<GdTileDesc> tiles;
+  build_chains(c, c->chains, ch, &tiles);
+  CK(cudaStreamSynchronize(c->stream));
+  if ((int)tiles.size() > c->chain_tiles_cap) {
+    if (c->d_chain_tiles) cudaFree(c->d_chain_tiles);
+    c->d_chain_tiles = nullptr;
+    c->chain_tiles_cap = 0;
+    CK(cudaMalloc(&c->d_chain_tiles, sizeof(GdTileDesc) * tiles.size()));
+    c->chain_tiles_cap = (int)tiles.size();
+  }
+  CK(cudaMemcpy(c->d_chain_tiles, tiles.data(), sizeof(GdTileDesc) * tiles.size(),
+                cudaMemcpyHostToDevice));
+  int rc = ensure_chain_streams(c, (int)ch.size());
+  if (rc) return rc;
+  c->chain = ch;
+  c->chain_gen = c->tile_gen;
+  return GD_OK;
+}
+
+/* during capture on c->stream: the chains' streams join the capture / rejoin the main stream */
+void chains_fork(gd_ctx *c, int n) {
+  if (n <= 1) return;
+  cudaEventRecord(c->ev_fork, c->stream);
+  for (int k = 1; k < n; ++k) cudaStreamWaitEvent(c->aux[k - 1], c->ev_fork, 0);
+}
+void chains_join(gd_ctx *c, int n) {
+  for (int k = 1; k < n; ++k) {
+    cudaEventRecord(c->ev_join[k - 1], c->aux[k - 1]);
+    cudaStreamWaitEvent(c->stream, c->ev_join[k - 1], 0);
+  }
+}
+cudaStream_t chain_stream(gd_ctx *c, int k) { return k ? c->aux[k - 1] : c->stream; }
+
 void da_free(gd_ctx *c);        /* delayed-acceptance state, defined with its entry points */
 void da_drop_graphs(gd_ctx *c);
 
@@ -473,6 +598,10 @@ int gd_destroy(gd_ctx *c) {
   if (c->d_e_out) cudaFree(c->d_e_out);
   if (c->d_eval_tiles) cudaFree(c->d_eval_tiles);
   if (c->h_cursor) cudaFreeHost(c->h_cursor);
+  if (c->d_chain_tiles) cudaFree(c->d_chain_tiles);
+  for (cudaStream_t st : c->aux) cudaStreamDestroy(st);
+  for (cudaEvent_t ev : c->ev_join) cudaEventDestroy(ev);
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return GD_OK;
@@ -938,6 +1067,19 @@ int gd_autotune(gd_ctx *c, const gd_tile *cand, int n_cand, int repeats, gd_tile
   return rc;
 }
 
+int gd_set_concurrency(gd_ctx *c, int plain_chains, int da_chains) {
+  if (!c || plain_chains < 1 || plain_chains > 16 || da_chains < 1 || da_chains > 16)
+    return fail(GD_ERR_INVALID, "chains must be in 1..16");
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->stream));
+  c->chains = plain_chains;
+  c->chains_da = da_chains;
+  c->chain_gen = -1;
+  c->chain.clear();
+  drop_graphs(c);
+  return GD_OK;
+}
+
 int gd_set_rng_stream(gd_ctx *c, int k, int stream) {
   if (!c || k < 0 || k >= c->n_complex || stream < 0)
     return fail(GD_ERR_INVALID, "bad complex index or stream");
@@ -1015,8 +1157,8 @@ int gd_exchange(gd_ctx *c, int mode_l, int mode_t) {
   if (mode_t < 0) return fail(GD_ERR_INVALID, "mode_t must be >= 0");
   CK(cudaSetDevice(c->device));
   gd::gd_exchange_kernel<<<(c->n_groups + 127) / 128, 128, 0, c->stream>>>(
-      c->d_cx, c->d_group_base, c->n_complex, c->n_groups, c->d_replica, c->d_etotal, c->d_acs,
-      c->mc.seed, nullptr, c->exchange_calls, mode_t);
+      c->d_cx, c->d_group_base, c->n_complex, 0, c->n_groups, c->d_replica, c->d_etotal,
+      c->d_acs, c->mc.seed, nullptr, c->exchange_calls, mode_t);
   CK(cudaGetLastError());
   c->exchange_calls += 1;
   return GD_OK;
@@ -1029,36 +1171,42 @@ int gd_mc_run_fused(gd_ctx *c, int s1, int n_steps, int exchange) {
   if (n_steps < 1 || n_steps % spe)
     return fail(GD_ERR_INVALID, "n_steps must be a positive multiple of steps_per_exchange");
   CK(cudaSetDevice(c->device));
-  const int chunks = n_steps / spe;
-  int rc = ensure_counters(c, chunks);
+  int rc = ensure_chains(c);
   if (rc) return rc;
+  const int nch = (int)c->chain.size();
+  const int chunks = n_steps / spe;
+  if ((rc = ensure_counters(c, chunks * nch))) return rc;
   const long long key = ((long long)n_steps << 1) | (exchange ? 1 : 0);
   auto it = c->graphs.find(key);
   if (it == c->graphs.end()) {
-    int n = 0;
-    if ((rc = upload_tiles(c, 0, c->n_rep - 1, &n))) return rc;
     CK(cudaStreamSynchronize(c->stream));
     const size_t smem = smem_bytes(c);
     if ((rc = set_kernel_attrs(c, smem))) return rc;
-    const int grid = grid_for(c, n, smem);
     cudaGraph_t graph;
     CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    cudaMemsetAsync(c->d_counters, 0, sizeof(int) * chunks, c->stream);
-    for (int i = 0; i < chunks; ++i) {
-      GdMcArgs a = base_args(c);
-      a.mode = 0;
-      a.n_steps = spe;
-      a.step0 = i * spe;
-      a.step_base = c->d_cursor;
-      a.tiles = c->d_tiles;
-      a.n_tiles = n;
-      a.tile_counter = c->d_counters + i;
-      mc_kernel(c->unroll)<<<grid, c->threads, smem, c->stream>>>(a, c->fc);
-      if (exchange)
-        gd::gd_exchange_kernel<<<(c->n_groups + 127) / 128, 128, 0, c->stream>>>(
-            c->d_cx, c->d_group_base, c->n_complex, c->n_groups, c->d_replica, c->d_etotal,
-            c->d_acs, c->mc.seed, c->d_cursor + 1, i, !(i % 2));
+    cudaMemsetAsync(c->d_counters, 0, sizeof(int) * chunks * nch, c->stream);
+    chains_fork(c, nch);
+    for (int k = 0; k < nch; ++k) {
+      const Chain &ch = c->chain[k];
+      cudaStream_t st = chain_stream(c, k);
+      const int grid = grid_for(c, ch.t_cnt, smem);
+      for (int i = 0; i < chunks; ++i) {
+        GdMcArgs a = base_args(c);
+        a.mode = 0;
+        a.n_steps = spe;
+        a.step0 = i * spe;
+        a.step_base = c->d_cursor;
+        a.tiles = c->d_chain_tiles + ch.t_off;
+        a.n_tiles = ch.t_cnt;
+        a.tile_counter = c->d_counters + k * chunks + i;
+        mc_kernel(c->unroll)<<<grid, c->threads, smem, st>>>(a, c->fc);
+        if (exchange)
+          gd::gd_exchange_kernel<<<(ch.xg1 - ch.xg0 + 127) / 128, 128, 0, st>>>(
+              c->d_cx, c->d_group_base, c->n_complex, ch.xg0, ch.xg1, c->d_replica, c->d_etotal,
+              c->d_acs, c->mc.seed, c->d_cursor + 1, i, !(i % 2));
+      }
     }
+    chains_join(c, nch);
     cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
     if (ce != cudaSuccess) return fail(GD_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
     cudaGraphExec_t exec;
@@ -1067,12 +1215,7 @@ int gd_mc_run_fused(gd_ctx *c, int s1, int n_steps, int exchange) {
     if (ce != cudaSuccess) return fail(GD_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ce));
     it = c->graphs.emplace(key, exec).first;
   }
-  /* the graph reads the full-range tile list and its step and exchange-call bases from
-   * the device cursor */
-  {
-    int n = 0;
-    if ((rc = upload_tiles(c, 0, c->n_rep - 1, &n))) return rc;
-  }
+  /* the graph reads its step and exchange-call bases from the device cursor */
   CK(cudaStreamSynchronize(c->stream));
   c->h_cursor[0] = s1;
   c->h_cursor[1] = c->exchange_calls;
@@ -1422,16 +1565,21 @@ struct DaState {
   std::vector<gd::GdGroup> groups;
   int n_tiles = 0, built_gen = -1;
   std::vector<void *> allocs;
-  gd::GdGroup *d_groups = nullptr;
-  int *d_rep_cx = nullptr, *d_emb_base = nullptr, *d_active = nullptr;
+  int *d_rep_cx = nullptr, *d_rep_group = nullptr, *d_group_b0 = nullptr;
+  int *d_emb_base = nullptr, *d_active = nullptr;
   float *d_pocket = nullptr;
-  float *d_mm_prop = nullptr, *d_u1 = nullptr, *d_u2 = nullptr, *d_s_cur = nullptr,
-        *d_s_new = nullptr, *d_pose_mm = nullptr;
-  int *d_pose_rep = nullptr, *d_pose_lc = nullptr, *d_group_cnt = nullptr;
-  gd_energy *d_pose_e = nullptr;
+  float *d_u2 = nullptr, *d_s_cur = nullptr, *d_s_new = nullptr, *d_pose_mm = nullptr;
+  int *d_pose_rep = nullptr, *d_pose_lc = nullptr;
+  int *d_cnt = nullptr;                          /* [2][n_groups] survivor counters */
   GdTileDesc *d_tiles = nullptr;
-  unsigned long long *d_stats = nullptr;
-  double *d_err = nullptr;
+  /* per-replica counters */
+  int *d_prop = nullptr, *d_pass = nullptr, *d_plain = nullptr, *d_acc = nullptr,
+      *d_plain_acc = nullptr, *d_nerr = nullptr;
+  double *d_err2 = nullptr;
+  GdDaEpi epi{};                                 /* host copy of the device struct */
+  GdDaEpi *d_epi = nullptr;
+  unsigned long long *d_stats = nullptr;         /* [n_complex][GD_DA_NSTAT] (da_stats) */
+  double *d_err = nullptr;                       /* [n_complex][GD_DA_NERR] */
   __nv_bfloat16 *smp_X = nullptr;
   int *smp_conf = nullptr;
   float *smp_t = nullptr;
@@ -1450,7 +1598,7 @@ struct DaState {
   std::vector<int> active;
   std::vector<unsigned long long> window0; /* counters at the last controller decision */
   std::map<long long, cudaGraphExec_t> graphs;
-  int *d_counters = nullptr;
+  int *d_counters = nullptr;               /* persistent-CTA queue heads, one per step */
   int counters_cap = 0;
 };
 
@@ -1497,12 +1645,42 @@ void da_free(gd_ctx *c) {
   c->da = nullptr;
 }
 
-/* groups and their fixed tile positions for the current tile shapes */
+/* the device struct the exact kernel reads in mode 3 (trace pointers included) */
+int da_upload_epi(gd_ctx *c) {
+  DaState *d = c->da;
+  GdDaEpi &e = d->epi;
+  e.group_b0 = d->d_group_b0;
+  e.n_groups = (int)d->groups.size();
+  e.n_rep = c->n_rep;
+  e.pose_rep = d->d_pose_rep;
+  e.s_new = d->d_s_new;
+  e.s_cur = d->d_s_cur;
+  e.u2 = d->d_u2;
+  e.active = d->d_active;
+  e.acc = d->d_acc;
+  e.plain_acc = d->d_plain_acc;
+  e.err2 = d->d_err2;
+  e.nerr = d->d_nerr;
+  e.smp_t = d->smp_t;
+  e.smp_cap = d->smp_cap;
+  e.tr_s = d->tr_s;
+  e.tr_e = d->tr_e;
+  e.tr_flag = d->tr_flag;
+  e.tr_cap = d->tr_cap;
+  e.tr_step0 = d->tr_step0;
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaMemcpy(d->d_epi, &e, sizeof(e), cudaMemcpyHostToDevice));
+  return GD_OK;
+}
+
+/* groups and the exact kernel's static tile list for the current tile shapes: tile i of
+ * group g covers pose slots [b0 + i k, b0 + i k + cap) and carries (g << 8) | cap */
 int da_build_groups(gd_ctx *c) {
   DaState *d = c->da;
   if (d->built_gen == c->tile_gen && d->d_tiles) return GD_OK;
   std::vector<gd::GdGroup> g;
-  int tb = 0;
+  std::vector<GdTileDesc> tiles;
+  std::vector<int> rep_group(c->n_rep), b0s;
   for (int ci = 0; ci < c->n_complex; ++ci) {
     const ComplexInfo &x = c->info[ci];
     const int block = x.n_tmp * x.n_lig;
@@ -1514,31 +1692,49 @@ int da_build_groups(gd_ctx *c) {
       q.n = block;
       q.k = x.k;
       q.n_tiles = (block + x.k - 1) / x.k;
-      q.tile_base = tb;
+      q.tile_base = (int)tiles.size();
       q.pad = 0;
-      tb += q.n_tiles;
+      const int gi = (int)g.size();
+      for (int i = 0; i < q.n_tiles; ++i) {
+        GdTileDesc t;
+        t.complex_index = ci;
+        t.prt_conf = p;
+        t.rep_begin = q.b0 + i * q.k;
+        t.count = (gi << 8) | std::min(q.k, block - i * q.k);
+        tiles.push_back(t);
+      }
+      for (int r = 0; r < block; ++r) rep_group[q.b0 + r] = gi;
+      b0s.push_back(q.b0);
       g.push_back(q);
     }
   }
+  if (g.size() >= (1u << 23)) return fail(GD_ERR_CAPACITY, "too many compaction groups");
   CK(cudaStreamSynchronize(c->stream));
-  if ((int)g.size() != (int)d->groups.size() || tb > d->n_tiles) {
-    /* sizes only grow with smaller k; reallocate the tile list when needed */
+  const bool first = d->d_group_b0 == nullptr;
+  if (first) {
+    int rc;
+    if ((rc = da_alloc(d, &d->d_group_b0, g.size()))) return rc;
+    if ((rc = da_alloc(d, &d->d_rep_group, (size_t)c->n_rep))) return rc;
+    if ((rc = da_alloc(d, &d->d_cnt, 2 * g.size()))) return rc;
+    CK(cudaMemcpy(d->d_group_b0, b0s.data(), sizeof(int) * b0s.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d->d_rep_group, rep_group.data(), sizeof(int) * c->n_rep,
+                  cudaMemcpyHostToDevice));
+    CK(cudaMemset(d->d_cnt, 0, sizeof(int) * 2 * g.size()));
+  }
+  if ((int)tiles.size() > d->n_tiles) {
     if (d->d_tiles) {
       cudaFree(d->d_tiles);
       d->allocs.erase(std::remove(d->allocs.begin(), d->allocs.end(), (void *)d->d_tiles),
                       d->allocs.end());
       d->d_tiles = nullptr;
     }
-    int rc = da_alloc(d, &d->d_tiles, tb);
+    int rc = da_alloc(d, &d->d_tiles, tiles.size());
     if (rc) return rc;
-    if (!d->d_groups) {
-      if ((rc = da_alloc(d, &d->d_groups, g.size()))) return rc;
-      if ((rc = da_alloc(d, &d->d_group_cnt, g.size()))) return rc;
-    }
   }
-  CK(cudaMemcpy(d->d_groups, g.data(), sizeof(gd::GdGroup) * g.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d->d_tiles, tiles.data(), sizeof(GdTileDesc) * tiles.size(),
+                cudaMemcpyHostToDevice));
   d->groups = g;
-  d->n_tiles = tb;
+  d->n_tiles = (int)tiles.size();
   d->built_gen = c->tile_gen;
   da_drop_graphs(c);
   return GD_OK;
@@ -1550,38 +1746,30 @@ gd::GdDaDev da_args(gd_ctx *c) {
   memset(&a, 0, sizeof(a));
   a.cx = c->d_cx;
   a.rep_cx = d->d_rep_cx;
+  a.rep_group = d->d_rep_group;
+  a.group_b0 = d->d_group_b0;
   a.emb_base = d->d_emb_base;
   a.pocket_feat = d->d_pocket;
   a.active = d->d_active;
-  a.groups = d->d_groups;
-  a.n_groups = (int)d->groups.size();
   a.n_rep = c->n_rep;
   a.replica = c->d_replica;
   a.mm_old = c->d_mm;
-  a.e_old = c->d_eold;
-  a.etotal = c->d_etotal;
-  a.n_accept = c->d_nacc;
-  a.rec = c->mc.record ? c->d_rec : nullptr;
-  a.rec_next = c->d_rec_next;
-  a.rec_cap = c->rec_cap;
-  a.mm_prop = d->d_mm_prop;
-  a.u1 = d->d_u1;
   a.u2 = d->d_u2;
   a.s_cur = d->d_s_cur;
   a.s_new = d->d_s_new;
   a.pose_rep = d->d_pose_rep;
   a.pose_mm = d->d_pose_mm;
   a.pose_lc = d->d_pose_lc;
-  a.pose_e = d->d_pose_e;
-  a.tiles = d->d_tiles;
-  a.group_cnt = d->d_group_cnt;
-  a.X = d->net.X;
-  a.conf = d->net.conf;
-  a.y = d->net.y;
+  a.prop = d->d_prop;
+  a.pass = d->d_pass;
+  a.plain = d->d_plain;
+  a.theta = d->net.theta;
+  a.wh = d->net.wh;
+  a.L = d->net.L;
   a.mu = d->net.mu;
   a.sigma = d->net.sigma;
-  a.stats = d->d_stats;
-  a.err = d->d_err;
+  a.X = d->net.X;
+  a.conf = d->net.conf;
   a.smp_X = d->smp_X;
   a.smp_conf = d->smp_conf;
   a.smp_t = d->smp_t;
@@ -1595,29 +1783,39 @@ gd::GdDaDev da_args(gd_ctx *c) {
   a.move_kind = c->mc.move_kind;
   for (int i = 0; i < 6; ++i) a.move_scale[i] = c->mc.move_scale[i];
   a.step_base = c->d_cursor;
-  a.errw = c->d_err;
   return a;
 }
 
-/* exact energies of the survivors: gd_mc_kernel in pose-evaluation mode over the DA tiles */
-void da_launch_exact(gd_ctx *c, int step, size_t smem, int grid) {
+/* the exact stage of step j of one chain: gd_mc_kernel mode 3 over the chain's part of the
+ * static tile list */
+void da_launch_exact(gd_ctx *c, const Chain &ch, int k, int n_steps, int j, bool collect,
+                     size_t smem, cudaStream_t st) {
   DaState *d = c->da;
+  const int ng = (int)d->groups.size();
+  const int t0 = d->groups[ch.g0].tile_base;
+  const int t1 = d->groups[ch.g1 - 1].tile_base + d->groups[ch.g1 - 1].n_tiles;
   GdMcArgs a = base_args(c);
-  a.mode = 2;
+  a.mode = 3;
   a.n_steps = 1;
-  a.rec = nullptr;
+  a.step0 = j;
+  a.step_base = c->d_cursor;
   a.trace_e = nullptr;
   a.trace_acc = nullptr;
   a.mm_in = d->d_pose_mm;
   a.lig_conf_in = d->d_pose_lc;
-  a.e_out = d->d_pose_e;
-  a.tiles = d->d_tiles;
-  a.n_tiles = d->n_tiles;
-  a.tile_counter = d->d_counters + step;
-  mc_kernel(c->unroll)<<<grid, c->threads, smem, c->stream>>>(a, c->fc);
+  a.tiles = d->d_tiles + t0;
+  a.n_tiles = t1 - t0;
+  a.tile_counter = d->d_counters + (size_t)k * n_steps + j;
+  a.da = d->d_epi;
+  a.da_cnt = d->d_cnt + (size_t)(j & 1) * ng;
+  a.da_cnt_next = d->d_cnt + (size_t)((j + 1) & 1) * ng;
+  a.da_g0 = ch.g0;
+  a.da_g1 = ch.g1;
+  a.da_collect = collect ? 1 : 0;
+  mc_kernel(c->unroll)<<<grid_for(c, t1 - t0, smem), c->threads, smem, st>>>(a, c->fc);
 }
 
-/* the graph of n_steps steps (collect: plain steps that store samples) */
+/* the graph of n_steps steps (collect: plain steps that store samples), one chain per stream */
 int da_graph(gd_ctx *c, int n_steps, int exchange, bool collect, cudaGraphExec_t *out) {
   DaState *d = c->da;
   const long long key = ((long long)n_steps << 2) | (exchange ? 2 : 0) | (collect ? 1 : 0);
@@ -1626,44 +1824,54 @@ int da_graph(gd_ctx *c, int n_steps, int exchange, bool collect, cudaGraphExec_t
     *out = it->second;
     return GD_OK;
   }
-  if (n_steps > d->counters_cap) {
+  std::vector<Chain> chains;
+  build_chains(c, c->chains_da, chains, nullptr);
+  int rc = ensure_chain_streams(c, (int)chains.size());
+  if (rc) return rc;
+  const int nch = (int)chains.size();
+  if (n_steps * nch > d->counters_cap) {
     if (d->d_counters) cudaFree(d->d_counters);
     d->d_counters = nullptr;
     d->counters_cap = 0;
-    CK(cudaMalloc(&d->d_counters, sizeof(int) * n_steps));
-    d->counters_cap = n_steps;
+    CK(cudaMalloc(&d->d_counters, sizeof(int) * n_steps * nch));
+    d->counters_cap = n_steps * nch;
   }
+  if ((rc = da_upload_epi(c))) return rc;
   CK(cudaStreamSynchronize(c->stream));
   const size_t smem = smem_bytes(c);
-  int rc = set_kernel_attrs(c, smem);
-  if (rc) return rc;
-  const int grid = grid_for(c, d->n_tiles, smem);
+  if ((rc = set_kernel_attrs(c, smem))) return rc;
   const gd::GdDaDev a = da_args(c);
   const int spe = c->mc.steps_per_exchange;
+  const int ng = (int)d->groups.size();
   cudaGraph_t graph;
   CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-  cudaMemsetAsync(d->d_counters, 0, sizeof(int) * n_steps, c->stream);
-  if (!collect) {
-    /* surrogate at the current poses under the current network */
-    gd::da_propose(a, 0, true, c->stream);
-    gd::mlp_forward(d->net, c->n_rep, c->stream);
-    gd::da_set_current(a, c->stream);
-  }
-  for (int j = 0; j < n_steps; ++j) {
-    gd::da_propose(a, j, false, c->stream);
-    if (!collect) gd::mlp_forward(d->net, c->n_rep, c->stream);
-    gd::da_stage1(a, j, collect, c->stream);
-    da_launch_exact(c, j, smem, grid);
-    gd::da_stage2(a, j, collect, c->stream);
-    if (exchange && (j + 1) % spe == 0) {
-      const int i = (j + 1) / spe - 1;
-      gd::gd_exchange_kernel<<<(c->n_groups + 127) / 128, 128, 0, c->stream>>>(
-          c->d_cx, c->d_group_base, c->n_complex, c->n_groups, c->d_replica, c->d_etotal,
-          c->d_acs, c->mc.seed, c->d_cursor + 1, i, !(i % 2));
+  int frc = 0;
+  cudaMemsetAsync(d->d_counters, 0, sizeof(int) * n_steps * nch, c->stream);
+  cudaMemsetAsync(d->d_cnt, 0, sizeof(int) * 2 * ng, c->stream);
+  chains_fork(c, nch);
+  for (int k = 0; k < nch; ++k) {
+    const Chain &ch = chains[k];
+    cudaStream_t st = chain_stream(c, k);
+    if (!collect) frc |= gd::da_front(a, GD_DA_CURRENT, 0, d->d_cnt, ch.r0, ch.r1, st);
+    for (int j = 0; j < n_steps; ++j) {
+      frc |= gd::da_front(a, collect ? GD_DA_COLLECT : GD_DA_STEP, j,
+                          d->d_cnt + (size_t)(j & 1) * ng, ch.r0, ch.r1, st);
+      da_launch_exact(c, ch, k, n_steps, j, collect, smem, st);
+      if (exchange && (j + 1) % spe == 0) {
+        const int i = (j + 1) / spe - 1;
+        gd::gd_exchange_kernel<<<(ch.xg1 - ch.xg0 + 127) / 128, 128, 0, st>>>(
+            c->d_cx, c->d_group_base, c->n_complex, ch.xg0, ch.xg1, c->d_replica, c->d_etotal,
+            c->d_acs, c->mc.seed, c->d_cursor + 1, i, !(i % 2));
+      }
     }
   }
+  chains_join(c, nch);
   cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
   if (ce != cudaSuccess) return fail(GD_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+  if (frc) {
+    cudaGraphDestroy(graph);
+    return fail(GD_ERR_INVALID, "delayed acceptance needs hidden = 128 or 256");
+  }
   cudaGraphExec_t exec;
   ce = cudaGraphInstantiate(&exec, graph, 0);
   cudaGraphDestroy(graph);
@@ -1701,6 +1909,8 @@ int da_read_stats(gd_ctx *c, std::vector<unsigned long long> &st, std::vector<do
   DaState *d = c->da;
   st.assign((size_t)c->n_complex * GD_DA_NSTAT, 0);
   er.assign((size_t)c->n_complex * GD_DA_NERR, 0.0);
+  gd::da_stats(da_args(c), d->epi, c->d_cx, c->n_complex, d->d_stats, d->d_err, c->stream);
+  CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->stream));
   CK(cudaMemcpy(st.data(), d->d_stats, st.size() * sizeof(unsigned long long),
                 cudaMemcpyDeviceToHost));
@@ -1718,9 +1928,14 @@ int da_upload_active(gd_ctx *c) {
 
 int da_reset_counters(gd_ctx *c) {
   DaState *d = c->da;
-  CK(cudaMemsetAsync(d->d_stats, 0, sizeof(unsigned long long) * c->n_complex * GD_DA_NSTAT,
-                     c->stream));
-  CK(cudaMemsetAsync(d->d_err, 0, sizeof(double) * c->n_complex * GD_DA_NERR, c->stream));
+  const size_t R = c->n_rep;
+  CK(cudaMemsetAsync(d->d_prop, 0, sizeof(int) * R, c->stream));
+  CK(cudaMemsetAsync(d->d_pass, 0, sizeof(int) * R, c->stream));
+  CK(cudaMemsetAsync(d->d_plain, 0, sizeof(int) * R, c->stream));
+  CK(cudaMemsetAsync(d->d_acc, 0, sizeof(int) * R, c->stream));
+  CK(cudaMemsetAsync(d->d_plain_acc, 0, sizeof(int) * R, c->stream));
+  CK(cudaMemsetAsync(d->d_nerr, 0, sizeof(int) * R, c->stream));
+  CK(cudaMemsetAsync(d->d_err2, 0, sizeof(double) * R, c->stream));
   d->window0.assign((size_t)c->n_complex * GD_DA_NSTAT, 0);
   return GD_OK;
 }
@@ -1821,7 +2036,11 @@ int gd_sur_create(gd_ctx *c, const gd_sur_params *p) {
     return fail(GD_ERR_INVALID, "hidden must be a multiple of 16 in 16..1024");
   if (p->batch < 16 || p->sample_cap < 0 || p->lr <= 0.0f)
     return fail(GD_ERR_INVALID, "bad batch / sample_cap / lr");
+  if (p->hidden != 128 && p->hidden != 256)
+    return fail(GD_ERR_INVALID, "delayed-acceptance steps run the network fused: hidden must be "
+                                "128 or 256");
   CK(cudaSetDevice(c->device));
+  if (gd::da_prepare(p->hidden)) return fail(GD_ERR_CUDA, "front kernel attributes");
   CK(cudaStreamSynchronize(c->stream));
   da_free(c);
   DaState *d = new DaState();
@@ -1876,15 +2095,20 @@ int gd_sur_create(gd_ctx *c, const gd_sur_params *p) {
   DA_TRY(da_alloc(d, &d->d_emb_base, c->n_complex));
   DA_TRY(da_alloc(d, &d->d_active, c->n_complex));
   DA_TRY(da_alloc(d, &d->d_pocket, pf.size()));
-  DA_TRY(da_alloc(d, &d->d_mm_prop, R * 6));
-  DA_TRY(da_alloc(d, &d->d_u1, R));
   DA_TRY(da_alloc(d, &d->d_u2, R));
   DA_TRY(da_alloc(d, &d->d_s_cur, R));
   DA_TRY(da_alloc(d, &d->d_s_new, R));
   DA_TRY(da_alloc(d, &d->d_pose_mm, R * 6));
   DA_TRY(da_alloc(d, &d->d_pose_rep, R));
   DA_TRY(da_alloc(d, &d->d_pose_lc, R));
-  DA_TRY(da_alloc(d, &d->d_pose_e, R));
+  DA_TRY(da_alloc(d, &d->d_prop, R));
+  DA_TRY(da_alloc(d, &d->d_pass, R));
+  DA_TRY(da_alloc(d, &d->d_plain, R));
+  DA_TRY(da_alloc(d, &d->d_acc, R));
+  DA_TRY(da_alloc(d, &d->d_plain_acc, R));
+  DA_TRY(da_alloc(d, &d->d_nerr, R));
+  DA_TRY(da_alloc(d, &d->d_err2, R));
+  DA_TRY(da_alloc(d, &d->d_epi, 1));
   DA_TRY(da_alloc(d, &d->d_stats, (size_t)c->n_complex * GD_DA_NSTAT));
   DA_TRY(da_alloc(d, &d->d_err, (size_t)c->n_complex * GD_DA_NERR));
   DA_TRY(da_alloc(d, &d->d_t, (size_t)rows));
@@ -1906,6 +2130,7 @@ int gd_sur_create(gd_ctx *c, const gd_sur_params *p) {
   rc = da_upload_active(c);
   if (!rc) rc = da_reset_counters(c);
   if (!rc) rc = da_build_groups(c);
+  if (!rc) rc = da_upload_epi(c);
   if (rc) {
     da_free(c);
     return rc;
@@ -2084,14 +2309,14 @@ int gd_da_trace_enable(gd_ctx *c, int step0, int max_steps) {
   da_free_trace(d);
   da_drop_graphs(c);
   d->tr_step0 = step0;
-  if (max_steps == 0) return GD_OK;
+  if (max_steps == 0) return da_upload_epi(c);
   const size_t n = (size_t)c->n_rep * max_steps;
   CK(cudaMalloc(&d->tr_s, sizeof(float) * n));
   CK(cudaMalloc(&d->tr_e, sizeof(float) * n));
   CK(cudaMalloc(&d->tr_flag, sizeof(int) * n));
   CK(cudaMemset(d->tr_flag, 0xff, sizeof(int) * n));
   d->tr_cap = max_steps;
-  return GD_OK;
+  return da_upload_epi(c);
 }
 
 int gd_da_trace_get(gd_ctx *c, float *s_new, float *e_new, int *outcome) {

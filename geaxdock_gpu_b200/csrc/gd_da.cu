@@ -1,30 +1,37 @@
 /*
  * gd_da.cu -- delayed-acceptance Monte Carlo steps around the exact energy kernel.
  *
- * One delayed-acceptance step of every replica is five launches on one stream (captured in a
+ * One delayed-acceptance step of every replica is two launches on one stream (captured in a
  * CUDA graph by the host):
- *   1. da_propose   the plain step's move and accept uniform (gd_draw_step, same Philox
- *                   counters as gd_mc_kernel), the surrogate-stage uniform, feature row
- *   2. mlp_forward  surrogate energy of every proposal (BF16 tensor-core MLP)
- *   3. da_stage1    surrogate Metropolis test u1 < exp(mb (S_new - S_cur)); survivors are
- *                   compacted per (complex, protein conformer) block and cut into tiles
- *   4. gd_mc_kernel mode 2: exact energies of the survivors only
- *   5. da_stage2    exact test u2 < exp(mb ((E_new - E_old) - (S_new - S_cur))), state
- *                   update, records
+ *   1. da_front     per CTA of 32 replicas: the plain step's move and accept uniform
+ *                   (gd_draw_step, the Philox counters of gd_mc_kernel), the surrogate-stage
+ *                   uniform, the feature rows in shared memory, the BF16 tensor-core network
+ *                   on them, the surrogate Metropolis test u1 < exp(mb (S_new - S_cur)), and
+ *                   the survivors' compaction into their (complex, protein conformer) group's
+ *                   pose slots
+ *   2. gd_mc_kernel mode 3: exact energies of the survivors only (tiles past a group's
+ *                   survivors exit at once) and, in its epilogue, the exact test
+ *                   u2 < exp(mb ((E_new - E_old) - (S_new - S_cur))), state update, records
  * The pair is a valid Metropolis-Hastings kernel for the exact distribution (Christen & Fox,
  * "Markov chain Monte Carlo using an approximation", J. Comput. Graph. Stat. 14, 2005) for
  * any fixed surrogate S. With the stage switched off for a complex, S_new = S_cur, every
- * proposal survives and stage 2 is bit-identical to the plain Metropolis test with the plain
- * step's uniform: the step reproduces gd_mc_kernel's trajectory exactly.
+ * proposal survives and the second test is bit-identical to the plain Metropolis test with
+ * the plain step's uniform: the step reproduces gd_mc_kernel's trajectory exactly.
+ * Survivors take their slots through an atomic counter per group, so the order of the slots
+ * varies between runs; a replica's energy does not depend on its slot (per-lane sums and
+ * per-slot reductions in a fixed order), so the chains do not either.
  */
 #include <cuda_bf16.h>
 
 #include "gd_mlp.cuh"
+#include "gd_mlp_fwd.cuh"
 #include "gd_numerics.h"
 
 namespace gd {
 
 namespace {
+
+using bf16 = __nv_bfloat16;
 
 __device__ __forceinline__ int cur_step(const GdDaDev &d, int step0) {
   return step0 + (d.step_base ? *d.step_base : 0);
@@ -52,9 +59,9 @@ __device__ void quat_of(const float r[9], float q[4]) {
   q[0] = sg * w; q[1] = sg * x; q[2] = sg * y; q[3] = sg * z;
 }
 
-/* one feature row (layout in gd_mlp.cuh); the embedding columns are left to mlp_embed */
-__device__ void write_features(const GdDaDev &d, int ci, int lc, const float mm[6],
-                               __nv_bfloat16 *row) {
+/* one feature row (layout in gd_mlp.cuh), 16-byte aligned; the embedding columns are written
+ * as 0 (the network fills them from its table) */
+__device__ void write_features(const GdDaDev &d, int ci, int lc, const float mm[6], bf16 *row) {
   const GdDevComplex &cx = d.cx[ci];
   float rot[9];
   gd_rotation(mm, rot);
@@ -75,7 +82,6 @@ __device__ void write_features(const GdDaDev &d, int ci, int lc, const float mm[
   f[55] = rot[0]; f[56] = rot[3]; f[57] = rot[6];
   f[58] = rot[1]; f[59] = rot[4]; f[60] = rot[7];
   f[61] = 0.125f * sqrtf(tx * tx + ty * ty + tz * tz);
-  /* 8 x 16-byte stores; the embedding columns [7, 39) are written as 0 here */
   uint4 *dst = reinterpret_cast<uint4 *>(row);
 #pragma unroll
   for (int v = 0; v < 8; ++v) {
@@ -91,31 +97,99 @@ __device__ void write_features(const GdDaDev &d, int ci, int lc, const float mm[
   }
 }
 
-__global__ void propose_kernel(GdDaDev d, int step0, int current) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= d.n_rep) return;
-  const int ci = d.rep_cx[r];
-  const GdDevComplex &cx = d.cx[ci];
-  const gd_replica rp = d.replica[r];
-  float mm[6];
+template <int NT>
+__global__ void __launch_bounds__(256) front_kernel(GdDaDev d, int mode, int step0, int *cnt,
+                                                    int r_begin, int r_end) {
+  using D = fwd::Dims<NT>;
+  constexpr int FR = fwd::FR;
+  extern __shared__ __align__(128) unsigned char fsm[];
+  __shared__ int cf[FR];
+  __shared__ float ys[FR];
+  bf16 *xs = reinterpret_cast<bf16 *>(fsm);
+  bf16 *act = xs + FR * D::LDX;
+  float *stg = reinterpret_cast<float *>(act + FR * D::LDA);
+  const int tid = threadIdx.x;
+  const int r = r_begin + blockIdx.x * FR + tid; /* the row's replica (threads < FR) */
+  const int step = cur_step(d, step0);
+  float mm[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+  float u1 = 0.0f, u2 = 0.0f;
+  int ci = 0, lc = 0;
+  if (tid < FR) {
+    bf16 *row = xs + tid * D::LDX;
+    if (r < r_end) {
+      ci = d.rep_cx[r];
+      const GdDevComplex &cx = d.cx[ci];
+      const gd_replica rp = d.replica[r];
+      lc = rp.idx_lig;
 #pragma unroll
-  for (int i = 0; i < 6; ++i) mm[i] = d.mm_old[(size_t)r * 6 + i];
-  if (!current) {
-    const int step = cur_step(d, step0);
-    const uint32_t rl = (uint32_t)(r - cx.rep_offset);
-    float delta[6], u;
-    gd_draw_step(d.seed, (uint32_t)cx.stream, rl, (uint32_t)step, d.move_kind, d.move_scale,
-                 delta, &u);
+      for (int i = 0; i < 6; ++i) mm[i] = d.mm_old[(size_t)r * 6 + i];
+      if (mode != GD_DA_CURRENT) {
+        const uint32_t rl = (uint32_t)(r - cx.rep_offset);
+        float delta[6];
+        gd_draw_step(d.seed, (uint32_t)cx.stream, rl, (uint32_t)step, d.move_kind, d.move_scale,
+                     delta, &u2);
+        u1 = gd_draw_stage1(d.seed, (uint32_t)cx.stream, rl, (uint32_t)step);
 #pragma unroll
-    for (int i = 0; i < 6; ++i) {
-      mm[i] = GD_ADD(mm[i], delta[i]);
-      d.mm_prop[(size_t)r * 6 + i] = mm[i];
+        for (int i = 0; i < 6; ++i) mm[i] = GD_ADD(mm[i], delta[i]);
+      }
+      write_features(d, ci, lc, mm, row);
+      cf[tid] = d.emb_base[ci] >= 0 ? d.emb_base[ci] + rp.idx_prt * cx.n_lig + lc : -1;
+    } else {
+      uint4 *dst = reinterpret_cast<uint4 *>(row);
+#pragma unroll
+      for (int v = 0; v < 8; ++v) dst[v] = make_uint4(0u, 0u, 0u, 0u);
+      cf[tid] = -1;
     }
-    d.u2[r] = u;
-    d.u1[r] = gd_draw_stage1(d.seed, (uint32_t)cx.stream, rl, (uint32_t)step);
   }
-  write_features(d, ci, rp.idx_lig, mm, d.X + (size_t)r * GD_MLP_IN);
-  d.conf[r] = d.emb_base[ci] + rp.idx_prt * cx.n_lig + rp.idx_lig;
+  __syncthreads();
+  if (mode != GD_DA_COLLECT) {
+    fwd::fill_embedding<NT>(xs, cf, d.theta, d.L, tid);
+    __syncthreads();
+    fwd::rows_forward<NT>(xs, act, stg, d.theta, d.wh, d.L, ys, tid);
+  }
+  if (tid >= FR || r >= r_end) return;
+  if (mode == GD_DA_CURRENT) {
+    d.s_cur[r] = __fmaf_rn(ys[tid], d.sigma, d.mu);
+    return;
+  }
+  const bool act_on = mode == GD_DA_STEP && d.active[ci];
+  float sn = d.s_cur[r];
+  int pass = 1;
+  if (act_on) {
+    sn = __fmaf_rn(ys[tid], d.sigma, d.mu);
+    const float mb = d.cx[ci].minus_beta[d.replica[r].idx_tmp];
+    pass = gd_metropolis(sn, d.s_cur[r], mb, u1);
+    d.prop[r] += 1;
+    d.pass[r] += pass;
+  } else {
+    d.plain[r] += 1;
+  }
+  d.s_new[r] = sn;
+  d.u2[r] = u2;
+  if (pass) {
+    const int g = d.rep_group[r];
+    const int pos = d.group_b0[g] + atomicAdd(cnt + g, 1);
+    d.pose_rep[pos] = r;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) d.pose_mm[(size_t)pos * 6 + i] = mm[i];
+    d.pose_lc[pos] = lc;
+  } else if (d.tr_flag) {
+    const int ti = step - d.tr_step0;
+    if (ti >= 0 && ti < d.tr_cap) {
+      const size_t o = (size_t)r * d.tr_cap + ti;
+      d.tr_s[o] = sn;
+      d.tr_e[o] = __int_as_float(0x7fc00000);
+      d.tr_flag[o] = 0;
+    }
+  }
+  if (mode == GD_DA_COLLECT && d.smp_cap > 0) {
+    const long long idx = ((long long)step * d.n_rep + r) % d.smp_cap;
+    const uint4 *src = reinterpret_cast<const uint4 *>(xs + tid * D::LDX);
+    uint4 *dst = reinterpret_cast<uint4 *>(d.smp_X + (size_t)idx * GD_MLP_IN);
+#pragma unroll
+    for (int v = 0; v < 8; ++v) dst[v] = src[v];
+    d.smp_conf[idx] = cf[tid];
+  }
 }
 
 __global__ void pose_features_kernel(GdDaDev d, int ci, int pc, int lc, const float *mm, int n) {
@@ -125,167 +199,51 @@ __global__ void pose_features_kernel(GdDaDev d, int ci, int pc, int lc, const fl
 #pragma unroll
   for (int k = 0; k < 6; ++k) m[k] = mm[(size_t)i * 6 + k];
   write_features(d, ci, lc, m, d.X + (size_t)i * GD_MLP_IN);
-  d.conf[i] = d.emb_base[ci] + pc * d.cx[ci].n_lig + lc;
+  d.conf[i] = d.emb_base[ci] >= 0 ? d.emb_base[ci] + pc * d.cx[ci].n_lig + lc : -1;
 }
 
-__global__ void set_current_kernel(GdDaDev d) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= d.n_rep) return;
-  d.s_cur[r] = __fmaf_rn(d.y[r], d.sigma, d.mu);
-}
-
-/* one CTA per group; block-wide stable compaction of the survivors */
-__global__ void __launch_bounds__(256) stage1_kernel(GdDaDev d, int step0, int collect) {
-  const GdGroup G = d.groups[blockIdx.x];
-  const GdDevComplex &cx = d.cx[G.ci];
-  const bool act = !collect && d.active[G.ci];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
-  __shared__ int wsum[8];
-  int base = 0;
-  const int step = cur_step(d, step0);
-  const int ti = step - d.tr_step0;
-  const bool trace = d.tr_flag && ti >= 0 && ti < d.tr_cap;
-  for (int i0 = 0; i0 < G.n; i0 += blockDim.x) {
-    const int i = i0 + tid, r = G.b0 + i;
-    int pass = 0;
-    if (i < G.n) {
-      pass = 1;
-      float sn = d.s_cur[r];
-      if (act) {
-        sn = __fmaf_rn(d.y[r], d.sigma, d.mu);
-        const float mb = cx.minus_beta[d.replica[r].idx_tmp];
-        pass = gd_metropolis(sn, d.s_cur[r], mb, d.u1[r]);
-      }
-      d.s_new[r] = sn;
-      if (trace && !pass) {
-        const size_t o = (size_t)r * d.tr_cap + ti;
-        d.tr_s[o] = sn;
-        d.tr_e[o] = __int_as_float(0x7fc00000);
-        d.tr_flag[o] = 0;
-      }
-    }
-    const unsigned bal = __ballot_sync(0xffffffffu, pass);
-    if (lane == 0) wsum[warp] = __popc(bal);
-    __syncthreads();
-    int pre = 0, tot = 0;
-    for (int w = 0; w < nw; ++w) {
-      const int v = wsum[w];
-      pre += w < warp ? v : 0;
-      tot += v;
-    }
-    if (pass) {
-      const int pos = G.b0 + base + pre + __popc(bal & ((1u << lane) - 1u));
-      d.pose_rep[pos] = r;
-#pragma unroll
-      for (int k = 0; k < 6; ++k) d.pose_mm[(size_t)pos * 6 + k] = d.mm_prop[(size_t)r * 6 + k];
-      d.pose_lc[pos] = d.replica[r].idx_lig;
-    }
-    base += tot;
-    __syncthreads(); /* wsum is rewritten by the next round */
+/* one CTA per complex, fixed-order sums over its replicas */
+__global__ void __launch_bounds__(256) stats_kernel(GdDaDev d, GdDaEpi e, const GdDevComplex *cxs,
+                                                    unsigned long long *stats, double *err) {
+  const GdDevComplex &cx = cxs[blockIdx.x];
+  __shared__ unsigned long long sh[5][256];
+  __shared__ double she[2][256];
+  unsigned long long v[5] = {0, 0, 0, 0, 0};
+  double w[2] = {0.0, 0.0};
+  for (int i = threadIdx.x; i < cx.n_rep; i += 256) {
+    const int r = cx.rep_offset + i;
+    v[0] += (unsigned long long)d.prop[r];
+    v[1] += (unsigned long long)d.pass[r];
+    v[2] += (unsigned long long)e.acc[r];
+    v[3] += (unsigned long long)d.plain[r];
+    v[4] += (unsigned long long)e.plain_acc[r];
+    w[0] += e.err2[r];
+    w[1] += (double)e.nerr[r];
   }
-  for (int i = tid; i < G.n_tiles; i += blockDim.x) {
-    GdTileDesc t;
-    t.complex_index = G.ci;
-    t.prt_conf = G.pc;
-    t.rep_begin = G.b0 + i * G.k;
-    t.count = max(0, min(G.k, base - i * G.k));
-    d.tiles[G.tile_base + i] = t;
-  }
-  if (tid == 0) {
-    d.group_cnt[blockIdx.x] = base;
-    unsigned long long *st = d.stats + (size_t)G.ci * GD_DA_NSTAT;
-    if (act) {
-      atomicAdd(st + GD_DA_PROPOSED, (unsigned long long)G.n);
-      atomicAdd(st + GD_DA_PASSED, (unsigned long long)base);
-    } else {
-      atomicAdd(st + GD_DA_PLAIN, (unsigned long long)G.n);
-    }
-  }
-}
-
-__global__ void __launch_bounds__(256) stage2_kernel(GdDaDev d, int step0, int collect) {
-  const GdGroup G = d.groups[blockIdx.x];
-  const GdDevComplex &cx = d.cx[G.ci];
-  const bool act = !collect && d.active[G.ci];
-  const int cnt = d.group_cnt[blockIdx.x];
-  const int tid = threadIdx.x;
-  const int step = cur_step(d, step0);
-  const int ti = step - d.tr_step0;
-  const bool trace = d.tr_flag && ti >= 0 && ti < d.tr_cap;
-  int nacc = 0;
-  double e2 = 0.0;
-  for (int i = tid; i < cnt; i += blockDim.x) {
-    const int pos = G.b0 + i, r = d.pose_rep[pos];
-    const gd_energy en = d.pose_e[pos];
-    const float enew = en.e[GD_MAXWEI - 1];
-    const float eold = d.e_old[r].e[GD_MAXWEI - 1];
-    const gd_replica rp = d.replica[r];
-    const float mb = cx.minus_beta[rp.idx_tmp];
-    const float sn = d.s_new[r], so = d.s_cur[r];
-    const int acc = gd_da_stage2(enew, eold, sn, so, mb, d.u2[r]);
-    if (act) {
-      const double e = (double)sn - (double)enew;
-      e2 += e * e;
-    }
-    if (collect && d.smp_cap > 0) {
-      const long long idx = ((long long)step * d.n_rep + r) % d.smp_cap;
-      const uint4 *src = reinterpret_cast<const uint4 *>(d.X + (size_t)r * GD_MLP_IN);
-      uint4 *dst = reinterpret_cast<uint4 *>(d.smp_X + (size_t)idx * GD_MLP_IN);
+  const int t = threadIdx.x;
 #pragma unroll
-      for (int v = 0; v < 8; ++v) dst[v] = src[v];
-      d.smp_conf[idx] = d.conf[r];
-      d.smp_t[idx] = enew;
-    }
-    if (trace) {
-      const size_t o = (size_t)r * d.tr_cap + ti;
-      d.tr_s[o] = sn;
-      d.tr_e[o] = enew;
-      d.tr_flag[o] = 1 + acc;
-    }
-    if (acc) {
-      ++nacc;
-      d.e_old[r] = en;
-      d.etotal[r] = enew;
-#pragma unroll
-      for (int k = 0; k < 6; ++k) d.mm_old[(size_t)r * 6 + k] = d.pose_mm[(size_t)pos * 6 + k];
-      d.n_accept[r] += 1;
-      d.s_cur[r] = sn;
-      if (d.rec) {
-        const int kslot = d.rec_next[r];
-        if (kslot < d.rec_cap) {
-          gd_record_step *q = d.rec + (size_t)r * d.rec_cap + kslot;
-          q->replica = rp;
-          q->energy = en;
-#pragma unroll
-          for (int k = 0; k < 6; ++k) q->movematrix[k] = d.pose_mm[(size_t)pos * 6 + k];
-          q->step = step;
-          d.rec_next[r] = kslot + 1;
-        } else {
-          atomicOr(d.errw, GD_DEV_ERR_RECORD_FULL);
-        }
-      }
-    }
-  }
-  /* block totals, fixed order */
-  __shared__ int s_acc[256];
-  __shared__ double s_e2[256];
-  s_acc[tid] = nacc;
-  s_e2[tid] = e2;
+  for (int k = 0; k < 5; ++k) sh[k][t] = v[k];
+  she[0][t] = w[0];
+  she[1][t] = w[1];
   __syncthreads();
-  for (int o = blockDim.x >> 1; o > 0; o >>= 1) {
-    if (tid < o) {
-      s_acc[tid] += s_acc[tid + o];
-      s_e2[tid] += s_e2[tid + o];
+  for (int o = 128; o > 0; o >>= 1) {
+    if (t < o) {
+#pragma unroll
+      for (int k = 0; k < 5; ++k) sh[k][t] += sh[k][t + o];
+      she[0][t] += she[0][t + o];
+      she[1][t] += she[1][t + o];
     }
     __syncthreads();
   }
-  if (tid == 0) {
-    unsigned long long *st = d.stats + (size_t)G.ci * GD_DA_NSTAT;
-    atomicAdd(st + (act ? GD_DA_ACCEPTED : GD_DA_PLAIN_ACC), (unsigned long long)s_acc[0]);
-    if (act && cnt) {
-      atomicAdd(d.err + (size_t)G.ci * GD_DA_NERR, s_e2[0]);
-      atomicAdd(d.err + (size_t)G.ci * GD_DA_NERR + 1, (double)cnt);
-    }
+  if (t == 0) {
+    unsigned long long *st = stats + (size_t)blockIdx.x * GD_DA_NSTAT;
+    st[GD_DA_PROPOSED] = sh[0][0];
+    st[GD_DA_PASSED] = sh[1][0];
+    st[GD_DA_ACCEPTED] = sh[2][0];
+    st[GD_DA_PLAIN] = sh[3][0];
+    st[GD_DA_PLAIN_ACC] = sh[4][0];
+    err[(size_t)blockIdx.x * GD_DA_NERR] = she[0][0];
+    err[(size_t)blockIdx.x * GD_DA_NERR + 1] = she[1][0];
   }
 }
 
@@ -338,8 +296,27 @@ inline int nblk(long long n, int t) { return (int)((n + t - 1) / t); }
 
 }  // namespace
 
-void da_propose(const GdDaDev &d, int step0, bool current, cudaStream_t s) {
-  propose_kernel<<<nblk(d.n_rep, 128), 128, 0, s>>>(d, step0, current ? 1 : 0);
+int da_prepare(int hidden) {
+  if (hidden == 128)
+    return cudaFuncSetAttribute(front_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)fwd::Dims<1>::smem) == cudaSuccess ? 0 : -2;
+  if (hidden == 256)
+    return cudaFuncSetAttribute(front_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)fwd::Dims<2>::smem) == cudaSuccess ? 0 : -2;
+  return -1;
+}
+
+int da_front(const GdDaDev &d, int mode, int step0, int *cnt, int r_begin, int r_end,
+             cudaStream_t s) {
+  if (r_end <= r_begin) return 0;
+  const int grid = nblk(r_end - r_begin, fwd::FR);
+  if (d.L.hidden == 128)
+    front_kernel<1><<<grid, 256, fwd::Dims<1>::smem, s>>>(d, mode, step0, cnt, r_begin, r_end);
+  else if (d.L.hidden == 256)
+    front_kernel<2><<<grid, 256, fwd::Dims<2>::smem, s>>>(d, mode, step0, cnt, r_begin, r_end);
+  else
+    return -1; /* the fused step needs H = 128 or 256 */
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
 void da_pose_features(const GdDaDev &d, int ci, int pc, int lc, const float *mm, int n,
@@ -347,16 +324,9 @@ void da_pose_features(const GdDaDev &d, int ci, int pc, int lc, const float *mm,
   pose_features_kernel<<<nblk(n, 128), 128, 0, s>>>(d, ci, pc, lc, mm, n);
 }
 
-void da_set_current(const GdDaDev &d, cudaStream_t s) {
-  set_current_kernel<<<nblk(d.n_rep, 256), 256, 0, s>>>(d);
-}
-
-void da_stage1(const GdDaDev &d, int step0, bool collect, cudaStream_t s) {
-  stage1_kernel<<<d.n_groups, 256, 0, s>>>(d, step0, collect ? 1 : 0);
-}
-
-void da_stage2(const GdDaDev &d, int step0, bool collect, cudaStream_t s) {
-  stage2_kernel<<<d.n_groups, 256, 0, s>>>(d, step0, collect ? 1 : 0);
+void da_stats(const GdDaDev &d, const GdDaEpi &e_host, const GdDevComplex *cx_dev, int n_complex,
+              unsigned long long *stats, double *err, cudaStream_t s) {
+  stats_kernel<<<n_complex, 256, 0, s>>>(d, e_host, cx_dev, stats, err);
 }
 
 void da_gather(const GdDaDev &d, long long start, long long n_valid, int rows, int iter,

@@ -85,6 +85,27 @@ struct GdForceConst {
   float hpl0[GD_MAXTP2], hpl1[GD_MAXTP2], hpl2[GD_MAXTP2];
 };
 
+/* Delayed-acceptance state read by the exact kernel in mode 3 (device-resident). Survivors of
+ * the surrogate stage are compacted per (complex, protein conformer) group into pose slots
+ * [group_b0[g], group_b0[g] + count[g]); pose_rep maps a slot to its replica. */
+struct GdDaEpi {
+  const int *group_b0;        /* [n_groups] */
+  int n_groups, n_rep;
+  const int *pose_rep;        /* [n_rep] */
+  const float *s_new;         /* [n_rep] surrogate energy of the proposal */
+  float *s_cur;               /* [n_rep] surrogate energy of the current pose */
+  const float *u2;            /* [n_rep] final accept uniform (the plain step's) */
+  const int *active;          /* [n_complex] surrogate stage on */
+  int *acc, *plain_acc;       /* [n_rep] accepted moves with the stage on / off */
+  double *err2;               /* [n_rep] sum of (S_new - E_new)^2 with the stage on */
+  int *nerr;                  /* [n_rep] its count */
+  float *smp_t;               /* [smp_cap] training targets (collect steps) */
+  long long smp_cap;
+  float *tr_s, *tr_e;         /* decision trace, [n_rep*tr_cap] or null */
+  int *tr_flag;
+  int tr_cap, tr_step0;
+};
+
 /* Arguments of the fused Monte Carlo / energy kernel. */
 struct GdMcArgs {
   const GdDevComplex *cx;     /* [n_complex] */
@@ -92,7 +113,8 @@ struct GdMcArgs {
   const GdTileDesc *tiles;    /* [n_tiles] */
   int n_tiles;
   int *tile_counter;          /* persistent-CTA work queue head */
-  int mode;                   /* 0: MC steps, 1: init (energy at movematrix 0), 2: eval poses */
+  int mode;                   /* 0: MC steps, 1: init (energy at movematrix 0), 2: eval poses,
+                                 3: delayed-acceptance exact stage (eval + decision) */
   int n_steps;                /* steps in this launch (mode 0) */
   int step0;                  /* step number of the first step (s1 + s2), added to *step_base */
   const int *step_base;       /* device cursor for graph replays (null: 0) */
@@ -120,6 +142,13 @@ struct GdMcArgs {
   gd_energy *e_out;
   unsigned *err;              /* device error word */
   long long timeout_ns;       /* bounded waits */
+  /* mode 3: tile.count holds (group << 8) | capacity; the survivors come from da_cnt */
+  const GdDaEpi *da;
+  const int *da_cnt;          /* [n_groups] survivors this step */
+  int *da_cnt_next;           /* [n_groups] the next step's counters; block 0 zeroes the
+                                 range [da_g0, da_g1) this launch serves */
+  int da_g0, da_g1;
+  int da_collect;             /* collect step: stage off everywhere, targets stored */
 };
 
 #endif

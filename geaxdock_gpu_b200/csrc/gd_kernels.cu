@@ -266,6 +266,60 @@ __device__ __forceinline__ void pair_dispatch(int kind, const float4 *PA, const 
 #undef GD_PR
 }
 
+/* Delayed acceptance, second stage, for the survivor in pose slot `pos` (mode 3): the
+ * corrected Metropolis test u2 < exp(mb ((E_new - E_old) - (S_new - S_cur))) (gd_da_stage2),
+ * surrogate-error sums, the collect step's training target, the trace, and on acceptance the
+ * state update and the record, as the plain epilogue does them. */
+__device__ __forceinline__ void da_decide(const GdMcArgs &a, const GdDevComplex &cx, int ci, int pos,
+                                       const gd_energy &en, const float *mm_new, int step) {
+  const GdDaEpi &da = *a.da;
+  const int r = da.pose_rep[pos];
+  const gd_replica rp = a.replica[r];
+  const float mb = cx.minus_beta[rp.idx_tmp];
+  const float enew = en.e[GD_MAXWEI - 1];
+  const float sn = da.s_new[r], so = da.s_cur[r];
+  const int acc = gd_da_stage2(enew, a.e_old[r].e[GD_MAXWEI - 1], sn, so, mb, da.u2[r]);
+  const bool active = !a.da_collect && da.active[ci];
+  if (active) {
+    const double e = (double)sn - (double)enew;
+    da.err2[r] += e * e;
+    da.nerr[r] += 1;
+  }
+  if (a.da_collect && da.smp_cap > 0)
+    da.smp_t[((long long)step * da.n_rep + r) % da.smp_cap] = enew;
+  if (da.tr_flag) {
+    const int ti = step - da.tr_step0;
+    if (ti >= 0 && ti < da.tr_cap) {
+      const size_t o = (size_t)r * da.tr_cap + ti;
+      da.tr_s[o] = sn;
+      da.tr_e[o] = enew;
+      da.tr_flag[o] = 1 + acc;
+    }
+  }
+  if (!acc) return;
+  a.e_old[r] = en;
+  a.etotal[r] = enew;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) a.mm_old[(size_t)r * 6 + i] = mm_new[i];
+  a.n_accept[r] += 1;
+  da.s_cur[r] = sn;
+  if (active) da.acc[r] += 1; else da.plain_acc[r] += 1;
+  if (a.rec) {
+    const int kslot = a.rec_next[r];
+    if (kslot < a.rec_cap) {
+      gd_record_step *q = a.rec + (size_t)r * a.rec_cap + kslot;
+      q->replica = rp;
+      q->energy = en;
+#pragma unroll
+      for (int i = 0; i < 6; ++i) q->movematrix[i] = mm_new[i];
+      q->step = step;
+      a.rec_next[r] = kslot + 1;
+    } else {
+      atomicOr(a.err, GD_DEV_ERR_RECORD_FULL);
+    }
+  }
+}
+
 /*
  * Shared memory: two mbarriers, two protein buffers of D points (float4 + float2), the
  * placed atoms, NQ FP64 partials per lane, the slots. The protein buffers form a two-stage
@@ -303,6 +357,8 @@ __global__ void __launch_bounds__(GD_MAX_TPB, GD_MIN_BLOCKS(UNROLL))
   uint32_t consumed0 = 0, consumed1 = 0; /* completed phases waited for, per buffer */
   const int step_first = a.step0 + (a.step_base ? *a.step_base : 0);
   const int warp = tid >> 5, lane = tid & 31, nwarps = T >> 5;
+  if (a.mode == 3 && blockIdx.x == 0)
+    for (int g = a.da_g0 + tid; g < a.da_g1; g += T) a.da_cnt_next[g] = 0;
 
   for (;;) {
     if (tid == 0) s_tile = atomicAdd(a.tile_counter, 1);
@@ -310,14 +366,20 @@ __global__ void __launch_bounds__(GD_MAX_TPB, GD_MIN_BLOCKS(UNROLL))
     const int t = s_tile;
     if (t >= a.n_tiles || s_abort) break;
     const GdTileDesc tile = a.tiles[t];
-    if (tile.count <= 0) {
+    int k = tile.count;
+    if (a.mode == 3) {
+      /* slot (group, capacity): the survivors of the group past this tile's first slot */
+      const int g = tile.count >> 8, cap = tile.count & 255;
+      k = max(0, min(cap, a.da_cnt[g] - (tile.rep_begin - a.da->group_b0[g])));
+    }
+    if (k <= 0) {
       /* an empty tile (a delayed-acceptance block with fewer survivors than tiles): no copy
        * issued, nothing to wait for; the barrier keeps s_tile until every thread read it */
       __syncthreads();
       continue;
     }
     const GdDevComplex &cx = a.cx[tile.complex_index];
-    const int L = cx.lna, k = tile.count;
+    const int L = cx.lna;
     const bool active = tid < k * L;
     const int j = active ? tid / L : 0;
     const int l = active ? tid - j * L : 0;
@@ -328,7 +390,7 @@ __global__ void __launch_bounds__(GD_MAX_TPB, GD_MIN_BLOCKS(UNROLL))
       const int id = tile.rep_begin + tid;
       s.rep = id;
       s.accept = 0;
-      if (a.mode == 2) {
+      if (a.mode >= 2) {
         s.lig_conf = a.lig_conf_in[id];
       } else {
         s.replica = a.replica[id];
@@ -392,7 +454,7 @@ __global__ void __launch_bounds__(GD_MAX_TPB, GD_MIN_BLOCKS(UNROLL))
                        (uint32_t)(step_first + s), a.move_kind, a.move_scale, delta, &u);
 #pragma unroll
           for (int i = 0; i < 6; ++i) mmn[i] = GD_ADD(sl.mm_old[i], delta[i]);
-        } else if (a.mode == 2) {
+        } else if (a.mode >= 2) {
 #pragma unroll
           for (int i = 0; i < 6; ++i) mmn[i] = a.mm_in[(size_t)sl.rep * 6 + i];
         } else {
@@ -592,6 +654,8 @@ __global__ void __launch_bounds__(GD_MAX_TPB, GD_MIN_BLOCKS(UNROLL))
           const int rid = sl.rep;
           if (a.mode == 2) {
             a.e_out[rid] = en;
+          } else if (a.mode == 3) {
+            da_decide(a, cx, tile.complex_index, rid, en, sl.mm_new, step_first + s);
           } else {
             int acc = 1;
             if (a.mode == 0)
@@ -643,7 +707,7 @@ __global__ void __launch_bounds__(GD_MAX_TPB, GD_MIN_BLOCKS(UNROLL))
     }
 
     /* ---- write back replica state ---- */
-    if (a.mode != 2 && tid < k) {
+    if (a.mode < 2 && tid < k) {
       const Slot &sl = slots[tid];
       a.e_old[sl.rep] = sl.e_old;
       a.etotal[sl.rep] = sl.e_old.e[GD_MAXWEI - 1];
@@ -661,13 +725,14 @@ template __global__ void gd_mc_kernel<1>(GdMcArgs, GdForceConst);
 template __global__ void gd_mc_kernel<2>(GdMcArgs, GdForceConst);
 template __global__ void gd_mc_kernel<4>(GdMcArgs, GdForceConst);
 
-/* ExchangeReplicas_d, one thread per (complex, protein conformer, ligand conformer) group. */
+/* ExchangeReplicas_d, one thread per (complex, protein conformer, ligand conformer) group of
+ * the range [g_begin, g_end). */
 __global__ void gd_exchange_kernel(const GdDevComplex *cxs, const int *group_base, int n_complex,
-                                   int n_groups, gd_replica *replica, const float *etotal,
-                                   int *acs, uint64_t seed, const int *call_base, int call_off,
-                                   int mode_t) {
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= n_groups || mode_t >= 2) return;
+                                   int g_begin, int g_end, gd_replica *replica,
+                                   const float *etotal, int *acs, uint64_t seed,
+                                   const int *call_base, int call_off, int mode_t) {
+  const int g = g_begin + blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= g_end || mode_t >= 2) return;
   int lo = 0, hi = n_complex - 1;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;

@@ -16,6 +16,7 @@
 #include <cmath>
 
 #include "gd_mlp.cuh"
+#include "gd_mlp_fwd.cuh"
 #include "gd_numerics.h"
 
 namespace gd {
@@ -241,71 +242,22 @@ __global__ void init_uniform(float *p, size_t n, float scale, uint32_t tensor, u
   p[i] = scale * gd_sym11(r.v[0]);
 }
 
-/* The whole forward pass of FR rows in one CTA of 8 warps: the rows (embedding columns filled
- * from the FP32 table) in shared memory, three BF16 tensor-core layers whose FP32 accumulators
- * are staged through shared memory for bias + SiLU, and the output dot product. Weight
- * fragments come straight from global memory (L2-resident). Per output element the MMA
- * sequence, the bias/SiLU arithmetic and the output reduction order are those of the layered
- * path (wmma_gemm, bias_silu, out_layer), so both paths give the same bits. */
-constexpr int FR = 64;
-
-template <int NT> /* 16-column tiles per warp: H = 128 * NT */
-struct FusedDims {
-  static constexpr int H = 128 * NT, LDX = GD_MLP_IN + 8, LDA = H + 8, LDS = H + 4;
-  static constexpr size_t smem = (size_t)FR * LDX * 2 + (size_t)FR * LDA * 2 + (size_t)FR * LDS * 4;
-};
-
-template <int NT>
-__device__ __forceinline__ void fused_layer(const bf16 *A, int lda, int K, const bf16 *__restrict__ W,
-                                            const float *__restrict__ bias, bf16 *act, float *stg,
-                                            int warp, int tid) {
-  using namespace nvcuda;
-  using D = FusedDims<NT>;
-  wmma::fragment<wmma::accumulator, 16, 16, 16, float> acc[4][NT];
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < NT; ++j) wmma::fill_fragment(acc[i][j], 0.0f);
-  for (int k = 0; k < K; k += 16) {
-    wmma::fragment<wmma::matrix_b, 16, 16, 16, bf16, wmma::row_major> b[NT];
-#pragma unroll
-    for (int j = 0; j < NT; ++j)
-      wmma::load_matrix_sync(b[j], W + (size_t)k * D::H + (warp * NT + j) * 16, D::H);
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      wmma::fragment<wmma::matrix_a, 16, 16, 16, bf16, wmma::row_major> a;
-      wmma::load_matrix_sync(a, A + i * 16 * lda + k, lda);
-#pragma unroll
-      for (int j = 0; j < NT; ++j) wmma::mma_sync(acc[i][j], a, b[j], acc[i][j]);
-    }
-  }
-  __syncthreads(); /* every warp is done reading A before act is rewritten below */
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < NT; ++j)
-      wmma::store_matrix_sync(stg + i * 16 * D::LDS + (warp * NT + j) * 16, acc[i][j], D::LDS,
-                              wmma::mem_row_major);
-  __syncthreads();
-  for (int e = tid; e < FR * D::H; e += 256) {
-    const int r = e / D::H, c = e - r * D::H;
-    act[r * D::LDA + c] = __float2bfloat16_rn(silu(stg[r * D::LDS + c] + bias[c]));
-  }
-  __syncthreads();
-}
-
+/* The whole forward pass of fwd::FR rows in one CTA of 8 warps (gd_mlp_fwd.cuh). */
 template <int NT>
 __global__ void __launch_bounds__(256) fused_forward(const bf16 *__restrict__ X,
                                                      const int *__restrict__ conf,
                                                      const float *__restrict__ theta,
                                                      const bf16 *__restrict__ wh, MlpLayout L,
                                                      int rows, float *__restrict__ y) {
-  using D = FusedDims<NT>;
+  using D = fwd::Dims<NT>;
+  constexpr int FR = fwd::FR;
   extern __shared__ __align__(128) unsigned char fsm[];
+  __shared__ int cf[FR];
+  __shared__ float ys[FR];
   bf16 *xs = reinterpret_cast<bf16 *>(fsm);
   bf16 *act = xs + FR * D::LDX;
   float *stg = reinterpret_cast<float *>(act + FR * D::LDA);
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int tid = threadIdx.x;
   const int row0 = blockIdx.x * FR;
   for (int i = tid; i < FR * 8; i += 256) {
     const int r = i >> 3, c = i & 7;
@@ -313,31 +265,17 @@ __global__ void __launch_bounds__(256) fused_forward(const bf16 *__restrict__ X,
     if (row0 + r < rows) v = reinterpret_cast<const uint4 *>(X + (size_t)(row0 + r) * GD_MLP_IN)[c];
     *reinterpret_cast<uint4 *>(xs + r * D::LDX + c * 8) = v;
   }
+  if (tid < FR) cf[tid] = row0 + tid < rows ? conf[row0 + tid] : -1;
   __syncthreads();
-  if (L.n_emb) {
-    for (int i = tid; i < FR * GD_MLP_EMB; i += 256) {
-      const int r = i / GD_MLP_EMB, c = i - r * GD_MLP_EMB;
-      if (row0 + r < rows) {
-        const int e = conf[row0 + r];
-        if (e >= 0)
-          xs[r * D::LDX + GD_MLP_EMB_OFF + c] =
-              __float2bfloat16_rn(theta[L.emb + (size_t)e * GD_MLP_EMB + c]);
-      }
-    }
-    __syncthreads();
-  }
-  fused_layer<NT>(xs, D::LDX, GD_MLP_IN, wh + L.w1, theta + L.b1, act, stg, warp, tid);
-  fused_layer<NT>(act, D::LDA, D::H, wh + L.w2, theta + L.b2, act, stg, warp, tid);
-  fused_layer<NT>(act, D::LDA, D::H, wh + L.w3, theta + L.b3, act, stg, warp, tid);
-  const float *w4 = theta + L.w4;
-  for (int r = warp; r < FR; r += 8) {
-    float s = 0.0f;
-    for (int j = lane; j < D::H; j += 32) s += __bfloat162float(act[r * D::LDA + j]) * w4[j];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-    if (lane == 0 && row0 + r < rows) y[row0 + r] = s + theta[L.b4];
-  }
+  fwd::fill_embedding<NT>(xs, cf, theta, L, tid);
+  __syncthreads();
+  fwd::rows_forward<NT>(xs, act, stg, theta, wh, L, ys, tid);
+  if (tid < FR && row0 + tid < rows) y[row0 + tid] = ys[tid];
 }
+
+constexpr int FR = fwd::FR;
+template <int NT>
+using FusedDims = fwd::Dims<NT>;
 
 inline int blocks(size_t n, int t = 256) { return (int)((n + t - 1) / t); }
 

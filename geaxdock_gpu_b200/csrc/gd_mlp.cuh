@@ -85,14 +85,14 @@ int mlp_refresh_bf16(Mlp &n, cudaStream_t s);
 /* ---------------- delayed acceptance (gd_da.cu) ---------------- */
 
 /* One (complex, protein conformer) block of replicas: the unit of survivor compaction. Its
- * tiles occupy the fixed positions [tile_base, tile_base + n_tiles) of the stage-2 tile list;
- * tiles past the survivors get count 0. */
+ * tiles occupy the fixed positions [tile_base, tile_base + n_tiles) of the exact kernel's tile
+ * list; their counts come from the group's survivor counter at run time. */
 struct GdGroup {
   int ci, pc, b0, n;          /* complex, protein conformer, first replica, replicas */
   int tile_base, n_tiles, k, pad;
 };
 
-/* per-complex counters (unsigned long long): */
+/* per-complex statistics (reduced from per-replica counters by da_stats) */
 #define GD_DA_PROPOSED 0      /* proposals seen with the surrogate stage on */
 #define GD_DA_PASSED 1        /* ... that passed the surrogate stage */
 #define GD_DA_ACCEPTED 2      /* ... that the exact energy then accepted */
@@ -102,47 +102,44 @@ struct GdGroup {
 /* per-complex double sums: squared surrogate error and its count over exact evaluations */
 #define GD_DA_NERR 2
 
+/* front kernel modes */
+#define GD_DA_STEP 0          /* proposal, surrogate stage, compaction */
+#define GD_DA_COLLECT 1       /* proposal, every proposal passes, feature rows to the samples */
+#define GD_DA_CURRENT 2       /* surrogate of the current poses -> s_cur */
+
 struct GdDaDev {
   const GdDevComplex *cx;
   const int *rep_cx;          /* [n_rep] complex of each replica */
-  const int *emb_base;        /* [n_complex] first embedding row of the complex */
+  const int *rep_group;       /* [n_rep] compaction group of each replica */
+  const int *group_b0;        /* [n_groups] first replica (= first pose slot) of each group */
+  const int *emb_base;        /* [n_complex] first embedding row of the complex (< 0: none) */
   const float *pocket_feat;   /* [n_complex*16] */
   const int *active;          /* [n_complex] 1: surrogate stage on */
-  const GdGroup *groups;
-  int n_groups, n_rep;
+  int n_rep;
   /* replica state (the plain engine's arrays) */
-  gd_replica *replica;
-  float *mm_old;
-  gd_energy *e_old;
-  float *etotal;
-  int *n_accept;
-  gd_record_step *rec;
-  int *rec_next;
-  int rec_cap;
+  const gd_replica *replica;
+  const float *mm_old;
   /* per step */
-  float *mm_prop;             /* [n_rep*6] proposed movematrix */
   float *u2;                  /* [n_rep] final accept uniform (the plain step's) */
-  float *u1;                  /* [n_rep] surrogate-stage uniform */
   float *s_cur, *s_new;       /* [n_rep] surrogate energy at the current / proposed pose */
   int *pose_rep;              /* [n_rep] survivors, compacted per group */
   float *pose_mm;             /* [n_rep*6] */
   int *pose_lc;               /* [n_rep] */
-  gd_energy *pose_e;          /* [n_rep] exact energies of the survivors */
-  GdTileDesc *tiles;          /* [sum n_tiles] */
-  int *group_cnt;             /* [n_groups] survivors */
-  /* network rows */
-  __nv_bfloat16 *X;           /* [>= n_rep rows * 64] */
-  int *conf;
-  const float *y;
+  /* per-replica counters */
+  int *prop, *pass, *plain;
+  /* the network */
+  const float *theta;
+  const __nv_bfloat16 *wh;
+  MlpLayout L;
   float mu, sigma;
-  unsigned long long *stats;  /* [n_complex*GD_DA_NSTAT] */
-  double *err;                /* [n_complex*GD_DA_NERR] */
-  /* training samples (collect mode), ring of smp_cap rows */
+  __nv_bfloat16 *X;           /* global feature rows (surrogate predictions of given poses) */
+  int *conf;
+  /* training samples, ring of smp_cap rows */
   __nv_bfloat16 *smp_X;
   int *smp_conf;
   float *smp_t;
   long long smp_cap;
-  /* decision trace (replay checks), [n_rep*tr_cap] */
+  /* decision trace, [n_rep*tr_cap] or null */
   float *tr_s, *tr_e;
   int *tr_flag;
   int tr_cap, tr_step0;
@@ -151,21 +148,23 @@ struct GdDaDev {
   int move_kind;
   float move_scale[6];
   const int *step_base;       /* device step cursor */
-  unsigned *errw;             /* device error word */
 };
 
-/* proposal (or, with current = true, the current pose) of every replica -> mm_prop, u1, u2,
- * and its feature row in X / conf */
-void da_propose(const GdDaDev &d, int step0, bool current, cudaStream_t s);
+/* Front kernel of one delayed-acceptance step (mode GD_DA_*) for replicas [r_begin, r_end):
+ * the plain step's proposal and accept uniform (same Philox counters as gd_mc_kernel), the
+ * surrogate-stage uniform, the feature rows, the network on them, the surrogate Metropolis
+ * test and the survivors' compaction into their group's pose slots (cnt[group] survivors). */
+int da_front(const GdDaDev &d, int mode, int step0, int *cnt, int r_begin, int r_end,
+             cudaStream_t s);
+/* kernel attributes of da_front for a hidden width (call once per device, outside capture) */
+int da_prepare(int hidden);
 /* feature rows 0..n-1 of X / conf for n poses of one (complex, protein, ligand conformer) */
 void da_pose_features(const GdDaDev &d, int ci, int pc, int lc, const float *mm, int n,
                       cudaStream_t s);
-/* s_cur = surrogate of the rows (after a forward over the current poses) */
-void da_set_current(const GdDaDev &d, cudaStream_t s);
-/* surrogate stage and survivor compaction; collect: every proposal passes (plain step) */
-void da_stage1(const GdDaDev &d, int step0, bool collect, cudaStream_t s);
-/* exact stage on the survivors' energies, state update, records, samples when collect */
-void da_stage2(const GdDaDev &d, int step0, bool collect, cudaStream_t s);
+/* per-complex sums of the per-replica counters (one CTA per complex, fixed order):
+ * stats[ci*GD_DA_NSTAT + k], err[ci*GD_DA_NERR + k] */
+void da_stats(const GdDaDev &d, const GdDaEpi &e_host, const GdDevComplex *cx_dev, int n_complex,
+              unsigned long long *stats, double *err, cudaStream_t s);
 /* training batch: rows drawn from the sample ring into X / conf / t (normalised, clipped) */
 void da_gather(const GdDaDev &d, long long start, long long n_valid, int rows, int iter,
                float *t, cudaStream_t s);

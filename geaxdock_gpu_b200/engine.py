@@ -69,6 +69,7 @@ def lib() -> C.CDLL:
         "gd_trace_get": [vp, fp, ip, ip],
         "gd_get_stream": [vp, C.POINTER(vp)],
         "gd_set_rng_stream": [vp, C.c_int, C.c_int],
+        "gd_set_concurrency": [vp, C.c_int, C.c_int],
         "gd_set_wait_timeout": [vp, C.c_longlong],
         "gd_sur_create": [vp, C.POINTER(abi.SurParams)],
         "gd_sur_collect": [vp, C.c_int, C.c_int, C.c_int],
@@ -195,6 +196,9 @@ class Engine:
         s = C.c_void_p()
         check(lib().gd_get_stream(self.h, C.byref(s)))
         return s.value or 0
+
+    def set_concurrency(self, plain_chains: int, da_chains: int = 3):
+        check(lib().gd_set_concurrency(self.h, plain_chains, da_chains))
 
     def set_rng_stream(self, complex_index: int, stream: int):
         check(lib().gd_set_rng_stream(self.h, complex_index, stream))

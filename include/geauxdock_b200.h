@@ -206,6 +206,12 @@ int gd_get_tile(const gd_ctx *ctx, int complex_index, gd_tile *tile);
  * ms_out[i] per candidate (may be null). */
 int gd_autotune(gd_ctx *ctx, const gd_tile *candidates, int n_candidates, int repeats,
                 gd_tile *best, float *ms_out);
+/* Independent replica chains that gd_mc_run_fused (default 1) and the delayed-acceptance loops
+ * (default 3) run concurrently on separate streams of one CUDA graph: a chain is a contiguous
+ * range of (complex, protein conformer) blocks, so chains share no replica or exchange group,
+ * and one chain's kernels fill the other's last wave and launch gaps. Results do not depend on
+ * the numbers. */
+int gd_set_concurrency(gd_ctx *ctx, int plain_chains, int da_chains);
 /* RNG stream id of a complex (default: its index in the batch). Draws depend only on
  * (seed, stream, complex-local replica, step), so a complex run alone with the stream id it
  * has in a batch reproduces its batched trajectory. */

@@ -7,7 +7,8 @@
   surrogate energies and the exact energies (checked against the FP64 oracle): stage 1 is
   u1 < exp(mb (S_new - S_cur)), stage 2 is u2 < exp(mb ((E_new - E_old) - (S_new - S_cur)));
 * per-temperature energy distributions of delayed acceptance and plain Monte Carlo from the
-  same equilibrated start are indistinguishable (two-sample KS, p > 0.01);
+  same equilibrated start are indistinguishable (two-sample KS per temperature, the family of
+  20 tests at level 0.01);
 * the fallback controller switches a complex whose stage-2 acceptance is below the threshold
   back to plain Monte Carlo.
 """
@@ -57,7 +58,7 @@ def test_collect_is_the_plain_trajectory(raw):
         a.mc_init()
         b.mc_init()
         a.run_fused(0, 60, exchange=True)
-        sur = engine.Surrogate(b, hidden=64, batch=256, sample_cap=1 << 16)
+        sur = engine.Surrogate(b, hidden=128, batch=256, sample_cap=1 << 16)
         sur.collect(0, 60, exchange=True)
         a.sync()
         b.sync()
@@ -69,6 +70,28 @@ def test_collect_is_the_plain_trajectory(raw):
         assert st["plain_accepted"] == int(b.state()["n_accept"].sum())
 
 
+def test_concurrent_chains_collect_is_plain(raw):
+    """Collect steps on a ragged batch split into 3 concurrent chains equal the plain fused
+    loop on one chain."""
+    w = system.config(2, raw, n_ligands=6)
+    params = w.params
+    params.steps_per_dump = 40
+    with engine.Engine(w.ff, w.complexes, params) as a, \
+            engine.Engine(w.ff, w.complexes, params) as b:
+        a.set_concurrency(1, 1)
+        b.set_concurrency(1, 3)
+        for e in (a, b):
+            e.set_tile(4, 256)
+            e.mc_init()
+        a.run_fused(0, 20, exchange=True)
+        sur = engine.Surrogate(b, hidden=128, batch=256, sample_cap=1 << 16)
+        sur.collect(0, 20, exchange=True)
+        a.sync()
+        b.sync()
+        assert a.state().tobytes() == b.state().tobytes()
+        _same_records(a, b)
+
+
 def test_stage_off_is_the_plain_step(raw):
     w = _small(raw)
     cx, ff, params = w.complexes[0], w.ff, w.params
@@ -76,7 +99,7 @@ def test_stage_off_is_the_plain_step(raw):
         a.mc_init()
         b.mc_init()
         a.run_fused(0, 60, exchange=True)
-        sur = engine.Surrogate(b, hidden=64, batch=256, sample_cap=1 << 16, fallback_accept=0.0)
+        sur = engine.Surrogate(b, hidden=128, batch=256, sample_cap=1 << 16, fallback_accept=0.0)
         sur.collect(0, 60, exchange=True)
         sur.train(20)
         assert sur.stats()[0]["active"] == 1
@@ -188,9 +211,12 @@ def test_energy_distributions_match_plain(raw):
     assert st["rmse"] < 0.5
     ea, eb = sa["energy_old"]["e"][:, 9], sb["energy_old"]["e"][:, 9]
     ta, tb = sa["replica"]["idx_tmp"], sb["replica"]["idx_tmp"]
-    for t in range(cx.n_tmp):
-        p = stats.ks_2samp(ea[ta == t], eb[tb == t]).pvalue
-        assert p > 0.01, (t, p)
+    ps = [stats.ks_2samp(ea[ta == t], eb[tb == t]).pvalue for t in range(cx.n_tmp)]
+    # 20 KS tests at p > 0.01 each fail somewhere ~18 % of the time for identical processes;
+    # the family is held at level 0.01 (Bonferroni) and at most two temperatures may sit
+    # below 0.01 (their expected number under equality is 0.2)
+    assert min(ps) > 0.01 / cx.n_tmp, ps
+    assert sum(p <= 0.01 for p in ps) <= 2, ps
 
 
 def test_fallback_to_plain(raw):
@@ -198,7 +224,7 @@ def test_fallback_to_plain(raw):
     cx, ff, params = w.complexes[0], w.ff, w.params
     with engine.Engine(ff, [cx], params) as eng:
         eng.mc_init()
-        sur = engine.Surrogate(eng, hidden=32, batch=64, sample_cap=1 << 14,
+        sur = engine.Surrogate(eng, hidden=128, batch=64, sample_cap=1 << 14,
                                fallback_accept=0.999, fallback_window=500)
         sur.collect(0, 20, exchange=True)
         sur.train(1)  # barely trained: stage-2 acceptance below 0.999

@@ -184,6 +184,30 @@ def test_fused_graph_equals_stepwise(raw):
         assert np.array_equal(a.state().view(np.uint8), b.state().view(np.uint8))
 
 
+@pytest.mark.parametrize("chains", [3, 5])
+def test_concurrent_chains_give_the_same_chains(raw, chains):
+    """The fused graph split into concurrent chains (streams) reproduces the single-chain run
+    bit for bit, records included."""
+    w = system.config(2, raw, n_ligands=6)
+    params = w.params
+    params.steps_per_dump = 40
+    with engine.Engine(w.ff, w.complexes, params) as a, \
+            engine.Engine(w.ff, w.complexes, params) as b:
+        a.set_concurrency(1, 1)
+        b.set_concurrency(chains, chains)
+        for e in (a, b):
+            e.set_tile(4, 256)
+            e.mc_init()
+            e.run_fused(0, 20, exchange=True)
+            e.run_fused(20, 20, exchange=True)
+            e.sync()
+        assert a.state().tobytes() == b.state().tobytes()
+        ra, na = a.records()
+        rb, nb = b.records()
+        assert np.array_equal(na, nb)
+        assert ra.tobytes() == rb.tobytes()
+
+
 def test_batch_equals_alone(raw):
     """Config-2 style batch (uneven ligands and pockets): each complex's trajectory in the
     batch is bit-identical to running it alone with the same stream id and tile."""
