@@ -440,6 +440,24 @@ def run_ours(args, rank, world, local_rank):
     print(json.dumps(out), flush=True)
 
 
+def profile_da(args):
+    from geaxdock_gpu_b200 import engine
+    w = workload(42)
+    cx, ff, params = w.complexes[0], w.ff, w.params
+    params.record = 0
+    with engine.Engine(ff, [cx], params) as b:
+        if args.tile:
+            b.set_tile(*(int(v) for v in args.tile.split(",")))
+        b.mc_init()
+        sur = engine.Surrogate(b, sample_cap=1 << 20, fallback_accept=0.0)
+        sur.collect(0, 20, exchange=True)
+        sur.train(20)
+        sur.run(20, 20, exchange=True)
+        b.run_fused(40, 10, exchange=True)
+        b.sync()
+        print(json.dumps({"profile_da": sur.stats()[0]}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -450,7 +468,14 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-da", action="store_true", help="skip the delayed-acceptance runs")
     ap.add_argument("--tile", default="", help="replicas_per_cta,chunk_points[,unroll] (default: tuned)")
+    ap.add_argument("--profile-da", action="store_true",
+                    help="only a short delayed-acceptance sequence on the config-1 system (20 "
+                         "collect steps, 20 Adam steps, 20 DA steps, 10 plain steps), for "
+                         "profiler launch lists; prints its statistics")
     args = ap.parse_args()
+    if args.profile_da:
+        profile_da(args)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
