@@ -20,7 +20,7 @@ collective (replicas shard without exchange across shards): weak scaling.
 delayed_acceptance (N = 1): the config-3 workload on the config-1 system (2,000 burn-in steps of
            training samples, one epoch of Adam, then K intervals of delayed-acceptance and of
            plain steps from the same state, device-timed), at the configured moves and at 20x
-           larger moves; surrogate RMSE, stage acceptances, per-temperature KS p-values.
+           and 60x larger moves; surrogate RMSE, stage acceptances, per-temperature KS p-values.
 """
 from __future__ import annotations
 
@@ -219,7 +219,8 @@ def delayed_acceptance(w, dev, tile, scale_mult, intervals, burn=2000, iters=166
         train_s = time.perf_counter() - t0
         info = sur.info()
         a.mc_init()
-        a.set_state(b.state())
+        start = b.state()
+        a.set_state(start)
         a.sync()
         sa = torch.cuda.ExternalStream(a.cuda_stream(), device=dev)
         sb = torch.cuda.ExternalStream(b.cuda_stream(), device=dev)
@@ -251,11 +252,24 @@ def delayed_acceptance(w, dev, tile, scale_mult, intervals, burn=2000, iters=166
         plain_ms = sum(x[0].elapsed_time(x[1]) for x in ev)
         da_ms = sum(x[2].elapsed_time(x[3]) for x in ev)
         st = sur.stats()[0]
+        split_used = sur.split()
         fa, fb = a.state(), b.state()
         del flush
+    # null reference for the KS test: plain steps from the same start with another seed
+    p2 = type(p).from_buffer_copy(p)
+    p2.seed = p.seed + 1
+    with engine.Engine(ff, [cx], p2, device=dev) as c2:
+        c2.set_tile(*tile)
+        c2.mc_init()
+        c2.set_state(start)
+        c2.run_fused(burn + spe, spe * intervals, exchange=True)
+        c2.sync()
+        fc = c2.state()
     ea, eb = fa["energy_old"]["e"][:, 9], fb["energy_old"]["e"][:, 9]
     ta, tb = fa["replica"]["idx_tmp"], fb["replica"]["idx_tmp"]
     ks = [float(stats.ks_2samp(ea[ta == t], eb[tb == t]).pvalue) for t in range(cx.n_tmp)]
+    ec, tc = fc["energy_old"]["e"][:, 9], fc["replica"]["idx_tmp"]
+    ks_null = [float(stats.ks_2samp(ea[ta == t], ec[tc == t]).pvalue) for t in range(cx.n_tmp)]
     rs = cx.n_rep * spe * intervals
     passed = max(1, st["passed"])
     return {"metric": "MC replica-steps/s (surrogate delayed acceptance)",
@@ -269,9 +283,14 @@ def delayed_acceptance(w, dev, tile, scale_mult, intervals, burn=2000, iters=166
             "surrogate_rmse": st["rmse"], "target_mu_sigma": [info["mu"], info["sigma"]],
             "surrogate_active": st["active"],
             "ks_min_p": min(ks), "ks_p_per_temperature": ks,
+            "ks_null_min_p": min(ks_null),
+            "ks_note": "final states, 341 independent chains per temperature; ks_null: plain vs "
+                       "plain with another seed from the same start (what equal distributions "
+                       "give for the smallest of 20 p-values)",
             "collect_steps": burn, "collect_s": collect_s, "samples": info["n_samples"],
             "train_iterations": iters, "train_batch": 8192, "train_s": train_s,
             "train_loss_first_last": [float(losses[0]), float(losses[-1])],
+            "exact_stage_split": split_used,
             "intervals": intervals, "ms_per_interval": da_ms / intervals,
             "gpu_launches_per_interval": 3 + 5 * spe + 1,
             "timing": "CUDA events on each engine's stream, L2 flushed between intervals"}
@@ -417,7 +436,8 @@ def run_ours(args, rank, world, local_rank):
     da = None
     if world == 1 and not args.no_da:
         da = {"configured_moves": delayed_acceptance(w, dev, tile_used, 1.0, args.steps),
-              "moves_x20": delayed_acceptance(w, dev, tile_used, 20.0, args.steps)}
+              "moves_x20": delayed_acceptance(w, dev, tile_used, 20.0, args.steps),
+              "moves_x60": delayed_acceptance(w, dev, tile_used, 60.0, args.steps)}
 
     cpu = None
     if world == 1 and not args.no_cpu:
@@ -432,7 +452,8 @@ def run_ours(args, rank, world, local_rank):
                       "step": "10 MC steps + 1 exchange, all replicas",
                       "l2": "flushed between steps (256 MB write)",
                       "tile": {"replicas_per_cta": tile_used[0], "chunk_points": tile_used[1],
-                               "unroll": tile_used[2], "source": tile_source},
+                               "unroll": tile_used[2], "split": tile_used[3],
+                               "source": tile_source},
                       "parallelism": "replica shards, no collective" if world > 1 else "1 GPU"},
            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
            "gpu_launches": 2 * args.steps + args.steps // max(1, intervals_per_dump),
@@ -445,6 +466,8 @@ def profile_da(args):
     w = workload(42)
     cx, ff, params = w.complexes[0], w.ff, w.params
     params.record = 0
+    for i in range(6):
+        params.move_scale[i] *= args.move_mult
     with engine.Engine(ff, [cx], params) as b:
         if args.tile:
             b.set_tile(*(int(v) for v in args.tile.split(",")))
@@ -472,6 +495,8 @@ def main():
                     help="only a short delayed-acceptance sequence on the config-1 system (20 "
                          "collect steps, 20 Adam steps, 20 DA steps, 10 plain steps), for "
                          "profiler launch lists; prints its statistics")
+    ap.add_argument("--move-mult", type=float, default=1.0,
+                    help="--profile-da: move scales multiplied by this factor")
     args = ap.parse_args()
     if args.profile_da:
         profile_da(args)

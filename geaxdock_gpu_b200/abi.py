@@ -112,7 +112,7 @@ class McParams(C.Structure):
 
 
 class Tile(C.Structure):
-    _fields_ = [("replicas_per_cta", I), ("chunk_points", I), ("unroll", I)]
+    _fields_ = [("replicas_per_cta", I), ("chunk_points", I), ("unroll", I), ("split", I)]
 
 
 class ReplicaState(C.Structure):
@@ -126,6 +126,7 @@ class SurParams(C.Structure):
     _fields_ = [
         ("hidden", I), ("embedding", I), ("lr", F), ("batch", I), ("sample_cap", C.c_longlong),
         ("fallback_accept", F), ("fallback_window", C.c_longlong), ("seed", C.c_uint64),
+        ("split", I), ("pad", I),
     ]
 
 

@@ -25,11 +25,14 @@
 #include "gd_numerics.h"
 
 namespace gd {
-template <int UNROLL>
+template <int UNROLL, bool SPLIT, bool DA>
 __global__ void gd_mc_kernel(GdMcArgs a, GdForceConst f);
-extern template __global__ void gd_mc_kernel<1>(GdMcArgs, GdForceConst);
-extern template __global__ void gd_mc_kernel<2>(GdMcArgs, GdForceConst);
-extern template __global__ void gd_mc_kernel<4>(GdMcArgs, GdForceConst);
+#define GD_EXT(U, S, D) extern template __global__ void gd_mc_kernel<U, S, D>(GdMcArgs, GdForceConst);
+GD_EXT(1, false, false) GD_EXT(2, false, false) GD_EXT(4, false, false)
+GD_EXT(1, true, false) GD_EXT(2, true, false) GD_EXT(4, true, false)
+GD_EXT(1, false, true) GD_EXT(2, false, true) GD_EXT(4, false, true)
+GD_EXT(1, true, true) GD_EXT(2, true, true) GD_EXT(4, true, true)
+#undef GD_EXT
 __global__ void gd_exchange_kernel(const GdDevComplex *cxs, const int *group_base, int n_complex,
                                    int g_begin, int g_end, gd_replica *replica,
                                    const float *etotal, int *acs, uint64_t seed,
@@ -104,7 +107,7 @@ struct gd_ctx {
   cudaStream_t stream = nullptr;
   gd_mc_params mc{};
   int n_complex = 0, n_rep = 0, n_groups = 0;
-  int threads = 256, chunk = 512, unroll = 2, num_sms = 148;
+  int threads = 256, chunk = 512, unroll = 2, split = 1, num_sms = 148;
   std::vector<ComplexInfo> info;
   std::vector<void *> allocs;
   GdForceConst fc{};
@@ -291,15 +294,22 @@ int ensure_counters(gd_ctx *c, int n) {
 
 typedef void (*McKernel)(GdMcArgs, GdForceConst);
 
-McKernel mc_kernel(int unroll) {
-  if (unroll >= 4) return gd::gd_mc_kernel<4>;
-  if (unroll >= 2) return gd::gd_mc_kernel<2>;
-  return gd::gd_mc_kernel<1>;
+/* the kernel variant for an unroll depth, a protein split and the mode-3 epilogue */
+template <bool S, bool D>
+McKernel mc_variant(int unroll) {
+  if (unroll >= 4) return gd::gd_mc_kernel<4, S, D>;
+  if (unroll >= 2) return gd::gd_mc_kernel<2, S, D>;
+  return gd::gd_mc_kernel<1, S, D>;
 }
 
-int grid_for(gd_ctx *c, int n_tiles, size_t smem) {
+McKernel mc_kernel(int unroll, int split, bool da = false) {
+  if (da) return split > 1 ? mc_variant<true, true>(unroll) : mc_variant<false, true>(unroll);
+  return split > 1 ? mc_variant<true, false>(unroll) : mc_variant<false, false>(unroll);
+}
+
+int grid_for(gd_ctx *c, int n_tiles, size_t smem, int split = 0, bool da = false) {
   int nb = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, mc_kernel(c->unroll), c->threads,
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, mc_kernel(c->unroll, split ? split : c->split, da), c->threads,
                                                     smem) != cudaSuccess ||
       nb < 1)
     nb = 1;
@@ -312,6 +322,7 @@ GdMcArgs base_args(gd_ctx *c) {
   a.cx = c->d_cx;
   a.pp = c->d_pp;
   a.chunk = c->chunk;
+  a.split = c->split;
   a.move_kind = c->mc.move_kind;
   a.seed = c->mc.seed;
   for (int i = 0; i < 6; ++i) a.move_scale[i] = c->mc.move_scale[i];
@@ -332,8 +343,8 @@ GdMcArgs base_args(gd_ctx *c) {
   return a;
 }
 
-int set_kernel_attrs(const gd_ctx *c, size_t smem) {
-  const McKernel k = mc_kernel(c->unroll);
+int set_kernel_attrs(const gd_ctx *c, size_t smem, int split = 0, bool da = false) {
+  const McKernel k = mc_kernel(c->unroll, split ? split : c->split, da);
   CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   CK(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
                           cudaSharedmemCarveoutMaxShared));
@@ -350,7 +361,7 @@ int launch_mc(gd_ctx *c, GdMcArgs a, const GdTileDesc *d_tiles, int n_tiles, int
   a.tile_counter = counter;
   CK(cudaMemsetAsync(counter, 0, sizeof(int), c->stream));
   const int grid = grid_for(c, n_tiles, smem);
-  mc_kernel(c->unroll)<<<grid, c->threads, smem, c->stream>>>(a, c->fc);
+  mc_kernel(c->unroll, a.split)<<<grid, c->threads, smem, c->stream>>>(a, c->fc);
   CK(cudaGetLastError());
   return GD_OK;
 }
@@ -954,17 +965,23 @@ int gd_set_tile(gd_ctx *c, int k, const gd_tile *t) {
     return fail(GD_ERR_INVALID, "chunk_points must be a multiple of 4 in 4..4096");
   if (t->replicas_per_cta < 1 || t->replicas_per_cta > GD_MAX_SLOTS)
     return fail(GD_ERR_INVALID, "replicas_per_cta outside 1..%d", GD_MAX_SLOTS);
+  if (t->split < 0 || t->split > 16) return fail(GD_ERR_INVALID, "split outside 0..16");
   if (k < -1 || k >= c->n_complex) return fail(GD_ERR_INVALID, "bad complex index");
+  const int S = t->split ? t->split : 1;
+  if ((t->chunk_points / 2) < S)
+    return fail(GD_ERR_INVALID, "chunk_points must hold at least two points per split");
   /* one block size per context: every complex's k must fit the block */
   std::vector<ComplexInfo> info = c->info;
   for (int i = 0; i < c->n_complex; ++i)
     if (k == -1 || k == i) info[i].k = std::min(t->replicas_per_cta, info[i].n_tmp * info[i].n_lig);
   int T = 32;
-  for (auto &x : info) T = std::max(T, ((x.k * x.lna + 31) / 32) * 32);
-  if (T > GD_MAX_TPB) return fail(GD_ERR_INVALID, "replicas_per_cta * lna exceeds %d", GD_MAX_TPB);
+  for (auto &x : info) T = std::max(T, ((x.k * S * x.lna + 31) / 32) * 32);
+  if (T > GD_MAX_TPB)
+    return fail(GD_ERR_INVALID, "replicas_per_cta * split * lna exceeds %d", GD_MAX_TPB);
   c->info = info;
   c->threads = T;
   c->chunk = t->chunk_points;
+  c->split = S;
   if (t->unroll) c->unroll = t->unroll;
   c->tile_gen += 1;
   build_tiles(c, 0, c->n_rep - 1, c->full_tiles);
@@ -1005,7 +1022,7 @@ int gd_autotune(gd_ctx *c, const gd_tile *cand, int n_cand, int repeats, gd_tile
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  const gd_tile keep_tile = {c->info[0].k, c->chunk, c->unroll};
+  const gd_tile keep_tile = {c->info[0].k, c->chunk, c->unroll, c->split};
   std::vector<int> keep_k;
   for (auto &x : c->info) keep_k.push_back(x.k);
   const int keep_threads = c->threads;
@@ -1054,12 +1071,14 @@ int gd_autotune(gd_ctx *c, const gd_tile *cand, int n_cand, int repeats, gd_tile
     rc = gd_set_tile(c, -1, &cand[best_i]);
     *best = cand[best_i];
     best->unroll = c->unroll;
+    best->split = c->split;
   } else {
     /* restore the tile in use before the probe */
     for (int i = 0; i < c->n_complex; ++i) c->info[i].k = keep_k[i];
     c->threads = keep_threads;
     c->chunk = keep_tile.chunk_points;
     c->unroll = keep_tile.unroll;
+    c->split = keep_tile.split;
     c->tile_gen += 1;
     build_tiles(c, 0, c->n_rep - 1, c->full_tiles);
     if (rc == GD_OK) rc = fail(GD_ERR_INVALID, "gd_autotune: no candidate fits this batch");
@@ -1105,6 +1124,7 @@ int gd_get_tile(const gd_ctx *c, int k, gd_tile *t) {
   t->replicas_per_cta = c->info[k].k;
   t->chunk_points = c->chunk;
   t->unroll = c->unroll;
+  t->split = c->split;
   return GD_OK;
 }
 
@@ -1199,7 +1219,7 @@ int gd_mc_run_fused(gd_ctx *c, int s1, int n_steps, int exchange) {
         a.tiles = c->d_chain_tiles + ch.t_off;
         a.n_tiles = ch.t_cnt;
         a.tile_counter = c->d_counters + k * chunks + i;
-        mc_kernel(c->unroll)<<<grid, c->threads, smem, st>>>(a, c->fc);
+        mc_kernel(c->unroll, a.split)<<<grid, c->threads, smem, st>>>(a, c->fc);
         if (exchange)
           gd::gd_exchange_kernel<<<(ch.xg1 - ch.xg0 + 127) / 128, 128, 0, st>>>(
               c->d_cx, c->d_group_base, c->n_complex, ch.xg0, ch.xg1, c->d_replica, c->d_etotal,
@@ -1552,7 +1572,7 @@ extern "C" int gd_eval_energy_noalloc(gd_ctx *c, int ci, int prt_conf, int lig_c
   const size_t smem = smem_bytes(c);
   if ((rc = set_kernel_attrs(c, smem))) return rc;
   const int grid = grid_for(c, n_tiles, smem);
-  mc_kernel(c->unroll)<<<grid, c->threads, smem, c->stream>>>(a, c->fc);
+  mc_kernel(c->unroll, a.split)<<<grid, c->threads, smem, c->stream>>>(a, c->fc);
   CK(cudaGetLastError());
   return GD_OK;
 }
@@ -1563,7 +1583,10 @@ struct DaState {
   gd::Mlp net;
   gd_sur_params prm{};
   std::vector<gd::GdGroup> groups;
-  int n_tiles = 0, built_gen = -1;
+  int n_tiles = 0, built_gen = -1, built_split = -1;
+  int split = 1;                                 /* protein split of the exact stage */
+  double last_pass = 1.0;                        /* surrogate-stage pass rate, last window */
+  unsigned long long prev_prop = 0, prev_pass = 0;
   std::vector<void *> allocs;
   int *d_rep_cx = nullptr, *d_rep_group = nullptr, *d_group_b0 = nullptr;
   int *d_emb_base = nullptr, *d_active = nullptr;
@@ -1673,11 +1696,12 @@ int da_upload_epi(gd_ctx *c) {
   return GD_OK;
 }
 
-/* groups and the exact kernel's static tile list for the current tile shapes: tile i of
- * group g covers pose slots [b0 + i k, b0 + i k + cap) and carries (g << 8) | cap */
-int da_build_groups(gd_ctx *c) {
+/* groups and the exact kernel's static tile list for the current tile shapes and the exact
+ * stage's split S: tile i of group g covers pose slots [b0 + i k, b0 + i k + cap), k the
+ * replicas a CTA holds at split S, and carries (g << 8) | cap */
+int da_build_groups(gd_ctx *c, int S) {
   DaState *d = c->da;
-  if (d->built_gen == c->tile_gen && d->d_tiles) return GD_OK;
+  if (d->built_gen == c->tile_gen && d->built_split == S && d->d_tiles) return GD_OK;
   std::vector<gd::GdGroup> g;
   std::vector<GdTileDesc> tiles;
   std::vector<int> rep_group(c->n_rep), b0s;
@@ -1690,8 +1714,8 @@ int da_build_groups(gd_ctx *c) {
       q.pc = p;
       q.b0 = x.rep_offset + p * block;
       q.n = block;
-      q.k = x.k;
-      q.n_tiles = (block + x.k - 1) / x.k;
+      q.k = std::max(1, std::min(x.k, c->threads / (S * x.lna)));
+      q.n_tiles = (block + q.k - 1) / q.k;
       q.tile_base = (int)tiles.size();
       q.pad = 0;
       const int gi = (int)g.size();
@@ -1736,8 +1760,30 @@ int da_build_groups(gd_ctx *c) {
   d->groups = g;
   d->n_tiles = (int)tiles.size();
   d->built_gen = c->tile_gen;
-  da_drop_graphs(c);
+  d->built_split = S;
   return GD_OK;
+}
+
+/* largest split every complex of the batch fits into the context's CTA */
+int da_max_split(const gd_ctx *c) {
+  int m = 16;
+  for (const auto &x : c->info) m = std::min(m, std::max(1, c->threads / x.lna));
+  return m;
+}
+
+/* split of the next delayed-acceptance run from the surrogate stage's last pass rate: with
+ * few survivors one exact-stage tile per CTA sets the step's latency, and more lanes per atom
+ * shorten it, at the price of fewer replicas sharing each staged protein chunk. Thresholds
+ * from config-1 sweeps (ms per 10 steps at pass 0.50 / 0.30 / 0.195 / 0.097: split 1 6.9 /
+ * 6.1 / 6.0 / 5.8, split 2 8.4 / 5.4 / 4.2 / 4.0, split 3 9.7 / 6.0 / 4.3 / 3.3). */
+int da_choose_split(const gd_ctx *c, bool collect) {
+  const DaState *d = c->da;
+  if (collect) return c->split;
+  const int mx = da_max_split(c);
+  if (d->prm.split > 0) return std::min(d->prm.split, mx);
+  const double p = d->last_pass;
+  const int S = p > 0.4 ? 1 : (p > 0.13 ? 2 : (p > 0.05 ? 3 : 4));
+  return std::max(c->split, std::min(S, mx));
 }
 
 gd::GdDaDev da_args(gd_ctx *c) {
@@ -1789,7 +1835,7 @@ gd::GdDaDev da_args(gd_ctx *c) {
 /* the exact stage of step j of one chain: gd_mc_kernel mode 3 over the chain's part of the
  * static tile list */
 void da_launch_exact(gd_ctx *c, const Chain &ch, int k, int n_steps, int j, bool collect,
-                     size_t smem, cudaStream_t st) {
+                     size_t smem, cudaStream_t st, int S) {
   DaState *d = c->da;
   const int ng = (int)d->groups.size();
   const int t0 = d->groups[ch.g0].tile_base;
@@ -1812,13 +1858,16 @@ void da_launch_exact(gd_ctx *c, const Chain &ch, int k, int n_steps, int j, bool
   a.da_g0 = ch.g0;
   a.da_g1 = ch.g1;
   a.da_collect = collect ? 1 : 0;
-  mc_kernel(c->unroll)<<<grid_for(c, t1 - t0, smem), c->threads, smem, st>>>(a, c->fc);
+  a.split = S;
+  mc_kernel(c->unroll, S, true)<<<grid_for(c, t1 - t0, smem, S, true), c->threads, smem, st>>>(
+      a, c->fc);
 }
 
 /* the graph of n_steps steps (collect: plain steps that store samples), one chain per stream */
-int da_graph(gd_ctx *c, int n_steps, int exchange, bool collect, cudaGraphExec_t *out) {
+int da_graph(gd_ctx *c, int n_steps, int exchange, bool collect, int S, cudaGraphExec_t *out) {
   DaState *d = c->da;
-  const long long key = ((long long)n_steps << 2) | (exchange ? 2 : 0) | (collect ? 1 : 0);
+  const long long key =
+      ((long long)n_steps << 7) | ((long long)S << 2) | (exchange ? 2 : 0) | (collect ? 1 : 0);
   auto it = d->graphs.find(key);
   if (it != d->graphs.end()) {
     *out = it->second;
@@ -1839,7 +1888,7 @@ int da_graph(gd_ctx *c, int n_steps, int exchange, bool collect, cudaGraphExec_t
   if ((rc = da_upload_epi(c))) return rc;
   CK(cudaStreamSynchronize(c->stream));
   const size_t smem = smem_bytes(c);
-  if ((rc = set_kernel_attrs(c, smem))) return rc;
+  if ((rc = set_kernel_attrs(c, smem, S, true))) return rc;
   const gd::GdDaDev a = da_args(c);
   const int spe = c->mc.steps_per_exchange;
   const int ng = (int)d->groups.size();
@@ -1856,7 +1905,7 @@ int da_graph(gd_ctx *c, int n_steps, int exchange, bool collect, cudaGraphExec_t
     for (int j = 0; j < n_steps; ++j) {
       frc |= gd::da_front(a, collect ? GD_DA_COLLECT : GD_DA_STEP, j,
                           d->d_cnt + (size_t)(j & 1) * ng, ch.r0, ch.r1, st);
-      da_launch_exact(c, ch, k, n_steps, j, collect, smem, st);
+      da_launch_exact(c, ch, k, n_steps, j, collect, smem, st, S);
       if (exchange && (j + 1) % spe == 0) {
         const int i = (j + 1) / spe - 1;
         gd::gd_exchange_kernel<<<(ch.xg1 - ch.xg0 + 127) / 128, 128, 0, st>>>(
@@ -1891,10 +1940,17 @@ int da_run_steps(gd_ctx *c, int s1, int n_steps, int exchange, bool collect) {
                                 "with exchange)");
   if (s1 < 0) return fail(GD_ERR_INVALID, "s1 must be >= 0");
   CK(cudaSetDevice(c->device));
-  int rc = da_build_groups(c);
+  const int S = da_choose_split(c, collect);
+  if (c->da->built_split != S || c->da->built_gen != c->tile_gen) {
+    /* tile lists and graphs of another split or tile shape are stale */
+    CK(cudaStreamSynchronize(c->stream));
+    da_drop_graphs(c);
+  }
+  int rc = da_build_groups(c, S);
   if (rc) return rc;
+  c->da->split = S;
   cudaGraphExec_t g;
-  if ((rc = da_graph(c, n_steps, exchange, collect, &g))) return rc;
+  if ((rc = da_graph(c, n_steps, exchange, collect, S, &g))) return rc;
   CK(cudaStreamSynchronize(c->stream));
   c->h_cursor[0] = s1;
   c->h_cursor[1] = c->exchange_calls;
@@ -1937,6 +1993,7 @@ int da_reset_counters(gd_ctx *c) {
   CK(cudaMemsetAsync(d->d_nerr, 0, sizeof(int) * R, c->stream));
   CK(cudaMemsetAsync(d->d_err2, 0, sizeof(double) * R, c->stream));
   d->window0.assign((size_t)c->n_complex * GD_DA_NSTAT, 0);
+  d->prev_prop = d->prev_pass = 0;
   return GD_OK;
 }
 
@@ -2129,7 +2186,7 @@ int gd_sur_create(gd_ctx *c, const gd_sur_params *p) {
   CK(cudaMemset(d->d_s_new, 0, sizeof(float) * R));
   rc = da_upload_active(c);
   if (!rc) rc = da_reset_counters(c);
-  if (!rc) rc = da_build_groups(c);
+  if (!rc) rc = da_build_groups(c, c->split);
   if (!rc) rc = da_upload_epi(c);
   if (rc) {
     da_free(c);
@@ -2198,10 +2255,21 @@ int gd_da_run(gd_ctx *c, int s1, int n_steps, int exchange) {
   int rc = da_run_steps(c, s1, n_steps, exchange, false);
   if (rc) return rc;
   DaState *d = c->da;
-  if (d->prm.fallback_accept <= 0.0f) return GD_OK;
+  const bool controller = d->prm.fallback_accept > 0.0f;
+  if (!controller && d->prm.split > 0) return GD_OK;
   std::vector<unsigned long long> st;
   std::vector<double> er;
   if ((rc = da_read_stats(c, st, er))) return rc;
+  /* pass rate of this run (all complexes with the stage on): picks the next run's split */
+  unsigned long long prop = 0, pass = 0;
+  for (int ci = 0; ci < c->n_complex; ++ci) {
+    prop += st[(size_t)ci * GD_DA_NSTAT + GD_DA_PROPOSED];
+    pass += st[(size_t)ci * GD_DA_NSTAT + GD_DA_PASSED];
+  }
+  if (prop > d->prev_prop) d->last_pass = (double)(pass - d->prev_pass) / (double)(prop - d->prev_prop);
+  d->prev_prop = prop;
+  d->prev_pass = pass;
+  if (!controller) return GD_OK;
   bool changed = false;
   for (int ci = 0; ci < c->n_complex; ++ci) {
     if (!d->active[ci]) continue;
@@ -2298,6 +2366,12 @@ int gd_sur_info(gd_ctx *c, float *mu, float *sigma, long long *n_samples) {
   if (mu) *mu = d->net.mu;
   if (sigma) *sigma = d->net.sigma;
   if (n_samples) *n_samples = d->smp_hi - std::max(d->smp_lo, d->smp_hi - d->smp_cap);
+  return GD_OK;
+}
+
+int gd_sur_split(gd_ctx *c, int *split) {
+  if (!c || !c->da || !split) return fail(GD_ERR_STATE, "gd_sur_create has not run");
+  *split = c->da->split;
   return GD_OK;
 }
 

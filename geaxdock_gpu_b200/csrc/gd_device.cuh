@@ -119,6 +119,7 @@ struct GdMcArgs {
   int step0;                  /* step number of the first step (s1 + s2), added to *step_base */
   const int *step_base;       /* device cursor for graph replays (null: 0) */
   int chunk;                  /* protein points per shared-memory buffer (multiple of 4) */
+  int split;                  /* lanes per ligand atom (protein split), >= 1 */
   int move_kind;
   uint64_t seed;
   float move_scale[6];

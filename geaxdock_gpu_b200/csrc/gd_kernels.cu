@@ -328,7 +328,7 @@ __device__ __forceinline__ void da_decide(const GdMcArgs &a, const GdDevComplex 
  * chunk two ahead. Every wait is bounded (globaltimer); a wait that runs out sets the error
  * word, the CTA leaves at the next step barrier after letting its copies in flight land.
  */
-template <int UNROLL>
+template <int UNROLL, bool SPLIT, bool DA>
 __global__ void __launch_bounds__(GD_MAX_TPB, GD_MIN_BLOCKS(UNROLL))
     gd_mc_kernel(GdMcArgs a, GdForceConst f) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -357,7 +357,7 @@ __global__ void __launch_bounds__(GD_MAX_TPB, GD_MIN_BLOCKS(UNROLL))
   uint32_t consumed0 = 0, consumed1 = 0; /* completed phases waited for, per buffer */
   const int step_first = a.step0 + (a.step_base ? *a.step_base : 0);
   const int warp = tid >> 5, lane = tid & 31, nwarps = T >> 5;
-  if (a.mode == 3 && blockIdx.x == 0)
+  if (DA && a.mode == 3 && blockIdx.x == 0)
     for (int g = a.da_g0 + tid; g < a.da_g1; g += T) a.da_cnt_next[g] = 0;
 
   for (;;) {
@@ -367,7 +367,7 @@ __global__ void __launch_bounds__(GD_MAX_TPB, GD_MIN_BLOCKS(UNROLL))
     if (t >= a.n_tiles || s_abort) break;
     const GdTileDesc tile = a.tiles[t];
     int k = tile.count;
-    if (a.mode == 3) {
+    if (DA && a.mode == 3) {
       /* slot (group, capacity): the survivors of the group past this tile's first slot */
       const int g = tile.count >> 8, cap = tile.count & 255;
       k = max(0, min(cap, a.da_cnt[g] - (tile.rep_begin - a.da->group_b0[g])));
@@ -379,10 +379,13 @@ __global__ void __launch_bounds__(GD_MAX_TPB, GD_MIN_BLOCKS(UNROLL))
       continue;
     }
     const GdDevComplex &cx = a.cx[tile.complex_index];
-    const int L = cx.lna;
-    const bool active = tid < k * L;
-    const int j = active ? tid / L : 0;
-    const int l = active ? tid - j * L : 0;
+    /* lane = (slot j, protein split sp, ligand atom l): the S copies of an atom each walk
+     * 1/S of every protein segment; S = 1 is one lane per atom */
+    const int L = cx.lna, S = SPLIT ? a.split : 1, SL = S * L;
+    const bool active = tid < k * SL;
+    const int j = active ? tid / SL : 0;
+    const int sp = active ? (tid - j * SL) / L : 0;
+    const int l = active ? tid - j * SL - sp * L : 0;
 
     /* ---- slot set-up (one thread per replica) ---- */
     if (tid < k) {
@@ -506,8 +509,16 @@ __global__ void __launch_bounds__(GD_MAX_TPB, GD_MIN_BLOCKS(UNROLL))
           const int c0 = ci * D, c1 = min(pnp_pad, c0 + D);
           for (int sg = 0; sg < nseg; ++sg) {
             const int4 g = segs[sg];
-            const int i0 = max(g.x, c0) - c0, i1 = min(g.y, c1) - c0;
+            int i0 = max(g.x, c0) - c0, i1 = min(g.y, c1) - c0;
             if (i0 >= i1) continue;
+            if (S > 1) {
+              /* this split's run of point pairs (i0 is even; the odd tail goes to the last) */
+              const int np = (i1 - i0 + 1) >> 1;
+              const int e = i0 + 2 * (np * (sp + 1) / S);
+              i0 += 2 * (np * sp / S);
+              i1 = min(i1, e);
+              if (i0 >= i1) continue;
+            }
             const float4 *pr = reinterpret_cast<const float4 *>(pprow + g.z);
             const float4 q0 = __ldg(pr), q1 = __ldg(pr + 1), q2 = __ldg(pr + 2);
             Pair2 pq;
@@ -548,8 +559,21 @@ __global__ void __launch_bounds__(GD_MAX_TPB, GD_MIN_BLOCKS(UNROLL))
         }
       }
 
-      /* ---- per-atom tail: hpc, kde, rmsd, reference contacts ---- */
+      /* ---- per-atom tail: hpc, kde, rmsd, reference contacts (split 0 of each atom) ---- */
+      if (S > 1) {
+        /* hpc is nonlinear in the atom's hydrophobic sum: gather the splits' parts first */
+        __syncthreads();
+        if (active && sp == 0)
+          for (int q = 1; q < S; ++q) {
+            part[5 * T + tid] += part[5 * T + tid + q * L];
+            part[5 * T + tid + q * L] = 0.0;
+          }
+      }
       if (active && !aborted) {
+        part[1 * T + tid] *= (double)orig.w;
+        part[8 * T + tid] = (double)ncon;
+      }
+      if (active && !aborted && sp == 0) {
         const double hpc2 = (part[5 * T + tid] - (double)f.hpl0[tl]) / (double)f.hpl1[tl];
         part[5 * T + tid] = 0.5 * hpc2 * hpc2 - (double)f.hpl2[tl];
         float ks = 0.0f;
@@ -574,8 +598,6 @@ __global__ void __launch_bounds__(GD_MAX_TPB, GD_MIN_BLOCKS(UNROLL))
           const float4 rp = __ldg(cx.ref_pts + i);
           tp += dist2(ax, ay, az, rp.x, rp.y, rp.z) <= rp.w ? 1 : 0;
         }
-        part[1 * T + tid] *= (double)orig.w;
-        part[8 * T + tid] = (double)ncon;
         part[9 * T + tid] = (double)tp;
       }
       if (__syncthreads_or(aborted)) {
@@ -587,11 +609,11 @@ __global__ void __launch_bounds__(GD_MAX_TPB, GD_MIN_BLOCKS(UNROLL))
       for (int js = warp; js < k; js += nwarps) {
         Slot &sl = slots[js];
         /* slot totals are written back over the slot's first partial */
-        double *tot = part + js * L;
+        double *tot = part + js * SL;
 #pragma unroll 1
         for (int qi = 0; qi < NQ; ++qi) {
           double v = 0.0;
-          for (int i = lane; i < L; i += 32) v += part[qi * T + js * L + i];
+          for (int i = lane; i < SL; i += 32) v += part[qi * T + js * SL + i];
           v = warp_sum(v);
           if (lane == 0) tot[qi * T] = v;
         }
@@ -604,7 +626,7 @@ __global__ void __launch_bounds__(GD_MAX_TPB, GD_MIN_BLOCKS(UNROLL))
             const int idx = cx.lig_meta[sl.lig_conf * L + i].y;
             const float mx = cx.mcs_x[(size_t)m * cx.mcs_ld + idx];
             if (mx != GD_MCS_INVALID_COORD) {
-              const float4 at = atoms[js * L + i];
+              const float4 at = atoms[js * SL + i];
               const float dx = at.x - mx;
               const float dy = at.y - cx.mcs_y[(size_t)m * cx.mcs_ld + idx];
               const float dz = at.z - cx.mcs_z[(size_t)m * cx.mcs_ld + idx];
@@ -654,7 +676,7 @@ __global__ void __launch_bounds__(GD_MAX_TPB, GD_MIN_BLOCKS(UNROLL))
           const int rid = sl.rep;
           if (a.mode == 2) {
             a.e_out[rid] = en;
-          } else if (a.mode == 3) {
+          } else if (DA && a.mode == 3) {
             da_decide(a, cx, tile.complex_index, rid, en, sl.mm_new, step_first + s);
           } else {
             int acc = 1;
@@ -720,10 +742,14 @@ __global__ void __launch_bounds__(GD_MAX_TPB, GD_MIN_BLOCKS(UNROLL))
   }
 }
 
-/* the kernel variants the host can launch (point pairs in flight per lane) */
-template __global__ void gd_mc_kernel<1>(GdMcArgs, GdForceConst);
-template __global__ void gd_mc_kernel<2>(GdMcArgs, GdForceConst);
-template __global__ void gd_mc_kernel<4>(GdMcArgs, GdForceConst);
+/* the kernel variants the host can launch: point pairs in flight per lane; protein split
+ * and the delayed-acceptance exact stage (mode 3) compiled out when false */
+#define GD_INST(U, S, D) template __global__ void gd_mc_kernel<U, S, D>(GdMcArgs, GdForceConst);
+GD_INST(1, false, false) GD_INST(2, false, false) GD_INST(4, false, false)
+GD_INST(1, true, false) GD_INST(2, true, false) GD_INST(4, true, false)
+GD_INST(1, false, true) GD_INST(2, false, true) GD_INST(4, false, true)
+GD_INST(1, true, true) GD_INST(2, true, true) GD_INST(4, true, true)
+#undef GD_INST
 
 /* ExchangeReplicas_d, one thread per (complex, protein conformer, ligand conformer) group of
  * the range [g_begin, g_end). */

@@ -81,6 +81,7 @@ def lib() -> C.CDLL:
         "gd_sur_info": [vp, C.POINTER(C.c_float), C.POINTER(C.c_float),
                         C.POINTER(C.c_longlong)],
         "gd_da_trace_enable": [vp, C.c_int, C.c_int],
+        "gd_sur_split": [vp, ip],
         "gd_da_trace_get": [vp, fp, fp, ip],
         "gd_mlp_create": [C.c_int, C.c_int, C.c_int, C.c_uint64, C.POINTER(vp)],
         "gd_mlp_destroy": [vp],
@@ -186,9 +187,10 @@ class Engine:
         check(lib().gd_sync(self.h))
 
     def set_tile(self, replicas_per_cta: int, chunk_points: int, unroll: int = 0,
-                 complex_index: int = -1):
+                 split: int = 0, complex_index: int = -1):
         t = abi.Tile()
         t.replicas_per_cta, t.chunk_points, t.unroll = replicas_per_cta, chunk_points, unroll
+        t.split = split
         check(lib().gd_set_tile(self.h, complex_index, C.byref(t)))
 
     def cuda_stream(self) -> int:
@@ -207,9 +209,10 @@ class Engine:
         check(lib().gd_set_wait_timeout(self.h, ns))
 
     def tile(self, complex_index=0):
+        """(replicas_per_cta, chunk_points, unroll, split)"""
         t = abi.Tile()
         check(lib().gd_get_tile(self.h, complex_index, C.byref(t)))
-        return t.replicas_per_cta, t.chunk_points, t.unroll
+        return t.replicas_per_cta, t.chunk_points, t.unroll, t.split
 
     # ---- results ----
     def records(self, r0=0, r1=None):
@@ -353,6 +356,11 @@ class Surrogate:
         mu, sg, n = C.c_float(), C.c_float(), C.c_longlong()
         check(lib().gd_sur_info(self.eng.h, C.byref(mu), C.byref(sg), C.byref(n)))
         return {"mu": mu.value, "sigma": sg.value, "n_samples": n.value}
+
+    def split(self) -> int:
+        v = C.c_int()
+        check(lib().gd_sur_split(self.eng.h, C.byref(v)))
+        return v.value
 
     def trace_enable(self, step0: int, max_steps: int):
         check(lib().gd_da_trace_enable(self.eng.h, step0, max_steps))

@@ -165,6 +165,10 @@ typedef struct {
   int replicas_per_cta;     /* replicas sharing one protein tile in one CTA */
   int chunk_points;         /* protein points staged per shared-memory buffer */
   int unroll;               /* protein point pairs in flight per lane: 1, 2 or 4 (0: keep) */
+  int split;                /* lanes per ligand atom, each walking 1/split of every protein
+                               segment (0 or 1: one lane per atom); replicas_per_cta * split *
+                               atoms must fit one CTA. The energies' FP32 summation order depends
+                               on it (results within the parity tolerance of each other). */
 } gd_tile;
 
 /* Per-replica Monte Carlo state (checkpoint unit). */
@@ -302,6 +306,10 @@ typedef struct {
                                below this reverts to plain MC (0: never) */
   long long fallback_window;/* surviving proposals per complex between decisions */
   uint64_t seed;            /* weight init and batch draws */
+  int split;                /* protein split of the exact stage (gd_tile.split); 0: chosen per
+                               gd_da_run from the surrogate stage's pass rate (1 when every
+                               proposal survives, up to the CTA's limit when few do) */
+  int pad;
 } gd_sur_params;
 
 /* per-complex counters since gd_sur_create / the last gd_sur_train */
@@ -335,6 +343,8 @@ int gd_sur_predict(gd_ctx *ctx, int complex_index, int prt_conf, int lig_conf,
                    const float *movematrix, int n_poses, float *energy);
 /* normalisation of the targets (E = mu + sigma * network output), valid samples */
 int gd_sur_info(gd_ctx *ctx, float *mu, float *sigma, long long *n_samples);
+/* protein split the last gd_da_run's exact stage ran with (gd_sur_params.split) */
+int gd_sur_split(gd_ctx *ctx, int *split);
 /* decision trace of gd_da_run: per replica and step the surrogate energy of the proposal,
  * its exact energy (NaN when the surrogate stage rejected it) and the outcome
  * (0 stage-1 reject, 1 stage-2 reject, 2 accept); index r * max_steps + (step - step0) */

@@ -117,7 +117,9 @@ def _stage1_uniform(seed, stream, replica, step):
     return np.float32((w >> 8) * 2.0 ** -24)
 
 
-def test_decisions_replay(raw):
+@pytest.mark.parametrize("split", [0, 3])
+def test_decisions_replay(raw, split):
+    """split 3: the exact stage walks each protein segment with 3 lanes per atom."""
     scale = (0.6, 0.6, 0.6, 0.3, 0.3, 0.3)  # larger moves: both stages reject
     w = _small(raw, move_scale=scale)
     cx, ff, params = w.complexes[0], w.ff, w.params
@@ -125,7 +127,7 @@ def test_decisions_replay(raw):
     with engine.Engine(ff, [cx], params) as eng:
         eng.mc_init()
         sur = engine.Surrogate(eng, hidden=128, batch=512, sample_cap=1 << 16,
-                               fallback_accept=0.0)
+                               fallback_accept=0.0, split=split)
         sur.collect(0, s0, exchange=True)
         losses = sur.train(150)
         assert losses[-1] < losses[0]

@@ -184,6 +184,25 @@ def test_fused_graph_equals_stepwise(raw):
         assert np.array_equal(a.state().view(np.uint8), b.state().view(np.uint8))
 
 
+@pytest.mark.parametrize("split,k", [(2, 3), (3, 2), (7, 1)])
+def test_protein_split_energies(raw, split, k):
+    """Lanes per atom > 1 (each walks part of every protein segment): every term still within
+    1e-5 of the FP64 oracle, contact counts exact."""
+    z, cx, ff = load_ref("1a07C1")
+    refmap = po.ref_map(ff, cx)
+    rng = np.random.default_rng(11 + split)
+    with engine.Engine(ff, [cx], abi.mc_params(steps_per_dump=10)) as eng:
+        eng.set_tile(k, 128, 0, split)
+        assert eng.tile()[3] == split
+        eng.mc_init()
+        for ip, il in ((0, 0), (2, 5)):
+            mm = np.zeros((7, 6), np.float32)
+            mm[:, :3] = rng.normal(0, 1.0, (7, 3))
+            mm[:, 3:] = rng.normal(0, 0.5, (7, 3))
+            worst = _energy_check(eng, ff, cx, 0, ip, il, mm, refmap)
+            assert worst.max() <= TOL, worst
+
+
 @pytest.mark.parametrize("chains", [3, 5])
 def test_concurrent_chains_give_the_same_chains(raw, chains):
     """The fused graph split into concurrent chains (streams) reproduces the single-chain run
@@ -320,8 +339,8 @@ def test_autotune_picks_a_tile_and_keeps_the_chains(raw, tmp_path):
         before = eng.state()
         res = autotune.tune(eng, cache_path=str(tmp_path / "cache.json"), repeats=1)
         assert not res["cached"]
-        k, ch, u = eng.tile()
-        assert [k, ch, u] == res["tile"]
+        k, ch, u, sp = eng.tile()
+        assert [k, ch, u] == res["tile"] and sp == 1
         assert all(m > 0 or m == -1 for m in res["ms"].values())
         after = eng.state()
         assert np.array_equal(before.view(np.uint8), after.view(np.uint8))
