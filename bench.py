@@ -21,6 +21,8 @@ delayed_acceptance (N = 1): the config-3 workload on the config-1 system (2,000 
            training samples, one epoch of Adam, then K intervals of delayed-acceptance and of
            plain steps from the same state, device-timed), at the configured moves and at 20x
            and 60x larger moves; surrogate RMSE, stage acceptances, per-temperature KS p-values.
+batched_screen (N = 1): config 2 (2,048 uneven ligands x 8 uneven pockets, 1,048,576 replicas)
+           in one context, one persistent launch per 10-step interval, autotuned tile.
 """
 from __future__ import annotations
 
@@ -296,6 +298,48 @@ def delayed_acceptance(w, dev, tile, scale_mult, intervals, burn=2000, iters=166
             "timing": "CUDA events on each engine's stream, L2 flushed between intervals"}
 
 
+def batched_screen(dev, intervals=3):
+    """Config 2: 2,048 ligands (10-64 atoms, 8 conformers) round-robin over 8 pockets (1,200-6,000
+    points, 4 conformers), 16 temperatures = 1,048,576 replicas in one context; every interval is
+    one graph-captured persistent launch over all complexes (10 steps) + exchange. Tile autotuned
+    on this batch; device time from CUDA events; FLOP at 36 per ligand-protein pair."""
+    import torch
+    from geaxdock_gpu_b200 import autotune, engine, system
+    t0 = time.perf_counter()
+    w = system.config(2, load_raw())
+    gen_s = time.perf_counter() - t0
+    pairs = sum(c.n_rep * c.lna * c.pnp for c in w.complexes)
+    with engine.Engine(w.ff, w.complexes, w.params, device=dev) as eng:
+        eng.mc_init()
+        eng.sync()
+        tuned = autotune.tune(eng, device=dev)
+        st = torch.cuda.ExternalStream(eng.cuda_stream(), device=dev)
+        spe = w.params.steps_per_exchange
+        per_dump = w.params.steps_per_dump // spe
+        eng.run_fused(0, spe, exchange=True)
+        eng.sync()
+        ms = []
+        for i in range(1, intervals + 1):
+            if i % per_dump == 0:
+                eng.reset_records()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            eng.run_fused(i * spe, spe, exchange=True)
+            e1.record(st)
+            eng.sync()
+            ms.append(e0.elapsed_time(e1))
+        tile = eng.tile()
+    avg = sum(ms) / len(ms)
+    return {"workload": "config2: 2048 ligands (L 10-64, 8 conformers) x 8 pockets (P 1200-6000, "
+                        "4 conformers), 16 T, 1,048,576 replicas, one persistent launch per interval",
+            "value": w.n_rep * spe / (avg * 1e-3), "unit": UNIT, "ms_per_interval": avg,
+            "intervals": intervals, "tflops_at_36_flop_per_pair": pairs * 36 * spe / (avg * 1e-3) / 1e12,
+            "tile": {"replicas_per_cta": tile[0], "chunk_points": tile[1], "unroll": tile[2],
+                     "split": tile[3], "cached": tuned["cached"]},
+            "generate_s": gen_s}
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     from geaxdock_gpu_b200 import abi, engine
@@ -439,6 +483,10 @@ def run_ours(args, rank, world, local_rank):
               "moves_x20": delayed_acceptance(w, dev, tile_used, 20.0, args.steps),
               "moves_x60": delayed_acceptance(w, dev, tile_used, 60.0, args.steps)}
 
+    screen = None
+    if world == 1 and not args.no_screen:
+        screen = batched_screen(dev)
+
     cpu = None
     if world == 1 and not args.no_cpu:
         cpu = cpu_baseline_sample(w)
@@ -457,7 +505,7 @@ def run_ours(args, rank, world, local_rank):
                       "parallelism": "replica shards, no collective" if world > 1 else "1 GPU"},
            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
            "gpu_launches": 2 * args.steps + args.steps // max(1, intervals_per_dump),
-           "delayed_acceptance": da}
+           "delayed_acceptance": da, "batched_screen": screen}
     print(json.dumps(out), flush=True)
 
 
@@ -490,6 +538,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-da", action="store_true", help="skip the delayed-acceptance runs")
+    ap.add_argument("--no-screen", action="store_true", help="skip the config-2 batched screen")
     ap.add_argument("--tile", default="", help="replicas_per_cta,chunk_points[,unroll] (default: tuned)")
     ap.add_argument("--profile-da", action="store_true",
                     help="only a short delayed-acceptance sequence on the config-1 system (20 "

@@ -147,7 +147,7 @@ __device__ __forceinline__ void pair_body(const float4 A, const float4 B,
   } else {
     a.ele.x = __fmaf_rn(ep.x, ri.x, a.ele.x);
   }
-  if (d2.x < f.near2 || (PAIR && d2.y < f.near2)) {
+  if ((PAIR ? fminf(d2.x, d2.y) : d2.x) < f.near2) {
     const float2 s1 = __fmul2_rn(f2(f.el1), r);
     const float2 gn =
         __ffma2_rn(__fmul2_rn(s1, s1), __ffma2_rn(f2(f.b1), s1, f2(f.a1)), f2(f.el0));
