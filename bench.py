@@ -335,8 +335,9 @@ def batched_screen(dev, intervals=3):
                         "4 conformers), 16 T, 1,048,576 replicas, one persistent launch per interval",
             "value": w.n_rep * spe / (avg * 1e-3), "unit": UNIT, "ms_per_interval": avg,
             "intervals": intervals, "tflops_at_36_flop_per_pair": pairs * 36 * spe / (avg * 1e-3) / 1e12,
-            "tile": {"replicas_per_cta": tile[0], "chunk_points": tile[1], "unroll": tile[2],
-                     "split": tile[3], "cached": tuned["cached"]},
+            "tile": {"replicas_per_cta_first_complex": tile[0], "chunk_points": tile[1],
+                     "unroll": tile[2], "split": tile[3], "threads": tile[4],
+                     "cached": tuned["cached"]},
             "generate_s": gen_s}
 
 
@@ -501,7 +502,7 @@ def run_ours(args, rank, world, local_rank):
                       "l2": "flushed between steps (256 MB write)",
                       "tile": {"replicas_per_cta": tile_used[0], "chunk_points": tile_used[1],
                                "unroll": tile_used[2], "split": tile_used[3],
-                               "source": tile_source},
+                               "threads": tile_used[4], "source": tile_source},
                       "parallelism": "replica shards, no collective" if world > 1 else "1 GPU"},
            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
            "gpu_launches": 2 * args.steps + args.steps // max(1, intervals_per_dump),

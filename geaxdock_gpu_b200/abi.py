@@ -112,7 +112,8 @@ class McParams(C.Structure):
 
 
 class Tile(C.Structure):
-    _fields_ = [("replicas_per_cta", I), ("chunk_points", I), ("unroll", I), ("split", I)]
+    _fields_ = [("replicas_per_cta", I), ("chunk_points", I), ("unroll", I), ("split", I),
+                ("threads", I)]
 
 
 class ReplicaState(C.Structure):

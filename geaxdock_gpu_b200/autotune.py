@@ -19,15 +19,21 @@ from .engine import Engine, check, lib
 DEFAULT_CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tile_cache.json")
 
 
-def candidates(lna: int) -> List[Tuple[int, int, int]]:
-    """Replicas per CTA that fill 128..256 lanes, chunk depths, unroll depths."""
+def candidates(lna: int, ragged: bool = False) -> List[Tuple[int, int, int, int, int]]:
+    """(replicas_per_cta, chunk_points, unroll, split, threads) candidates: one replica count for
+    every complex that fills 128..256 lanes for the largest ligand, and for a ragged batch also
+    CTAs of 128..256 threads that every complex fills with as many replicas as fit."""
     ks = sorted({max(1, t // lna) for t in (128, 160, 192, 224, 256)} | {1})
     ks = [k for k in ks if k * lna <= 256]
     out = []
-    for k in ks:
-        for chunk in (256, 512, 1024):
-            for unroll in (1, 2):
-                out.append((k, chunk, unroll))
+    for chunk in (256, 512, 1024):
+        for unroll in (1, 2):
+            for k in ks:
+                out.append((k, chunk, unroll, 1, 0))
+            if ragged:
+                for threads in (128, 192, 256):
+                    if threads >= lna:
+                        out.append((0, chunk, unroll, 1, threads))
     return out
 
 
@@ -46,10 +52,13 @@ def _device_name(device: int) -> str:
         return "cuda%d" % device
 
 
-def time_candidates(eng: Engine, cands: Sequence[Tuple[int, int, int]], repeats: int = 2):
+def time_candidates(eng: Engine, cands: Sequence[Tuple[int, ...]], repeats: int = 2):
     arr = (abi.Tile * len(cands))()
-    for i, (k, ch, u) in enumerate(cands):
+    for i, c in enumerate(cands):
+        k, ch, u = c[:3]
         arr[i].replicas_per_cta, arr[i].chunk_points, arr[i].unroll = k, ch, u
+        arr[i].split = c[3] if len(c) > 3 else 1
+        arr[i].threads = c[4] if len(c) > 4 else 0
     best = abi.Tile()
     ms = (C.c_float * len(cands))()
     fn = lib().gd_autotune
@@ -57,7 +66,8 @@ def time_candidates(eng: Engine, cands: Sequence[Tuple[int, int, int]], repeats:
                    C.POINTER(C.c_float)]
     fn.restype = C.c_int
     check(fn(eng.h, arr, len(cands), repeats, C.byref(best), ms))
-    return (best.replicas_per_cta, best.chunk_points, best.unroll), list(ms)
+    return (best.replicas_per_cta, best.chunk_points, best.unroll, best.split, best.threads), \
+        list(ms)
 
 
 def tune(eng: Engine, cache_path: Optional[str] = DEFAULT_CACHE, device: int = 0,
@@ -70,14 +80,15 @@ def tune(eng: Engine, cache_path: Optional[str] = DEFAULT_CACHE, device: int = 0
             cache = json.load(open(cache_path))
         except (OSError, ValueError):
             cache = {}
-    if key in cache and not force:
-        k, ch, u = cache[key]["tile"]
-        eng.set_tile(k, ch, u)
+    if key in cache and not force and len(cache[key]["tile"]) == 5:
+        eng.set_tile(*cache[key]["tile"])
         return dict(cache[key], cached=True)
     lna = max(c.lna for c in eng.complexes)
-    cands = candidates(lna)
+    ragged = len({c.lna for c in eng.complexes}) > 1
+    cands = candidates(lna, ragged)
     best, ms = time_candidates(eng, cands, repeats)
-    entry = {"tile": list(best), "ms": {"%d,%d,%d" % c: round(m, 4) for c, m in zip(cands, ms)}}
+    entry = {"tile": list(best),
+             "ms": {",".join(str(v) for v in c): round(m, 4) for c, m in zip(cands, ms)}}
     cache[key] = entry
     if cache_path:
         try:

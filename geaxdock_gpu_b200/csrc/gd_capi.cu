@@ -963,19 +963,33 @@ int gd_set_tile(gd_ctx *c, int k, const gd_tile *t) {
     return fail(GD_ERR_INVALID, "unroll must be 1, 2 or 4 (0 keeps the current value)");
   if (t->chunk_points < 4 || (t->chunk_points & 3) || t->chunk_points > 4096)
     return fail(GD_ERR_INVALID, "chunk_points must be a multiple of 4 in 4..4096");
-  if (t->replicas_per_cta < 1 || t->replicas_per_cta > GD_MAX_SLOTS)
-    return fail(GD_ERR_INVALID, "replicas_per_cta outside 1..%d", GD_MAX_SLOTS);
+  if (t->replicas_per_cta < 0 || t->replicas_per_cta > GD_MAX_SLOTS ||
+      (t->replicas_per_cta == 0 && t->threads == 0))
+    return fail(GD_ERR_INVALID, "replicas_per_cta outside 1..%d (0 only with threads)",
+                GD_MAX_SLOTS);
   if (t->split < 0 || t->split > 16) return fail(GD_ERR_INVALID, "split outside 0..16");
+  if (t->threads < 0 || t->threads > GD_MAX_TPB || (t->threads & 31))
+    return fail(GD_ERR_INVALID, "threads must be a multiple of 32 in 0..%d", GD_MAX_TPB);
   if (k < -1 || k >= c->n_complex) return fail(GD_ERR_INVALID, "bad complex index");
   const int S = t->split ? t->split : 1;
   if ((t->chunk_points / 2) < S)
     return fail(GD_ERR_INVALID, "chunk_points must hold at least two points per split");
   /* one block size per context: every complex's k must fit the block */
   std::vector<ComplexInfo> info = c->info;
-  for (int i = 0; i < c->n_complex; ++i)
-    if (k == -1 || k == i) info[i].k = std::min(t->replicas_per_cta, info[i].n_tmp * info[i].n_lig);
+  for (int i = 0; i < c->n_complex; ++i) {
+    if (!(k == -1 || k == i)) continue;
+    int kk = info[i].n_tmp * info[i].n_lig;
+    if (t->replicas_per_cta > 0) kk = std::min(kk, t->replicas_per_cta);
+    if (t->threads > 0) {
+      if (S * info[i].lna > t->threads)
+        return fail(GD_ERR_INVALID, "complex %d: split * lna exceeds threads", i);
+      kk = std::min(kk, t->threads / (S * info[i].lna));
+    }
+    info[i].k = std::min(kk, GD_MAX_SLOTS);
+  }
   int T = 32;
   for (auto &x : info) T = std::max(T, ((x.k * S * x.lna + 31) / 32) * 32);
+  if (t->threads > 0) T = std::max(T, t->threads);
   if (T > GD_MAX_TPB)
     return fail(GD_ERR_INVALID, "replicas_per_cta * split * lna exceeds %d", GD_MAX_TPB);
   c->info = info;
@@ -1022,7 +1036,7 @@ int gd_autotune(gd_ctx *c, const gd_tile *cand, int n_cand, int repeats, gd_tile
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  const gd_tile keep_tile = {c->info[0].k, c->chunk, c->unroll, c->split};
+  const gd_tile keep_tile = {c->info[0].k, c->chunk, c->unroll, c->split, c->threads};
   std::vector<int> keep_k;
   for (auto &x : c->info) keep_k.push_back(x.k);
   const int keep_threads = c->threads;
@@ -1072,6 +1086,7 @@ int gd_autotune(gd_ctx *c, const gd_tile *cand, int n_cand, int repeats, gd_tile
     *best = cand[best_i];
     best->unroll = c->unroll;
     best->split = c->split;
+    best->threads = cand[best_i].threads;
   } else {
     /* restore the tile in use before the probe */
     for (int i = 0; i < c->n_complex; ++i) c->info[i].k = keep_k[i];
@@ -1125,6 +1140,7 @@ int gd_get_tile(const gd_ctx *c, int k, gd_tile *t) {
   t->chunk_points = c->chunk;
   t->unroll = c->unroll;
   t->split = c->split;
+  t->threads = c->threads;
   return GD_OK;
 }
 

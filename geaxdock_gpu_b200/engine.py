@@ -187,10 +187,12 @@ class Engine:
         check(lib().gd_sync(self.h))
 
     def set_tile(self, replicas_per_cta: int, chunk_points: int, unroll: int = 0,
-                 split: int = 0, complex_index: int = -1):
+                 split: int = 0, threads: int = 0, complex_index: int = -1):
+        """threads > 0: every complex gets as many replicas as fill a CTA of that size
+        (replicas_per_cta > 0 caps them)."""
         t = abi.Tile()
         t.replicas_per_cta, t.chunk_points, t.unroll = replicas_per_cta, chunk_points, unroll
-        t.split = split
+        t.split, t.threads = split, threads
         check(lib().gd_set_tile(self.h, complex_index, C.byref(t)))
 
     def cuda_stream(self) -> int:
@@ -209,10 +211,10 @@ class Engine:
         check(lib().gd_set_wait_timeout(self.h, ns))
 
     def tile(self, complex_index=0):
-        """(replicas_per_cta, chunk_points, unroll, split)"""
+        """(replicas_per_cta of the complex, chunk_points, unroll, split, threads)"""
         t = abi.Tile()
         check(lib().gd_get_tile(self.h, complex_index, C.byref(t)))
-        return t.replicas_per_cta, t.chunk_points, t.unroll, t.split
+        return t.replicas_per_cta, t.chunk_points, t.unroll, t.split, t.threads
 
     # ---- results ----
     def records(self, r0=0, r1=None):

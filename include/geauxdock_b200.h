@@ -169,6 +169,11 @@ typedef struct {
                                segment (0 or 1: one lane per atom); replicas_per_cta * split *
                                atoms must fit one CTA. The energies' FP32 summation order depends
                                on it (results within the parity tolerance of each other). */
+  int threads;              /* CTA size (multiple of 32, <= 256); 0: the smallest that holds
+                               replicas_per_cta replicas of every complex. With threads > 0 each
+                               complex gets as many replicas as fill the CTA (at most
+                               replicas_per_cta when that is > 0): a ragged batch keeps its
+                               lanes busy whatever its ligands' sizes. */
 } gd_tile;
 
 /* Per-replica Monte Carlo state (checkpoint unit). */

@@ -227,6 +227,28 @@ def test_concurrent_chains_give_the_same_chains(raw, chains):
         assert ra.tobytes() == rb.tobytes()
 
 
+def test_fill_tile_gives_each_complex_its_own_replica_count(raw):
+    """threads > 0: every complex of a ragged batch gets as many replicas as fill the CTA; the
+    chains equal those of a uniform tile (the replica count per CTA does not enter the
+    arithmetic)."""
+    w = system.config(2, raw, n_ligands=6)
+    params = w.params
+    params.steps_per_dump = 40
+    with engine.Engine(w.ff, w.complexes, params) as a, \
+            engine.Engine(w.ff, w.complexes, params) as b:
+        a.set_tile(2, 256)
+        b.set_tile(0, 256, 0, 1, 256)
+        ks = [b.tile(i)[0] for i in range(len(w.complexes))]
+        for i, cx in enumerate(w.complexes):
+            assert ks[i] == min(cx.n_tmp * cx.n_lig, 256 // cx.lna), (i, ks[i], cx.lna)
+        assert b.tile()[4] == 256
+        for e in (a, b):
+            e.mc_init()
+            e.run_fused(0, 20, exchange=True)
+            e.sync()
+        assert a.state().tobytes() == b.state().tobytes()
+
+
 def test_batch_equals_alone(raw):
     """Config-2 style batch (uneven ligands and pockets): each complex's trajectory in the
     batch is bit-identical to running it alone with the same stream id and tile."""
@@ -339,8 +361,8 @@ def test_autotune_picks_a_tile_and_keeps_the_chains(raw, tmp_path):
         before = eng.state()
         res = autotune.tune(eng, cache_path=str(tmp_path / "cache.json"), repeats=1)
         assert not res["cached"]
-        k, ch, u, sp = eng.tile()
-        assert [k, ch, u] == res["tile"] and sp == 1
+        k, ch, u, sp, thr = eng.tile()
+        assert [k, ch, u, sp] == res["tile"][:4] and sp == 1
         assert all(m > 0 or m == -1 for m in res["ms"].values())
         after = eng.state()
         assert np.array_equal(before.view(np.uint8), after.view(np.uint8))
