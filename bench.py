@@ -335,10 +335,86 @@ def batched_screen(dev, intervals=3):
                         "4 conformers), 16 T, 1,048,576 replicas, one persistent launch per interval",
             "value": w.n_rep * spe / (avg * 1e-3), "unit": UNIT, "ms_per_interval": avg,
             "intervals": intervals, "tflops_at_36_flop_per_pair": pairs * 36 * spe / (avg * 1e-3) / 1e12,
-            "tile": {"replicas_per_cta_first_complex": tile[0], "chunk_points": tile[1],
+            "tile": {"replicas_per_cta": tile[0], "chunk_points": tile[1],
                      "unroll": tile[2], "split": tile[3], "threads": tile[4],
                      "cached": tuned["cached"]},
             "generate_s": gen_s}
+
+
+def screen_da(dev, move_mult=1.0, burn=100, steps=100, iters=1665):
+    """Config 4: delayed acceptance on the config-2 screen (2,048 ligands x 8 pockets,
+    1,048,576 replicas). One network for the batch, conditioned on per-pocket features and a
+    learned embedding per (ligand, pocket conformer, ligand conformer); trained on the
+    proposals of `burn` plain burn-in steps; per-ligand fallback to plain steps. Then `steps`
+    delayed-acceptance steps and, from the same state, `steps` plain steps, device-timed; the
+    best (lowest) energy of each ligand's replicas at the end is compared between the runs."""
+    import torch
+    from geaxdock_gpu_b200 import autotune, engine, system
+    w = system.config(2, load_raw())
+    p = w.params
+    p.record = 0
+    for i in range(6):
+        p.move_scale[i] *= move_mult
+    spe = p.steps_per_exchange
+    with engine.Engine(w.ff, w.complexes, p, device=dev) as b, \
+            engine.Engine(w.ff, w.complexes, p, device=dev) as a:
+        b.mc_init()
+        b.sync()
+        autotune.tune(b, device=dev)
+        a.set_tile(*b.tile())
+        sur = engine.Surrogate(b, fallback_accept=0.5, fallback_window=2000)
+        t0 = time.perf_counter()
+        sur.collect(0, burn, exchange=True)
+        b.sync()
+        collect_s = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        losses = sur.train(iters)
+        train_s = time.perf_counter() - t0
+        a.mc_init()
+        start = b.state()
+        a.set_state(start)
+        a.sync()
+        sa = torch.cuda.ExternalStream(a.cuda_stream(), device=dev)
+        sb = torch.cuda.ExternalStream(b.cuda_stream(), device=dev)
+        da_ms = plain_ms = 0.0
+        for s in range(burn, burn + steps, spe):
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+            e[0].record(sb)
+            sur.run(s, spe, exchange=True)
+            e[1].record(sb)
+            b.sync()
+            e[2].record(sa)
+            a.run_fused(s, spe, exchange=True)
+            e[3].record(sa)
+            a.sync()
+            da_ms += e[0].elapsed_time(e[1])
+            plain_ms += e[2].elapsed_time(e[3])
+        stats = sur.stats()
+        fa, fb = a.state(), b.state()
+        offs = list(a.offsets)
+    best_a, best_b = [], []
+    for k, cx in enumerate(w.complexes):
+        sl = slice(offs[k], offs[k] + cx.n_rep)
+        best_a.append(float(fa["energy_old"]["e"][sl, 9].min()))
+        best_b.append(float(fb["energy_old"]["e"][sl, 9].min()))
+    best_a, best_b = np.array(best_a), np.array(best_b)
+    n_off = sum(1 for s_ in stats if not s_["active"])
+    prop = sum(s_["proposed"] for s_ in stats)
+    passed = sum(s_["passed"] for s_ in stats)
+    acc = sum(s_["accepted"] for s_ in stats)
+    rs = w.n_rep * steps
+    return {"workload": "config4: config-2 screen with delayed acceptance",
+            "move_scale": [p.move_scale[i] for i in range(6)],
+            "value": rs / (da_ms * 1e-3), "unit": UNIT,
+            "plain_same_state": rs / (plain_ms * 1e-3), "speedup_vs_plain": plain_ms / da_ms,
+            "stage1_pass": passed / max(1, prop), "stage2_accept": acc / max(1, passed),
+            "ligands_fallen_back_to_plain": n_off, "ligands": len(w.complexes),
+            "collect_steps": burn, "collect_s": collect_s, "train_iterations": iters,
+            "train_s": train_s, "train_loss_first_last": [float(losses[0]), float(losses[-1])],
+            "best_energy_mean_da_vs_plain": [float(best_b.mean()), float(best_a.mean())],
+            "best_energy_median_abs_diff": float(np.median(np.abs(best_b - best_a))),
+            "best_energy_corr": float(np.corrcoef(best_a, best_b)[0, 1]),
+            "steps": steps}
 
 
 def run_ours(args, rank, world, local_rank):
@@ -546,8 +622,14 @@ def main():
                          "collect steps, 20 Adam steps, 20 DA steps, 10 plain steps), for "
                          "profiler launch lists; prints its statistics")
     ap.add_argument("--move-mult", type=float, default=1.0,
-                    help="--profile-da: move scales multiplied by this factor")
+                    help="--profile-da / --screen-da: move scales multiplied by this factor")
+    ap.add_argument("--screen-da", action="store_true",
+                    help="only the config-4 run (delayed acceptance on the config-2 screen); "
+                         "prints its own JSON line")
     args = ap.parse_args()
+    if args.screen_da:
+        print(json.dumps(screen_da(0, args.move_mult)), flush=True)
+        return
     if args.profile_da:
         profile_da(args)
         return

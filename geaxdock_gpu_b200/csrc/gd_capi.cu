@@ -108,6 +108,7 @@ struct gd_ctx {
   gd_mc_params mc{};
   int n_complex = 0, n_rep = 0, n_groups = 0;
   int threads = 256, chunk = 512, unroll = 2, split = 1, num_sms = 148;
+  int fill_threads = 0, fill_cap = 0; /* the last gd_set_tile in fill mode (threads > 0) */
   std::vector<ComplexInfo> info;
   std::vector<void *> allocs;
   GdForceConst fc{};
@@ -996,6 +997,8 @@ int gd_set_tile(gd_ctx *c, int k, const gd_tile *t) {
   c->threads = T;
   c->chunk = t->chunk_points;
   c->split = S;
+  c->fill_threads = t->threads;
+  c->fill_cap = t->threads > 0 ? t->replicas_per_cta : 0;
   if (t->unroll) c->unroll = t->unroll;
   c->tile_gen += 1;
   build_tiles(c, 0, c->n_rep - 1, c->full_tiles);
@@ -1037,6 +1040,7 @@ int gd_autotune(gd_ctx *c, const gd_tile *cand, int n_cand, int repeats, gd_tile
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   const gd_tile keep_tile = {c->info[0].k, c->chunk, c->unroll, c->split, c->threads};
+  const int keep_fill_threads = c->fill_threads, keep_fill_cap = c->fill_cap;
   std::vector<int> keep_k;
   for (auto &x : c->info) keep_k.push_back(x.k);
   const int keep_threads = c->threads;
@@ -1094,11 +1098,19 @@ int gd_autotune(gd_ctx *c, const gd_tile *cand, int n_cand, int repeats, gd_tile
     c->chunk = keep_tile.chunk_points;
     c->unroll = keep_tile.unroll;
     c->split = keep_tile.split;
+    c->fill_threads = keep_fill_threads;
+    c->fill_cap = keep_fill_cap;
     c->tile_gen += 1;
     build_tiles(c, 0, c->n_rep - 1, c->full_tiles);
     if (rc == GD_OK) rc = fail(GD_ERR_INVALID, "gd_autotune: no candidate fits this batch");
   }
   return rc;
+}
+
+int gd_get_replicas_per_cta(const gd_ctx *c, int k, int *n) {
+  if (!c || !n || k < 0 || k >= c->n_complex) return fail(GD_ERR_INVALID, "bad argument");
+  *n = c->info[k].k;
+  return GD_OK;
 }
 
 int gd_set_concurrency(gd_ctx *c, int plain_chains, int da_chains) {
@@ -1136,11 +1148,13 @@ int gd_set_wait_timeout(gd_ctx *c, long long ns) {
 
 int gd_get_tile(const gd_ctx *c, int k, gd_tile *t) {
   if (!c || !t || k < 0 || k >= c->n_complex) return fail(GD_ERR_INVALID, "bad argument");
-  t->replicas_per_cta = c->info[k].k;
+  /* the tile as set: in fill mode the cap (0: none) and the CTA size, so that gd_set_tile of
+   * the result restores it; gd_get_replicas_per_cta gives each complex's count */
+  t->replicas_per_cta = c->fill_threads > 0 ? c->fill_cap : c->info[k].k;
   t->chunk_points = c->chunk;
   t->unroll = c->unroll;
   t->split = c->split;
-  t->threads = c->threads;
+  t->threads = c->fill_threads;
   return GD_OK;
 }
 
@@ -2137,7 +2151,7 @@ int gd_sur_create(gd_ctx *c, const gd_sur_params *p) {
     da_free(c);
     return fail(GD_ERR_NOMEM, "network allocation failed");
   }
-  const int rows = std::max(c->n_rep, p->batch);
+  const int rows = p->batch; /* DA steps keep their rows in shared memory */
   if (gd::mlp_reserve(d->net, rows)) {
     da_free(c);
     return fail(GD_ERR_NOMEM, "network work buffers (%d rows)", rows);

@@ -70,6 +70,7 @@ def lib() -> C.CDLL:
         "gd_get_stream": [vp, C.POINTER(vp)],
         "gd_set_rng_stream": [vp, C.c_int, C.c_int],
         "gd_set_concurrency": [vp, C.c_int, C.c_int],
+        "gd_get_replicas_per_cta": [vp, C.c_int, ip],
         "gd_set_wait_timeout": [vp, C.c_longlong],
         "gd_sur_create": [vp, C.POINTER(abi.SurParams)],
         "gd_sur_collect": [vp, C.c_int, C.c_int, C.c_int],
@@ -210,8 +211,14 @@ class Engine:
     def set_wait_timeout(self, ns: int):
         check(lib().gd_set_wait_timeout(self.h, ns))
 
+    def replicas_per_cta(self, complex_index=0) -> int:
+        n = C.c_int()
+        check(lib().gd_get_replicas_per_cta(self.h, complex_index, C.byref(n)))
+        return n.value
+
     def tile(self, complex_index=0):
-        """(replicas_per_cta of the complex, chunk_points, unroll, split, threads)"""
+        """The tile as set: (replicas_per_cta, chunk_points, unroll, split, threads); in fill
+        mode (threads > 0) replicas_per_cta is the cap (0: none)."""
         t = abi.Tile()
         check(lib().gd_get_tile(self.h, complex_index, C.byref(t)))
         return t.replicas_per_cta, t.chunk_points, t.unroll, t.split, t.threads

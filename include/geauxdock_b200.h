@@ -209,6 +209,8 @@ int gd_replica_offset(const gd_ctx *ctx, int complex_index, int *offset);
 /* Tile of the fused kernel for one complex (-1: all); one CTA size per context. */
 int gd_set_tile(gd_ctx *ctx, int complex_index, const gd_tile *tile);
 int gd_get_tile(const gd_ctx *ctx, int complex_index, gd_tile *tile);
+/* replicas per CTA the tile gives complex k (differs between complexes in fill mode) */
+int gd_get_replicas_per_cta(const gd_ctx *ctx, int complex_index, int *replicas);
 /* Autotuner: times each candidate tile by evaluating the energies of the replicas' current
  * poses (the pair loop of gd_mc_run, without touching the chains), `repeats` launches each,
  * applies the fastest to every complex and returns it with its mean launch time (ms) in

@@ -238,10 +238,10 @@ def test_fill_tile_gives_each_complex_its_own_replica_count(raw):
             engine.Engine(w.ff, w.complexes, params) as b:
         a.set_tile(2, 256)
         b.set_tile(0, 256, 0, 1, 256)
-        ks = [b.tile(i)[0] for i in range(len(w.complexes))]
+        ks = [b.replicas_per_cta(i) for i in range(len(w.complexes))]
         for i, cx in enumerate(w.complexes):
             assert ks[i] == min(cx.n_tmp * cx.n_lig, 256 // cx.lna), (i, ks[i], cx.lna)
-        assert b.tile()[4] == 256
+        assert b.tile() == (0, 256, 2, 1, 256)
         for e in (a, b):
             e.mc_init()
             e.run_fused(0, 20, exchange=True)
