@@ -10,11 +10,12 @@ synthetic data. One bench step = one exchange interval: 10 MC steps of every rep
 ours:      device time from CUDA events recorded on the library's own stream around each
            step, L2 flushed between steps (outside the events), max over ranks; `e2e` is a
            whole run through the C ABI from host buffers (gd_create uploads, init, K steps,
-           record download) timed on the host; `cpu_baseline` is the oracle's FP32 OpenMP
-           restatement on a bounded sample (rank 0, N = 1).
-reference: the reference's path restated on the host cores (the reference's own hot path is
-           GPU-only and its CPU port does not build): the oracle's FP32 OpenMP Monte Carlo on
-           a bounded sample per step, all host threads, same metric.
+           record download) timed on the host; `cpu_baseline` is the reference's own step code
+           on the host cores (as the reference arm) on a bounded sample (rank 0, N = 1).
+reference: the reference's own MonteCarlo_d step functions (Move_d, CalcEnergy_d, CalcMcc_d,
+           Accept_d, RecordLigand_d) compiled for the CPU from its sources (oracle/_ref/refpin),
+           one process per host core, a bounded replica sample per step, same metric; the
+           oracle's FP32 OpenMP restatement when that build is absent.
 Multi-GPU (torchrun): every rank runs its own config-1 system (own RNG stream), no data-path
 collective (replicas shard without exchange across shards): weak scaling.
 delayed_acceptance (N = 1): the config-3 workload on the config-1 system (2,000 burn-in steps of
@@ -132,14 +133,26 @@ def algorithmic_flops_per_replica_step(eng, w, n_sample=24):
 
 
 def cpu_baseline_sample(w, seconds=12.0, nthreads=0):
-    """Oracle FP32 OpenMP restatement on a bounded replica sample of the same workload."""
-    from oracle import pyoracle as po
+    """The reference's own MonteCarlo_d step code compiled for the CPU (oracle/_ref/refpin, one
+    process per host core) on a bounded replica sample of the same workload; the oracle's FP32
+    OpenMP restatement when that build is absent."""
+    from oracle import pyoracle as po, refbench
     cx, ff = w.complexes[0], w.ff
-    params = w.params
+    params = type(w.params).from_buffer_copy(w.params)
     params.record = 0
+    nt = nthreads or po.max_threads()
+    if refbench.available():
+        probe = refbench.run(cx, ff, params, n_rep=nt, steps=1, procs=nt)
+        rate = probe["replica_steps"] / max(probe["seconds"], 1e-3)
+        n_rep = int(min(cx.n_rep, max(nt, nt * round(seconds * rate / 10 / nt))))
+        r = refbench.run(cx, ff, params, n_rep=n_rep, steps=10, procs=nt)
+        return {"value": r["replica_steps"] / r["seconds"], "unit": UNIT, "cores": r["processes"],
+                "kind": "reference",
+                "sample": "%d replicas x 10 MC steps of the config-1 system through the reference's "
+                          "MonteCarlo_d step functions (oracle/_ref/refpin), one process per core, "
+                          "slowest process %.1f s" % (n_rep, r["seconds"])}
     mc = po.MC(ff, cx, params, stream=0, precision=32)
     mc.init()
-    nt = nthreads or po.max_threads()
     t0 = time.perf_counter()
     mc.run_range(0, nt, 0, 0, 1, nt)  # probe: one step on nt replicas
     rate = nt / max(time.perf_counter() - t0, 1e-3)  # replica-steps/s
@@ -152,40 +165,64 @@ def cpu_baseline_sample(w, seconds=12.0, nthreads=0):
 
 
 def run_reference(args, rank, world):
+    """The reference arm: the reference's own MonteCarlo_d step code on the host cores
+    (oracle/_ref/refpin, one process per core; the oracle's FP32 OpenMP port when that build is
+    absent), each bench step a bounded replica sample x 10 MC steps of the config-1 system."""
     if rank != 0:
         return
-    from oracle import pyoracle as po
+    from oracle import pyoracle as po, refbench
     w = workload(42)
     cx, ff, params = w.complexes[0], w.ff, w.params
     params.record = 0
     nt = po.max_threads()
-    mc = po.MC(ff, cx, params, stream=0, precision=32)
-    mc.init()
-    t0 = time.perf_counter()
-    mc.run_range(0, nt, 0, 0, 1, nt)
-    per_batch = max(time.perf_counter() - t0, 1e-3)  # one step of nt replicas
-    n_rep = int(min(cx.n_rep, max(nt, nt * int(0.8 / (10 * per_batch)))))
+    use_ref = refbench.available()
+    if use_ref:
+        probe = refbench.run(cx, ff, params, n_rep=nt, steps=1, procs=nt)
+        rate = probe["replica_steps"] / max(probe["seconds"], 1e-3)
+        n_rep = int(min(cx.n_rep, max(nt, nt * int(0.8 * rate / 10 / nt))))
+
+        def one_step(s2):
+            r = refbench.run(cx, ff, params, n_rep=n_rep, steps=10, procs=nt, seed=42 + s2)
+            return r["seconds"], r["replica_steps"]
+    else:
+        mc = po.MC(ff, cx, params, stream=0, precision=32)
+        mc.init()
+        t0 = time.perf_counter()
+        mc.run_range(0, nt, 0, 0, 1, nt)
+        per_batch = max(time.perf_counter() - t0, 1e-3)  # one step of nt replicas
+        n_rep = int(min(cx.n_rep, max(nt, nt * int(0.8 / (10 * per_batch)))))
+
+        def one_step(s2):
+            t0 = time.perf_counter()
+            mc.run_range(0, n_rep, 0, s2, 10, nt)
+            return time.perf_counter() - t0, n_rep * 10
     s2 = 0
     for _ in range(args.warmup):
-        mc.run_range(0, n_rep, 0, s2, 10, nt)
+        one_step(s2)
         s2 += 10
-    times = []
+    times, done = [], 0
     for _ in range(args.steps):
-        t0 = time.perf_counter()
-        mc.run_range(0, n_rep, 0, s2, 10, nt)
-        times.append(time.perf_counter() - t0)
+        dt, n = one_step(s2)
+        times.append(dt)
+        done += n
         s2 += 10
     tot = sum(times)
-    value = n_rep * 10 * args.steps / tot
+    value = done / tot
+    kind = "reference" if use_ref else "port"
+    sample = ("%d replicas x 10 MC steps per bench step through the reference's MonteCarlo_d step "
+              "functions compiled for the CPU (oracle/_ref/refpin), one process per core" % n_rep
+              if use_ref else "%d of 6820 replicas x 10 MC steps per bench step (oracle FP32 "
+              "OpenMP port)" % n_rep)
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
            "data": "synthetic (seeded, config-1 shapes)", "impl": "reference",
            "config": {"workload": "config1: P=3000 x 11 conf, L=40 x 31 conf, T=20, 6820 "
-                                  "replicas, gaussian moves, exchange/10",
+                                  "replicas (reference: its own uniform moves; the exchange, "
+                                  "< 0.2 % of a step, not timed)",
                       "replicas_sampled": n_rep},
-           "cpu_baseline": {"value": value, "unit": UNIT, "cores": nt, "kind": "port",
-                            "sample": "%d of 6820 replicas x 10 MC steps per bench step" % n_rep},
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": nt, "kind": kind,
+                            "sample": sample},
            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
