@@ -589,7 +589,8 @@ def run_ours(args, rank, world, local_rank):
         e2e = {"value": rs_per_step * args.steps / dt, "unit": UNIT,
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                "scope": "gd_create + gd_mc_init + K x (gd_mc_run + gd_exchange + gd_get_etotal)"
-                        " + gd_get_records_raw + gd_destroy, host wall clock"}
+                        " + gd_get_record_counts + gd_get_records_raw (filled rows) + gd_destroy,"
+                        " host wall clock"}
 
     da = None
     if world == 1 and not args.no_da:

@@ -1310,12 +1310,29 @@ int gd_get_records_raw(gd_ctx *c, gd_record_step *steps, int *next_ptr, int r0, 
   if (!c->mc.record || !c->d_rec) return fail(GD_ERR_STATE, "records are disabled");
   int rc = check_range(c, r0, r1);
   if (rc) return rc;
-  if (cap != c->rec_cap) return fail(GD_ERR_INVALID, "cap %d != record capacity %d", cap, c->rec_cap);
+  if (cap < 1 || cap > c->rec_cap)
+    return fail(GD_ERR_INVALID, "cap %d outside 1..record capacity %d", cap, c->rec_cap);
   const int n = r1 - r0 + 1;
   CK(cudaStreamSynchronize(c->stream));
-  CK(cudaMemcpy(steps, c->d_rec + (size_t)r0 * cap, sizeof(gd_record_step) * (size_t)n * cap,
-                cudaMemcpyDeviceToHost));
+  const size_t rs = sizeof(gd_record_step);
+  if (cap == c->rec_cap)
+    CK(cudaMemcpy(steps, c->d_rec + (size_t)r0 * cap, rs * (size_t)n * cap,
+                  cudaMemcpyDeviceToHost));
+  else /* the first cap records of each replica only */
+    CK(cudaMemcpy2D(steps, rs * cap, c->d_rec + (size_t)r0 * c->rec_cap, rs * c->rec_cap,
+                    rs * cap, n, cudaMemcpyDeviceToHost));
   CK(cudaMemcpy(next_ptr, c->d_rec_next + r0, sizeof(int) * n, cudaMemcpyDeviceToHost));
+  return GD_OK;
+}
+
+int gd_get_record_counts(gd_ctx *c, int *next_ptr, int r0, int r1) {
+  if (!c || !next_ptr) return fail(GD_ERR_INVALID, "null argument");
+  if (!c->mc.record || !c->d_rec) return fail(GD_ERR_STATE, "records are disabled");
+  int rc = check_range(c, r0, r1);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaMemcpy(next_ptr, c->d_rec_next + r0, sizeof(int) * (r1 - r0 + 1),
+                cudaMemcpyDeviceToHost));
   return GD_OK;
 }
 

@@ -59,6 +59,7 @@ def lib() -> C.CDLL:
         "gd_sync": [vp],
         "gd_get_records": [vp, vp, C.c_int, C.c_int],
         "gd_get_records_raw": [vp, vp, vp, C.c_int, C.c_int, C.c_int],
+        "gd_get_record_counts": [vp, vp, C.c_int, C.c_int],
         "gd_get_etotal": [vp, fp, C.c_int, C.c_int],
         "gd_get_replicas": [vp, vp, C.c_int, C.c_int],
         "gd_get_state": [vp, vp, C.c_int, C.c_int],
@@ -225,11 +226,15 @@ class Engine:
 
     # ---- results ----
     def records(self, r0=0, r1=None):
+        """(steps [n, m], next_ptr [n]): the filled records of each replica, m = the largest
+        count (only those rows cross the bus)."""
         r1 = self.n_rep - 1 if r1 is None else r1
         n = r1 - r0 + 1
-        steps = np.zeros((n, self.cap), abi.RECORD_DTYPE)
         nxt = np.zeros(n, np.int32)
-        check(lib().gd_get_records_raw(self.h, _p(steps), _p(nxt), r0, r1, self.cap))
+        check(lib().gd_get_record_counts(self.h, _p(nxt), r0, r1))
+        m = int(min(self.cap, max(1, nxt.max(initial=0))))
+        steps = np.empty((n, m), abi.RECORD_DTYPE)
+        check(lib().gd_get_records_raw(self.h, _p(steps), _p(nxt), r0, r1, m))
         return steps, nxt
 
     def lig_records(self, r0=0, r1=None) -> bytes:

@@ -258,9 +258,13 @@ int gd_get_stream(gd_ctx *ctx, void **stream);
 /* Copies LigRecord-identical records (capacity steps_per_dump + 1 must equal
  * GD_STEPS_PER_DUMP + 1) for rep_begin..rep_end into host[0..]. */
 int gd_get_records(gd_ctx *ctx, gd_lig_record *host, int rep_begin, int rep_end);
-/* Same data for any capacity: steps[(r - rep_begin) * cap + i], next_ptr[r - rep_begin]. */
+/* Same data for any record capacity: the first `cap` (1..steps_per_dump + 1) records of each
+ * replica, steps[(r - rep_begin) * cap + i], and next_ptr[r - rep_begin]; a cap just above the
+ * largest gd_get_record_counts value copies only the filled rows. */
 int gd_get_records_raw(gd_ctx *ctx, gd_record_step *steps, int *next_ptr, int rep_begin,
                        int rep_end, int cap);
+/* Records held per replica (next_ptr) for rep_begin..rep_end. */
+int gd_get_record_counts(gd_ctx *ctx, int *next_ptr, int rep_begin, int rep_end);
 int gd_get_etotal(gd_ctx *ctx, float *etotal, int rep_begin, int rep_end);
 int gd_get_replicas(gd_ctx *ctx, gd_replica *replicas, int rep_begin, int rep_end);
 int gd_get_state(gd_ctx *ctx, gd_replica_state *state, int rep_begin, int rep_end);
