@@ -1857,7 +1857,7 @@ gd::GdDaDev da_args(gd_ctx *c) {
   a.pass = d->d_pass;
   a.plain = d->d_plain;
   a.theta = d->net.theta;
-  a.wh = d->net.wh;
+  a.wf = d->net.wf;
   a.L = d->net.L;
   a.mu = d->net.mu;
   a.sigma = d->net.sigma;

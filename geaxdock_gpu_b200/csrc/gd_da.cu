@@ -105,17 +105,20 @@ __global__ void __launch_bounds__(256) front_kernel(GdDaDev d, int mode, int ste
   extern __shared__ __align__(128) unsigned char fsm[];
   __shared__ int cf[FR];
   __shared__ float ys[FR];
-  bf16 *xs = reinterpret_cast<bf16 *>(fsm);
-  bf16 *act = xs + FR * D::LDX;
-  float *stg = reinterpret_cast<float *>(act + FR * D::LDA);
+  /* a row's proposal, parked here across the network: pose, u1, u2 / complex, conformer */
+  __shared__ float rowf[FR][8];
+  __shared__ int rowi[FR][2];
+  const fwd::Smem<NT> sm(fsm);
+  bf16 *xs = sm.xs;
   const int tid = threadIdx.x;
+  if (mode != GD_DA_COLLECT) fwd::stage_params<NT>(sm, d.theta, d.L, tid);
   const int r = r_begin + blockIdx.x * FR + tid; /* the row's replica (threads < FR) */
   const int step = cur_step(d, step0);
-  float mm[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-  float u1 = 0.0f, u2 = 0.0f;
-  int ci = 0, lc = 0;
   if (tid < FR) {
     bf16 *row = xs + tid * D::LDX;
+    float mm[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    float u1 = 0.0f, u2 = 0.0f;
+    int ci = 0, lc = 0;
     if (r < r_end) {
       ci = d.rep_cx[r];
       const GdDevComplex &cx = d.cx[ci];
@@ -140,18 +143,29 @@ __global__ void __launch_bounds__(256) front_kernel(GdDaDev d, int mode, int ste
       for (int v = 0; v < 8; ++v) dst[v] = make_uint4(0u, 0u, 0u, 0u);
       cf[tid] = -1;
     }
+#pragma unroll
+    for (int i = 0; i < 6; ++i) rowf[tid][i] = mm[i];
+    rowf[tid][6] = u1;
+    rowf[tid][7] = u2;
+    rowi[tid][0] = ci;
+    rowi[tid][1] = lc;
   }
+  /* the first weight fragments are in flight while warp 0 finishes the proposals */
+  fwd::Ring<NT> ring;
+  if (mode != GD_DA_COLLECT) fwd::prefetch_first<NT>(ring, d.wf, tid);
   __syncthreads();
   if (mode != GD_DA_COLLECT) {
     fwd::fill_embedding<NT>(xs, cf, d.theta, d.L, tid);
     __syncthreads();
-    fwd::rows_forward<NT>(xs, act, stg, d.theta, d.wh, d.L, ys, tid);
+    fwd::rows_forward<NT>(sm, ring, d.wf, ys, tid);
   }
   if (tid >= FR || r >= r_end) return;
   if (mode == GD_DA_CURRENT) {
     d.s_cur[r] = __fmaf_rn(ys[tid], d.sigma, d.mu);
     return;
   }
+  const int ci = rowi[tid][0], lc = rowi[tid][1];
+  const float u1 = rowf[tid][6], u2 = rowf[tid][7];
   const bool act_on = mode == GD_DA_STEP && d.active[ci];
   float sn = d.s_cur[r];
   int pass = 1;
@@ -171,7 +185,7 @@ __global__ void __launch_bounds__(256) front_kernel(GdDaDev d, int mode, int ste
     const int pos = d.group_b0[g] + atomicAdd(cnt + g, 1);
     d.pose_rep[pos] = r;
 #pragma unroll
-    for (int i = 0; i < 6; ++i) d.pose_mm[(size_t)pos * 6 + i] = mm[i];
+    for (int i = 0; i < 6; ++i) d.pose_mm[(size_t)pos * 6 + i] = rowf[tid][i];
     d.pose_lc[pos] = lc;
   } else if (d.tr_flag) {
     const int ti = step - d.tr_step0;

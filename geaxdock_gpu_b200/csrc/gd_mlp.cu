@@ -233,6 +233,37 @@ __global__ void to_bf16(const float *__restrict__ a, bf16 *__restrict__ b, size_
   if (i < n) b[i] = __float2bfloat16_rn(a[i]);
 }
 
+/* Fragment-ordered BF16 copy of W1, W2, W3 for the fused forward (H = 64 NT8, NT8 = 2 or 4):
+ * in each layer block, element (((ks 8 + w) 32 + lane) NT8 + j) 4 + q holds W[k][n] with
+ * k = 16 ks + 2 (lane % 4) + (q % 2) + 8 (q / 2) and n = 8 (NT8 w + j) + lane / 4, the
+ * m16n8k16 B-operand fragment {b0, b1, b2, b3} of lane `lane` for 8-column tile j of warp w at
+ * k-step ks, so that a lane's fragments of one k-step are NT8 x 8 contiguous bytes. */
+__global__ void to_frag(const float *__restrict__ theta, MlpLayout L, bf16 *__restrict__ wf) {
+  const size_t H = L.hidden, n1 = (size_t)GD_MLP_IN * H, i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i >= n1 + 2 * H * H) return;
+  size_t e = i;
+  const float *W = theta + L.w1;
+  if (e >= n1 + H * H) {
+    e -= n1 + H * H;
+    W = theta + L.w3;
+  } else if (e >= n1) {
+    e -= n1;
+    W = theta + L.w2;
+  }
+  const int nt8 = (int)(H / 64);
+  const int q = (int)(e & 3);
+  size_t t = e >> 2;
+  const int j = (int)(t % nt8);
+  t /= nt8;
+  const int lane = (int)(t & 31);
+  t >>= 5;
+  const int w = (int)(t & 7);
+  const size_t ks = t >> 3;
+  const size_t k = 16 * ks + 2 * (lane & 3) + (q & 1) + 8 * (q >> 1);
+  const size_t n = 8 * ((size_t)nt8 * w + j) + (lane >> 2);
+  wf[i] = __float2bfloat16_rn(W[k * H + n]);
+}
+
 /* uniform(-scale, scale) from Philox, keyed by (seed, tensor id) */
 __global__ void init_uniform(float *p, size_t n, float scale, uint32_t tensor, uint64_t seed) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -247,18 +278,20 @@ template <int NT>
 __global__ void __launch_bounds__(256) fused_forward(const bf16 *__restrict__ X,
                                                      const int *__restrict__ conf,
                                                      const float *__restrict__ theta,
-                                                     const bf16 *__restrict__ wh, MlpLayout L,
+                                                     const bf16 *__restrict__ wf, MlpLayout L,
                                                      int rows, float *__restrict__ y) {
   using D = fwd::Dims<NT>;
   constexpr int FR = fwd::FR;
   extern __shared__ __align__(128) unsigned char fsm[];
   __shared__ int cf[FR];
   __shared__ float ys[FR];
-  bf16 *xs = reinterpret_cast<bf16 *>(fsm);
-  bf16 *act = xs + FR * D::LDX;
-  float *stg = reinterpret_cast<float *>(act + FR * D::LDA);
+  const fwd::Smem<NT> sm(fsm);
+  bf16 *xs = sm.xs;
   const int tid = threadIdx.x;
   const int row0 = blockIdx.x * FR;
+  fwd::Ring<NT> ring;
+  fwd::prefetch_first<NT>(ring, wf, tid);
+  fwd::stage_params<NT>(sm, theta, L, tid);
   for (int i = tid; i < FR * 8; i += 256) {
     const int r = i >> 3, c = i & 7;
     uint4 v = make_uint4(0u, 0u, 0u, 0u);
@@ -269,7 +302,7 @@ __global__ void __launch_bounds__(256) fused_forward(const bf16 *__restrict__ X,
   __syncthreads();
   fwd::fill_embedding<NT>(xs, cf, theta, L, tid);
   __syncthreads();
-  fwd::rows_forward<NT>(xs, act, stg, theta, wh, L, ys, tid);
+  fwd::rows_forward<NT>(sm, ring, wf, ys, tid);
   if (tid < FR && row0 + tid < rows) y[row0 + tid] = ys[tid];
 }
 
@@ -284,6 +317,10 @@ inline int blocks(size_t n, int t = 256) { return (int)((n + t - 1) / t); }
 int mlp_refresh_bf16(Mlp &n, cudaStream_t s) {
   const size_t nw = n.L.b4; /* W1..w4 region; biases converted too, unused */
   to_bf16<<<blocks(nw), 256, 0, s>>>(n.theta, n.wh, nw);
+  if (n.wf) {
+    const size_t H = n.L.hidden;
+    to_frag<<<blocks((size_t)GD_MLP_IN * H + 2 * H * H), 256, 0, s>>>(n.theta, n.L, n.wf);
+  }
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
@@ -293,6 +330,9 @@ int mlp_create(Mlp &n, int hidden, int n_emb, uint64_t seed, cudaStream_t s) {
   const size_t T = n.L.total;
   if (cudaMalloc(&n.theta, T * 4) || cudaMalloc(&n.grad, T * 4) || cudaMalloc(&n.m, T * 4) ||
       cudaMalloc(&n.v, T * 4) || cudaMalloc(&n.wh, n.L.b4 * 2) || cudaMalloc(&n.loss, 16))
+    return -3;
+  if ((hidden == 128 || hidden == 256) &&
+      cudaMalloc(&n.wf, ((size_t)GD_MLP_IN * hidden + 2 * (size_t)hidden * hidden) * 2))
     return -3;
   cudaMemsetAsync(n.theta, 0, T * 4, s);
   cudaMemsetAsync(n.m, 0, T * 4, s);
@@ -318,7 +358,7 @@ int mlp_create(Mlp &n, int hidden, int n_emb, uint64_t seed, cudaStream_t s) {
 }
 
 void mlp_destroy(Mlp &n) {
-  void *ps[] = {n.theta, n.grad, n.m, n.v, n.wh, n.loss, n.X, n.A1, n.A2, n.A3, n.D,
+  void *ps[] = {n.theta, n.grad, n.m, n.v, n.wh, n.wf, n.loss, n.X, n.A1, n.A2, n.A3, n.D,
                 n.Z1, n.Z2, n.Z3, n.C, n.y, n.dy, n.conf, n.P};
   for (void *p : ps)
     if (p) cudaFree(p);
@@ -383,10 +423,10 @@ int mlp_forward(Mlp &n, int rows, cudaStream_t s) {
   if (rows < 1) return 0;
   if (H == 128) {
     fused_forward<1><<<(rows + FR - 1) / FR, 256, FusedDims<1>::smem, s>>>(
-        n.X, n.conf, n.theta, n.wh, n.L, rows, n.y);
+        n.X, n.conf, n.theta, n.wf, n.L, rows, n.y);
   } else if (H == 256) {
     fused_forward<2><<<(rows + FR - 1) / FR, 256, FusedDims<2>::smem, s>>>(
-        n.X, n.conf, n.theta, n.wh, n.L, rows, n.y);
+        n.X, n.conf, n.theta, n.wf, n.L, rows, n.y);
   } else {
     int rc = mlp_embed(n, rows, s);
     if (rc) return rc;

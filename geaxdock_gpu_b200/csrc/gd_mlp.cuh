@@ -55,6 +55,7 @@ struct Mlp {
   MlpLayout L;
   float *theta = nullptr, *grad = nullptr, *m = nullptr, *v = nullptr; /* [L.total] */
   __nv_bfloat16 *wh = nullptr;        /* BF16 copies of W1, W2, W3 (same offsets as theta) */
+  __nv_bfloat16 *wf = nullptr;        /* W1, W2, W3 in MMA fragment order (H = 128, 256) */
   float mu = 0.0f, sigma = 1.0f;      /* target normalisation */
   int adam_t = 0;
   int cap = 0;                        /* rows of the work buffers */
@@ -79,7 +80,7 @@ int mlp_embed(Mlp &n, int rows, cudaStream_t s);
 /* forward + MSE loss against t (normalised targets) + backward into n.grad (zeroed first) */
 int mlp_loss_backward(Mlp &n, int rows, const float *t, cudaStream_t s);
 int mlp_adam(Mlp &n, float lr, cudaStream_t s);
-/* BF16 copies of the weight matrices from theta */
+/* BF16 copies of the weight matrices from theta (row-major, and in fragment order) */
 int mlp_refresh_bf16(Mlp &n, cudaStream_t s);
 
 /* ---------------- delayed acceptance (gd_da.cu) ---------------- */
@@ -129,7 +130,7 @@ struct GdDaDev {
   int *prop, *pass, *plain;
   /* the network */
   const float *theta;
-  const __nv_bfloat16 *wh;
+  const __nv_bfloat16 *wf;    /* fragment-ordered BF16 weights (Mlp::wf) */
   MlpLayout L;
   float mu, sigma;
   __nv_bfloat16 *X;           /* global feature rows (surrogate predictions of given poses) */

@@ -34,6 +34,21 @@ def test_forward_matches_oracle():
     assert _rel(y, y64) < 0.05  # what BF16 costs against the exact network
 
 
+@pytest.mark.parametrize("hidden,rows", [(128, 77), (256, 333)])
+def test_fused_forward_matches_oracle(hidden, rows):
+    """H = 128 and 256 take the one-kernel forward (register-fed m16n8k16 MMAs, in-register
+    bias + SiLU); it agrees with the oracle as the layer-by-layer path does, and its loss with
+    the layer-by-layer forward that training runs."""
+    net, orc, x, conf, t = _setup(hidden=hidden, rows=rows)
+    y = net.forward(x, conf)
+    yo = orc.forward(x, conf)
+    assert np.all(np.isfinite(y))
+    assert np.max(np.abs(y - yo)) <= 1e-2 * max(1.0, np.max(np.abs(yo))), np.max(np.abs(y - yo))
+    loss_layered, _ = net.backward(x, t, conf)
+    loss_fused = float(np.mean((y.astype(np.float64) - t) ** 2))
+    assert abs(loss_fused - loss_layered) <= 1e-3 * max(1.0, loss_layered)
+
+
 @pytest.mark.parametrize("hidden,rows", [(64, 40), (256, 333)])
 def test_gradient_matches_oracle(hidden, rows):
     net, orc, x, conf, t = _setup(hidden=hidden, rows=rows)
