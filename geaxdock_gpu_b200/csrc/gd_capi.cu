@@ -2289,6 +2289,7 @@ int gd_sur_train(gd_ctx *c, int iterations, float *losses) {
   }
   CK(cudaStreamSynchronize(c->stream));
   CK(cudaGetLastError());
+  if (gd::mlp_status(d->net)) return fail(GD_ERR_CUDA, "tensor-core GEMM wait timed out");
   if (losses && iterations)
     CK(cudaMemcpy(losses, d->d_loss_hist, sizeof(float) * iterations, cudaMemcpyDeviceToHost));
   /* the new network (and normalisation) replaces the old one in every later graph */
@@ -2539,6 +2540,7 @@ int gd_mlp_backward(gd_mlp *m, const float *x, const int *conf, const float *t, 
   if (gd::mlp_loss_backward(m->net, rows, m->d_t, m->stream))
     return fail(GD_ERR_CUDA, "backward failed");
   CK(cudaStreamSynchronize(m->stream));
+  if (gd::mlp_status(m->net)) return fail(GD_ERR_CUDA, "tensor-core GEMM wait timed out");
   if (loss) CK(cudaMemcpy(loss, m->net.loss, sizeof(float), cudaMemcpyDeviceToHost));
   if (grad)
     CK(cudaMemcpy(grad, m->net.grad, sizeof(float) * m->net.L.total, cudaMemcpyDeviceToHost));

@@ -1,23 +1,25 @@
 /*
  * gd_mlp.cu -- forward, backward and Adam kernels of the energy surrogate (gd_mlp.cuh).
  *
- * Matrix products run on the tensor cores as BF16 x BF16 -> FP32 warp-level MMA tiles
- * (16 x 16 x 16 fragments); every product the network needs is one kernel template:
- *   forward        Z = X W            (A row-major, B row-major)
- *   weight grad    dW = X^T dZ        (A read transposed from X, reduction over the batch)
- *   input grad     dX = dZ W^T        (B read transposed from W)
- * Bias, SiLU and its derivative, the 256 -> 1 output layer, the loss, column sums for the
- * bias gradients, the embedding gradient (atomic scatter) and Adam are elementwise kernels.
- * Master parameters, gradients and Adam moments are FP32; W1..W3 are mirrored in BF16 after
+ * Every matrix product of training runs on the fifth-generation tensor cores through
+ * umma_gemm (gd_umma.cu: TMA-staged BF16 operands, FP32 accumulator in tensor memory), with
+ * the elementwise step that follows it fused into its epilogue:
+ *   forward        Z = X W + b, A = bf16(SiLU(Z))         (X K-major, W MN-major)
+ *   input grad     dZ' = bf16((dZ W^T) SiLU'(Z'))         (dZ K-major, W K-major)
+ *   weight grad    dW = A^T dZ over chunks of 256 rows    (both MN-major, split-K partials)
+ * The 256 -> 1 output layer, the loss, column sums for the bias gradients, the embedding
+ * gradient (atomic scatter) and Adam are elementwise kernels. Batch reductions add per-chunk
+ * partials in a fixed order. Master parameters, gradients and Adam moments are FP32; W1..W3
+ * are mirrored in BF16 (row-major, and in MMA-fragment order for the one-kernel forward) after
  * every update.
  */
-#include <mma.h>
-
+#include <algorithm>
 #include <cmath>
 
 #include "gd_mlp.cuh"
 #include "gd_mlp_fwd.cuh"
 #include "gd_numerics.h"
+#include "gd_umma.cuh"
 
 namespace gd {
 
@@ -25,55 +27,8 @@ using bf16 = __nv_bfloat16;
 
 namespace {
 
-__device__ __forceinline__ float silu(float z) { return z / (1.0f + expf(-z)); }
-__device__ __forceinline__ float silu_grad(float z) {
-  const float s = 1.0f / (1.0f + expf(-z));
-  return s * (1.0f + z * (1.0f - s));
-}
-
-/* C[M,N] (fp32, row-major, ldc) = op(A)[M,K] op(B)[K,N]; M, N, K multiples of 16.
- * A_T: element (m, k) of A is A[k * lda + m]; otherwise A[m * lda + k].
- * B_T: element (k, n) of B is B[n * ldb + k]; otherwise B[k * ldb + n]. */
-template <bool A_T, bool B_T>
-__global__ void wmma_gemm(const bf16 *__restrict__ A, int lda, const bf16 *__restrict__ B,
-                          int ldb, float *__restrict__ C, int ldc, int M, int N, int K) {
-  using namespace nvcuda;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int tiles_n = N >> 4;
-  const int tm = warp / tiles_n, tn = warp - tm * tiles_n;
-  if (tm * 16 >= M) return;
-  wmma::fragment<wmma::accumulator, 16, 16, 16, float> acc;
-  wmma::fill_fragment(acc, 0.0f);
-  using LA = typename std::conditional<A_T, wmma::col_major, wmma::row_major>::type;
-  using LB = typename std::conditional<B_T, wmma::col_major, wmma::row_major>::type;
-  for (int k = 0; k < K; k += 16) {
-    wmma::fragment<wmma::matrix_a, 16, 16, 16, bf16, LA> a;
-    wmma::fragment<wmma::matrix_b, 16, 16, 16, bf16, LB> b;
-    wmma::load_matrix_sync(a, A_T ? A + (size_t)k * lda + tm * 16 : A + (size_t)tm * 16 * lda + k,
-                           lda);
-    wmma::load_matrix_sync(b, B_T ? B + (size_t)tn * 16 * ldb + k : B + (size_t)k * ldb + tn * 16,
-                           ldb);
-    wmma::mma_sync(acc, a, b, acc);
-  }
-  wmma::store_matrix_sync(C + (size_t)tm * 16 * ldc + tn * 16, acc, ldc, wmma::mem_row_major);
-}
-
-template <bool A_T, bool B_T>
-void gemm(const bf16 *A, int lda, const bf16 *B, int ldb, float *C, int ldc, int M, int N, int K,
-          cudaStream_t s) {
-  const int warps = (M / 16) * (N / 16);
-  wmma_gemm<A_T, B_T><<<(warps + 3) / 4, 128, 0, s>>>(A, lda, B, ldb, C, ldc, M, N, K);
-}
-
-/* Z = C + b (kept for the backward pass when Z != null), A = bf16(SiLU(Z)) */
-__global__ void bias_silu(const float *__restrict__ C, const float *__restrict__ b, float *Z,
-                          bf16 *__restrict__ A, int rows, int n) {
-  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= (size_t)rows * n) return;
-  const float z = C[i] + b[i % n];
-  if (Z) Z[i] = z;
-  A[i] = __float2bfloat16_rn(silu(z));
-}
+__device__ __forceinline__ float silu(float z) { return mlp_silu(z); }
+__device__ __forceinline__ float silu_grad(float z) { return mlp_silu_grad(z); }
 
 /* y[r] = A3[r] . w4 + b4, one warp per row */
 __global__ void out_layer(const bf16 *__restrict__ A3, const float *__restrict__ w4,
@@ -120,14 +75,6 @@ __global__ void out_backward(const float *__restrict__ dy, const float *__restri
   D[i] = __float2bfloat16_rn(dy[r] * w4[j] * silu_grad(Z3[i]));
 }
 
-/* dZ = dX * SiLU'(Z) -> bf16 */
-__global__ void act_backward(const float *__restrict__ dX, const float *__restrict__ Z,
-                             bf16 *__restrict__ D, size_t n) {
-  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  D[i] = __float2bfloat16_rn(dX[i] * silu_grad(Z[i]));
-}
-
 /* Reductions over the batch are split into chunks of SPLIT_ROWS rows: each chunk writes a
  * partial result, reduce_partials adds the chunks in a fixed order (deterministic). */
 constexpr int SPLIT_ROWS = 256;
@@ -167,31 +114,6 @@ __global__ void reduce_partials(const float *__restrict__ part, int chunks, size
   float s = 0.0f;
   for (int c = 0; c < chunks; ++c) s += part[(size_t)c * count + i];
   out[i] += s;
-}
-
-/* part[chunk] = A[chunk rows]^T D[chunk rows]: A [rows][K] row-major, D [rows][N] row-major,
- * one warp per 16 x 16 tile of the [K][N] result and chunk of SPLIT_ROWS rows */
-__global__ void wmma_tn_split(const bf16 *__restrict__ A, int K, const bf16 *__restrict__ D, int N,
-                              int rows, float *__restrict__ part) {
-  using namespace nvcuda;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int tiles_n = N >> 4, tiles = (K >> 4) * tiles_n;
-  const int chunk = warp / tiles, t = warp - chunk * tiles;
-  const int r0 = chunk * SPLIT_ROWS;
-  if (r0 >= rows) return;
-  const int r1 = min(rows, r0 + SPLIT_ROWS);
-  const int tm = t / tiles_n, tn = t - tm * tiles_n;
-  wmma::fragment<wmma::accumulator, 16, 16, 16, float> acc;
-  wmma::fill_fragment(acc, 0.0f);
-  for (int k = r0; k < r1; k += 16) {
-    wmma::fragment<wmma::matrix_a, 16, 16, 16, bf16, wmma::col_major> a;
-    wmma::fragment<wmma::matrix_b, 16, 16, 16, bf16, wmma::row_major> b;
-    wmma::load_matrix_sync(a, A + (size_t)k * K + tm * 16, K);
-    wmma::load_matrix_sync(b, D + (size_t)k * N + tn * 16, N);
-    wmma::mma_sync(acc, a, b, acc);
-  }
-  wmma::store_matrix_sync(part + (size_t)chunk * K * N + (size_t)tm * 16 * N + tn * 16, acc, N,
-                          wmma::mem_row_major);
 }
 
 /* embedding gradient: columns [7, 39) of dX1 scattered to the rows' conformer entries */
@@ -325,12 +247,14 @@ int mlp_refresh_bf16(Mlp &n, cudaStream_t s) {
 }
 
 int mlp_create(Mlp &n, int hidden, int n_emb, uint64_t seed, cudaStream_t s) {
-  if (hidden % 16 || hidden < 16) return -1;
+  if (hidden % 16 || hidden < 16 || hidden > 256) return -1;
   n.L.set(hidden, n_emb);
   const size_t T = n.L.total;
   if (cudaMalloc(&n.theta, T * 4) || cudaMalloc(&n.grad, T * 4) || cudaMalloc(&n.m, T * 4) ||
-      cudaMalloc(&n.v, T * 4) || cudaMalloc(&n.wh, n.L.b4 * 2) || cudaMalloc(&n.loss, 16))
+      cudaMalloc(&n.v, T * 4) || cudaMalloc(&n.wh, n.L.b4 * 2) || cudaMalloc(&n.loss, 16) ||
+      cudaMalloc(&n.err, sizeof(int)))
     return -3;
+  cudaMemsetAsync(n.err, 0, sizeof(int), s);
   if ((hidden == 128 || hidden == 256) &&
       cudaMalloc(&n.wf, ((size_t)GD_MLP_IN * hidden + 2 * (size_t)hidden * hidden) * 2))
     return -3;
@@ -358,7 +282,7 @@ int mlp_create(Mlp &n, int hidden, int n_emb, uint64_t seed, cudaStream_t s) {
 }
 
 void mlp_destroy(Mlp &n) {
-  void *ps[] = {n.theta, n.grad, n.m, n.v, n.wh, n.wf, n.loss, n.X, n.A1, n.A2, n.A3, n.D,
+  void *ps[] = {n.theta, n.grad, n.m, n.v, n.wh, n.wf, n.loss, n.err, n.X, n.A1, n.A2, n.A3, n.D, n.D2, n.Pb,
                 n.Z1, n.Z2, n.Z3, n.C, n.y, n.dy, n.conf, n.P};
   for (void *p : ps)
     if (p) cudaFree(p);
@@ -368,16 +292,17 @@ void mlp_destroy(Mlp &n) {
 int mlp_reserve(Mlp &n, int rows) {
   rows = (rows + 15) & ~15;
   if (rows <= n.cap) return 0;
-  void *ps[] = {n.X, n.A1, n.A2, n.A3, n.D, n.Z1, n.Z2, n.Z3, n.C, n.y, n.dy, n.conf};
+  void *ps[] = {n.X, n.A1, n.A2, n.A3, n.D, n.D2, n.Z1, n.Z2, n.Z3, n.C, n.y, n.dy, n.conf, n.Pb};
   for (void *p : ps)
     if (p) cudaFree(p);
   const size_t H = n.L.hidden, R = rows;
   if (cudaMalloc(&n.X, R * GD_MLP_IN * 2) || cudaMalloc(&n.A1, R * H * 2) ||
       cudaMalloc(&n.A2, R * H * 2) || cudaMalloc(&n.A3, R * H * 2) ||
-      cudaMalloc(&n.D, R * H * 2) || cudaMalloc(&n.Z1, R * H * 4) ||
+      cudaMalloc(&n.D, R * H * 2) || cudaMalloc(&n.D2, R * H * 2) || cudaMalloc(&n.Z1, R * H * 4) ||
       cudaMalloc(&n.Z2, R * H * 4) || cudaMalloc(&n.Z3, R * H * 4) ||
       cudaMalloc(&n.C, R * (H > GD_MLP_IN ? H : GD_MLP_IN) * 4) || cudaMalloc(&n.y, R * 4) ||
-      cudaMalloc(&n.dy, R * 4) || cudaMalloc(&n.conf, R * 4))
+      cudaMalloc(&n.dy, R * 4) || cudaMalloc(&n.conf, R * 4) ||
+      cudaMalloc(&n.Pb, ((R + 127) / 128) * H * 4))
     return -3;
   cudaMemset(n.X, 0, R * GD_MLP_IN * 2);
   cudaMemset(n.conf, 0xff, R * 4);
@@ -402,16 +327,22 @@ int mlp_embed(Mlp &n, int rows, cudaStream_t s) {
 static int forward_impl(Mlp &n, int rows, bool keep, cudaStream_t s) {
   const int M = (rows + 15) & ~15, H = n.L.hidden;
   if (M > n.cap) return -4;
-  const bf16 *W1 = n.wh + n.L.w1, *W2 = n.wh + n.L.w2, *W3 = n.wh + n.L.w3;
-  gemm<false, false>(n.X, GD_MLP_IN, W1, H, n.C, H, M, H, GD_MLP_IN, s);
-  bias_silu<<<blocks((size_t)M * H), 256, 0, s>>>(n.C, n.theta + n.L.b1, keep ? n.Z1 : nullptr,
-                                                  n.A1, M, H);
-  gemm<false, false>(n.A1, H, W2, H, n.C, H, M, H, H, s);
-  bias_silu<<<blocks((size_t)M * H), 256, 0, s>>>(n.C, n.theta + n.L.b2, keep ? n.Z2 : nullptr,
-                                                  n.A2, M, H);
-  gemm<false, false>(n.A2, H, W3, H, n.C, H, M, H, H, s);
-  bias_silu<<<blocks((size_t)M * H), 256, 0, s>>>(n.C, n.theta + n.L.b3, keep ? n.Z3 : nullptr,
-                                                  n.A3, M, H);
+  /* Z_l = A_{l-1} W_l + b_l, A_l = bf16(SiLU(Z_l)) in one tensor-core kernel per layer */
+  auto layer = [&](const bf16 *Ain, int K, size_t w, size_t b, float *Z, bf16 *Aout) {
+    const UmmaOperand a{Ain, M, K, 0}, wt{n.wh + w, K, H, 1};
+    UmmaEpilogue e{};
+    e.kind = UMMA_FWD;
+    e.bias = n.theta + b;
+    e.Z = keep ? Z : nullptr;
+    e.Ob = Aout;
+    e.ldo = H;
+    return umma_gemm(a, wt, M, H, K, 1, e, n.err, s);
+  };
+  int rc;
+  if ((rc = layer(n.X, GD_MLP_IN, n.L.w1, n.L.b1, n.Z1, n.A1)) ||
+      (rc = layer(n.A1, H, n.L.w2, n.L.b2, n.Z2, n.A2)) ||
+      (rc = layer(n.A2, H, n.L.w3, n.L.b3, n.Z3, n.A3)))
+    return rc;
   out_layer<<<blocks((size_t)rows * 32), 256, 0, s>>>(n.A3, n.theta + n.L.w4, n.theta + n.L.b4,
                                                       n.y, rows, H);
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
@@ -459,33 +390,79 @@ int mlp_loss_backward(Mlp &n, int rows, const float *t, cudaStream_t s) {
     colsum_split<<<dim3((ncol + 31) / 32, S), 256, 0, s>>>(A, w, M, H, n.P);
     reduce_partials<<<blocks(ncol), 256, 0, s>>>(n.P, S, (size_t)ncol, g);
   };
-  auto weight_grad = [&](const bf16 *A, int K, float *g) {
-    const int warps = S * (K / 16) * (H / 16);
-    wmma_tn_split<<<(warps + 7) / 8, 256, 0, s>>>(A, K, n.D, H, M, n.P);
+  /* dW[i][j] = sum_r Aprev[r][i] dZ[r][j] in chunks of SPLIT_ROWS rows (both operands
+   * MN-major, the rows are the reduction); W1 (64 rows) is computed as dW1^T = dZ1^T X so that
+   * the 128-row MMA tile runs along the hidden dimension, and stored transposed */
+  auto weight_grad = [&](const bf16 *Aprev, int K, const bf16 *D, float *g) {
+    UmmaEpilogue e{};
+    e.kind = UMMA_F32;
+    e.Of = n.P;
+    e.ldo = H;
+    e.split_stride = (size_t)K * H;
+    int rc;
+    if (K == H) {
+      rc = umma_gemm(UmmaOperand{Aprev, M, K, 1}, UmmaOperand{D, M, H, 1}, K, H, SPLIT_ROWS, S,
+                     e, n.err, s);
+    } else {
+      e.trans = 1;
+      rc = umma_gemm(UmmaOperand{D, M, H, 1}, UmmaOperand{Aprev, M, K, 1}, H, K, SPLIT_ROWS, S,
+                     e, n.err, s);
+    }
+    if (rc) return rc;
     reduce_partials<<<blocks((size_t)K * H), 256, 0, s>>>(n.P, S, (size_t)K * H, g);
+    return 0;
   };
+  /* dZ_{l-1} = bf16((dZ_l W_l^T) SiLU'(Z_{l-1})), and its column sums (db_{l-1}) per 128-row
+   * tile, added in tile order */
+  auto input_grad = [&](const bf16 *D, size_t w, const float *Zprev, bf16 *Dout, float *gb) {
+    UmmaEpilogue e{};
+    e.kind = UMMA_DGRAD;
+    e.Zin = Zprev;
+    e.Ob = Dout;
+    e.colsum = n.Pb;
+    e.ldo = H;
+    const int rc = umma_gemm(UmmaOperand{D, M, H, 0}, UmmaOperand{n.wh + w, H, H, 0}, M, H, H, 1,
+                             e, n.err, s);
+    if (rc) return rc;
+    reduce_partials<<<blocks(H), 256, 0, s>>>(n.Pb, (M + 127) / 128, (size_t)H, gb);
+    return 0;
+  };
+  bf16 *Dc = n.D, *Dn = n.D2;
   /* output layer: dw4 = A3^T dy and db4 = sum dy (b4 follows w4 in theta) */
   colsum(n.A3, n.dy, n.grad + n.L.w4);
-  out_backward<<<blocks((size_t)M * H), 256, 0, s>>>(n.dy, n.theta + n.L.w4, n.Z3, n.D, M, H);
-  /* layer 3: dW3 = A2^T dZ3, db3, dA2 = dZ3 W3^T */
-  weight_grad(n.A2, H, n.grad + n.L.w3);
-  colsum(n.D, nullptr, n.grad + n.L.b3);
-  gemm<false, true>(n.D, H, n.wh + n.L.w3, H, n.C, H, M, H, H, s);
-  act_backward<<<blocks((size_t)M * H), 256, 0, s>>>(n.C, n.Z2, n.D, (size_t)M * H);
-  /* layer 2 */
-  weight_grad(n.A1, H, n.grad + n.L.w2);
-  colsum(n.D, nullptr, n.grad + n.L.b2);
-  gemm<false, true>(n.D, H, n.wh + n.L.w2, H, n.C, H, M, H, H, s);
-  act_backward<<<blocks((size_t)M * H), 256, 0, s>>>(n.C, n.Z1, n.D, (size_t)M * H);
-  /* layer 1: dW1 = X^T dZ1 (64 x H), db1; dX1 = dZ1 W1^T for the embedding */
-  weight_grad(n.X, GD_MLP_IN, n.grad + n.L.w1);
-  colsum(n.D, nullptr, n.grad + n.L.b1);
+  out_backward<<<blocks((size_t)M * H), 256, 0, s>>>(n.dy, n.theta + n.L.w4, n.Z3, Dc, M, H);
+  /* layer 3: dW3 = A2^T dZ3, db3, dZ2 */
+  if ((rc = weight_grad(n.A2, H, Dc, n.grad + n.L.w3))) return rc;
+  colsum(Dc, nullptr, n.grad + n.L.b3);
+  if ((rc = input_grad(Dc, n.L.w3, n.Z2, Dn, n.grad + n.L.b2))) return rc;
+  std::swap(Dc, Dn);
+  /* layer 2 (db2 came with dZ2) */
+  if ((rc = weight_grad(n.A1, H, Dc, n.grad + n.L.w2))) return rc;
+  if ((rc = input_grad(Dc, n.L.w2, n.Z1, Dn, n.grad + n.L.b1))) return rc;
+  std::swap(Dc, Dn);
+  /* layer 1: dW1 = X^T dZ1 (64 x H) (db1 came with dZ1); dX = dZ1 W1^T (FP32) for the
+   * embedding */
+  if ((rc = weight_grad(n.X, GD_MLP_IN, Dc, n.grad + n.L.w1))) return rc;
   if (n.L.n_emb) {
-    gemm<false, true>(n.D, H, n.wh + n.L.w1, H, n.C, GD_MLP_IN, M, GD_MLP_IN, H, s);
+    UmmaEpilogue e{};
+    e.kind = UMMA_F32;
+    e.Of = n.C;
+    e.ldo = GD_MLP_IN;
+    if ((rc = umma_gemm(UmmaOperand{Dc, M, H, 0}, UmmaOperand{n.wh + n.L.w1, GD_MLP_IN, H, 0}, M,
+                        GD_MLP_IN, H, 1, e, n.err, s)))
+      return rc;
     emb_grad<<<blocks((size_t)rows * GD_MLP_EMB), 256, 0, s>>>(n.C, n.conf, rows,
                                                              n.grad + n.L.emb);
   }
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+int mlp_status(Mlp &n) {
+  int e = 0;
+  if (cudaMemcpy(&e, n.err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return -2;
+  if (!e) return 0;
+  cudaMemset(n.err, 0, sizeof(int));
+  return -6;
 }
 
 int mlp_adam(Mlp &n, float lr, cudaStream_t s) {

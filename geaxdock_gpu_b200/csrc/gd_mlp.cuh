@@ -30,6 +30,13 @@
 
 namespace gd {
 
+/* the activation and its derivative, written once for every kernel that applies them */
+__device__ __forceinline__ float mlp_silu(float z) { return z / (1.0f + expf(-z)); }
+__device__ __forceinline__ float mlp_silu_grad(float z) {
+  const float s = 1.0f / (1.0f + expf(-z));
+  return s * (1.0f + z * (1.0f - s));
+}
+
 struct MlpLayout {
   int hidden = 256, n_emb = 0;
   size_t w1, b1, w2, b2, w3, b3, w4, b4, emb, total;
@@ -60,10 +67,13 @@ struct Mlp {
   int adam_t = 0;
   int cap = 0;                        /* rows of the work buffers */
   __nv_bfloat16 *X = nullptr, *A1 = nullptr, *A2 = nullptr, *A3 = nullptr, *D = nullptr;
+  __nv_bfloat16 *D2 = nullptr;        /* second buffer of the back-propagated dZ (ping-pong) */
+  int *err = nullptr;                 /* [1] nonzero when a tensor-core GEMM's wait ran out */
   float *Z1 = nullptr, *Z2 = nullptr, *Z3 = nullptr, *C = nullptr, *y = nullptr, *dy = nullptr;
   float *loss = nullptr;              /* [1] */
   int *conf = nullptr;                /* [cap] embedding row per input row */
   float *P = nullptr;                 /* per-chunk partials of the batch reductions */
+  float *Pb = nullptr;                /* [cap / 128][hidden] per-tile bias-gradient partials */
   size_t p_cap = 0;
 };
 
@@ -82,6 +92,8 @@ int mlp_loss_backward(Mlp &n, int rows, const float *t, cudaStream_t s);
 int mlp_adam(Mlp &n, float lr, cudaStream_t s);
 /* BF16 copies of the weight matrices from theta (row-major, and in fragment order) */
 int mlp_refresh_bf16(Mlp &n, cudaStream_t s);
+/* after a synchronisation: 0, or -6 (and the flag cleared) if a GEMM's bounded wait ran out */
+int mlp_status(Mlp &n);
 
 /* ---------------- delayed acceptance (gd_da.cu) ---------------- */
 

@@ -33,7 +33,7 @@ using bf16 = __nv_bfloat16;
 
 constexpr int FR = 32; /* rows per CTA: short per-CTA chains, many CTAs */
 
-__device__ __forceinline__ float silu(float z) { return z / (1.0f + expf(-z)); }
+__device__ __forceinline__ float silu(float z) { return mlp_silu(z); }
 
 template <int NT> /* H = 128 * NT; a warp owns 2 NT 8-column MMA tiles */
 struct Dims {
