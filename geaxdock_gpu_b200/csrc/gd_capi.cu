@@ -18,6 +18,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "gd_device.cuh"
@@ -164,6 +165,34 @@ struct gd_ctx {
 };
 
 namespace {
+
+/* Device -> host copy of n rows (width bytes each; device pitch dpitch, host pitch hpitch). A
+ * large download into freshly allocated pageable memory is bound by the first touch of every
+ * host page (one thread faults pages in at about a quarter of the copy rate of resident pages),
+ * so above 32 MB the destination rows are first written by up to 8 host threads in parallel,
+ * then copied in one call. */
+cudaError_t d2h_rows(void *dst, size_t hpitch, const void *src, size_t dpitch, size_t width,
+                     int n) {
+  if (n < 1 || width == 0) return cudaSuccess;
+  int T = (int)std::min(8u, std::max(1u, std::thread::hardware_concurrency()));
+  if (width * (size_t)n < ((size_t)32 << 20)) T = 1;
+  T = std::min(T, n);
+  if (T > 1) {
+    auto touch = [&](int t) {
+      const int a = (int)((long long)n * t / T), b = (int)((long long)n * (t + 1) / T);
+      char *d = static_cast<char *>(dst) + (size_t)a * hpitch;
+      if (hpitch == width)
+        memset(d, 0, (size_t)(b - a) * width);
+      else
+        for (int i = a; i < b; ++i, d += hpitch) memset(d, 0, width);
+    };
+    std::vector<std::thread> th;
+    for (int t = 1; t < T; ++t) th.emplace_back(touch, t);
+    touch(0);
+    for (auto &x : th) x.join();
+  }
+  return cudaMemcpy2D(dst, hpitch, src, dpitch, width, n, cudaMemcpyDeviceToHost);
+}
 
 template <class T>
 int dalloc(gd_ctx *c, T **p, size_t n) {
@@ -1315,12 +1344,9 @@ int gd_get_records_raw(gd_ctx *c, gd_record_step *steps, int *next_ptr, int r0, 
   const int n = r1 - r0 + 1;
   CK(cudaStreamSynchronize(c->stream));
   const size_t rs = sizeof(gd_record_step);
-  if (cap == c->rec_cap)
-    CK(cudaMemcpy(steps, c->d_rec + (size_t)r0 * cap, rs * (size_t)n * cap,
-                  cudaMemcpyDeviceToHost));
-  else /* the first cap records of each replica only */
-    CK(cudaMemcpy2D(steps, rs * cap, c->d_rec + (size_t)r0 * c->rec_cap, rs * c->rec_cap,
-                    rs * cap, n, cudaMemcpyDeviceToHost));
+  /* the first cap records of each replica */
+  CK(d2h_rows(steps, rs * cap, c->d_rec + (size_t)r0 * c->rec_cap, rs * c->rec_cap,
+              rs * cap, n));
   CK(cudaMemcpy(next_ptr, c->d_rec_next + r0, sizeof(int) * n, cudaMemcpyDeviceToHost));
   return GD_OK;
 }
@@ -1347,11 +1373,9 @@ int gd_get_records(gd_ctx *c, gd_lig_record *host, int r0, int r1) {
   const int n = r1 - r0 + 1;
   std::vector<int> nxt(n);
   CK(cudaMemcpy(nxt.data(), c->d_rec_next + r0, sizeof(int) * n, cudaMemcpyDeviceToHost));
-  for (int i = 0; i < n; ++i) {
-    CK(cudaMemcpy(host[i].step, c->d_rec + (size_t)(r0 + i) * c->rec_cap,
-                  sizeof(gd_record_step) * c->rec_cap, cudaMemcpyDeviceToHost));
-    host[i].next_ptr = nxt[i];
-  }
+  CK(d2h_rows(host[0].step, sizeof(gd_lig_record), c->d_rec + (size_t)r0 * c->rec_cap,
+              sizeof(gd_record_step) * c->rec_cap, sizeof(gd_record_step) * c->rec_cap, n));
+  for (int i = 0; i < n; ++i) host[i].next_ptr = nxt[i];
   return GD_OK;
 }
 
