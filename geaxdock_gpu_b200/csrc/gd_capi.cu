@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "gd_device.cuh"
+#include "gd_kmeans.cuh"
 #include "gd_mlp.cuh"
 #include "gd_numerics.h"
 
@@ -2576,6 +2577,42 @@ int gd_mlp_adam(gd_mlp *m, float lr) {
   CK(cudaSetDevice(m->device));
   if (gd::mlp_adam(m->net, lr, m->stream)) return fail(GD_ERR_CUDA, "Adam step failed");
   CK(cudaStreamSynchronize(m->stream));
+  return GD_OK;
+}
+
+int gd_kmeans(int device, const float *objects, int n, int dim, const int *seg_off, int n_seg,
+              const int *k, uint64_t seed, float threshold, int max_iter, int *membership,
+              int *medoid, int *size, int *passes) {
+  if (!objects || !seg_off || !k || n < 0 || n_seg < 1 || max_iter < 0)
+    return fail(GD_ERR_INVALID, "gd_kmeans: bad arguments");
+  if (dim != GD_MAXWEI - 1) return fail(GD_ERR_INVALID, "gd_kmeans: dim must be %d", GD_MAXWEI - 1);
+  if (seg_off[0] != 0 || seg_off[n_seg] != n)
+    return fail(GD_ERR_INVALID, "gd_kmeans: segment offsets must run from 0 to n");
+  for (int s = 0; s < n_seg; ++s)
+    if (seg_off[s + 1] < seg_off[s] || k[s] < 1)
+      return fail(GD_ERR_INVALID, "gd_kmeans: segment %d: offsets decrease or k < 1", s);
+  CK(cudaSetDevice(device));
+  gd::KmeansJob job;
+  job.objects = objects;
+  job.dim = dim;
+  job.seg_off.assign(seg_off, seg_off + n_seg + 1);
+  job.k.assign(k, k + n_seg);
+  job.seed = seed;
+  job.threshold = threshold;
+  job.max_iter = max_iter;
+  gd::KmeansResult res;
+  std::string err;
+  if (gd::kmeans_device(job, res, err)) return fail(GD_ERR_CUDA, "gd_kmeans: %s", err.c_str());
+  if (membership) std::copy(res.membership.begin(), res.membership.end(), membership);
+  if (medoid) std::copy(res.medoid.begin(), res.medoid.end(), medoid);
+  if (size) std::copy(res.size.begin(), res.size.end(), size);
+  if (passes) std::copy(res.passes.begin(), res.passes.end(), passes);
+  return GD_OK;
+}
+
+int gd_kmeans_permutation(uint64_t seed, int segment, int n, int *perm) {
+  if (!perm || n < 0 || segment < 0) return fail(GD_ERR_INVALID, "gd_kmeans_permutation: bad arguments");
+  gd::kmeans_permutation(seed, segment, n, perm);
   return GD_OK;
 }
 

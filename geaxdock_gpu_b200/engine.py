@@ -93,6 +93,9 @@ def lib() -> C.CDLL:
         "gd_mlp_forward": [vp, fp, ip, C.c_int, fp],
         "gd_mlp_backward": [vp, fp, ip, fp, C.c_int, fp, fp],
         "gd_mlp_adam": [vp, C.c_float],
+        "gd_kmeans": [C.c_int, fp, C.c_int, C.c_int, ip, C.c_int, ip, C.c_uint64, C.c_float,
+                      C.c_int, ip, ip, ip, ip],
+        "gd_kmeans_permutation": [C.c_uint64, C.c_int, C.c_int, ip],
     }
     for name, args in sig.items():
         fn = getattr(L, name)

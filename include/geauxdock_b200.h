@@ -385,6 +385,30 @@ const char *gd_version(void);
  * the roofline denominator for the FP32-bound pair-energy kernel. No reference counterpart. */
 int gd_probe_fp32_peak(int device, int repeats, double *tflops);
 
+/* ---------------------------------------------------------------------------------------
+ * Post-Monte-Carlo clustering (post_mc, src/post_mc.C:40-101): k-means over the 9 energy
+ * terms of the records, clusterByKmeans (src/util.C:1801-1880) over seq_kmeans
+ * (src/seq_kmeans.c), for n_seg independent segments at once on the device.
+ * Segment s is objects[seg_off[s] .. seg_off[s+1]-1] (each `dim` = 9 floats) with k[s]
+ * clusters; a segment with fewer objects than k[s] is not clustered (each object is its own
+ * cluster, in order, as the reference returns them). Each segment is shuffled by the seeded
+ * permutation of gd_kmeans_permutation (the reference shuffles without a seed), its first k
+ * shuffled objects seed the centres, Lloyd passes run while more than `threshold` of its
+ * objects change cluster and at most max_iter + 1 passes, and the representative of each
+ * cluster is its last member in shuffled order. Clusters are numbered per segment from
+ * cluster base = sum over earlier segments of min(k, n):
+ *   membership[n]   cluster of each object within its segment (original object order)
+ *   medoid[total]   object index of each cluster's representative, -1 if it ended empty
+ *   size[total]     members of each cluster
+ *   passes[n_seg]   Lloyd passes per segment (the reference's loop_iterations)
+ * Any output may be NULL. */
+int gd_kmeans(int device, const float *objects, int n, int dim, const int *seg_off, int n_seg,
+              const int *k, uint64_t seed, float threshold, int max_iter, int *membership,
+              int *medoid, int *size, int *passes);
+/* The shuffle of segment `segment` of n objects: perm[i] = the object at shuffled position i
+ * (a 4-round Feistel permutation with cycle walking, keys from seed and segment). */
+int gd_kmeans_permutation(uint64_t seed, int segment, int n, int *perm);
+
 #ifdef __cplusplus
 }
 #endif
