@@ -454,6 +454,35 @@ def screen_da(dev, move_mult=1.0, burn=100, steps=100, iters=1665):
             "steps": steps}
 
 
+def post_mc_measure(eng, cx, args):
+    """post_mc clustering (per-replica k = 50, pooled k = 500) of the timed run's records on
+    the GPU, host wall clock including the upload; beside it the CPU restatement of the
+    reference's k-means (oracle/kmeans.py) on the first stage of a few replicas."""
+    from geaxdock_gpu_b200 import postmc
+    steps, nxt = eng.records()
+    recs = [steps[i, :nxt[i]] for i in range(cx.n_rep)]
+    n_rec = int(nxt.sum())
+    postmc.post_mc(recs[:8], seed=1)  # warm-up (module load, allocations)
+    t0 = time.perf_counter()
+    med, size = postmc.post_mc(recs, seed=1)
+    gpu_s = time.perf_counter() - t0
+    out = {"records": n_rec, "replicas": cx.n_rep, "representatives": int(med.shape[0]),
+           "gpu_s": gpu_s, "records_per_s": n_rec / gpu_s,
+           "scope": "postmc.post_mc: upload, batched k-means (50 per replica), pooled k-means "
+                    "(500), host wall clock"}
+    if not args.no_cpu:
+        from oracle import kmeans as ok
+        n_s = 4
+        t0 = time.perf_counter()
+        for i in range(n_s):
+            ok.cluster_by_kmeans(recs[i]["energy"]["e"][:, :9], 50, 1, i)
+        cpu_s = time.perf_counter() - t0
+        out["cpu_sample"] = {"s": cpu_s, "sample": "first-stage k-means of %d replicas with the "
+                             "oracle's numpy restatement of seq_kmeans, one core" % n_s,
+                             "first_stage_estimate_s": cpu_s * cx.n_rep / n_s}
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     from geaxdock_gpu_b200 import abi, engine
@@ -527,6 +556,9 @@ def run_ours(args, rank, world, local_rank):
     rs_per_step = cx.n_rep * spe
     value = world * rs_per_step * args.steps / (tot_ms * 1e-3)
     flops_rs = algorithmic_flops_per_replica_step(eng, w) if rank == 0 else 0.0
+    post = None
+    if world == 1 and not args.no_postmc:
+        post = post_mc_measure(eng, cx, args)
     eng.close()
     del flush
 
@@ -620,7 +652,7 @@ def run_ours(args, rank, world, local_rank):
                       "parallelism": "replica shards, no collective" if world > 1 else "1 GPU"},
            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
            "gpu_launches": 2 * args.steps + args.steps // max(1, intervals_per_dump),
-           "delayed_acceptance": da, "batched_screen": screen}
+           "delayed_acceptance": da, "batched_screen": screen, "post_mc": post}
     print(json.dumps(out), flush=True)
 
 
@@ -654,6 +686,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-da", action="store_true", help="skip the delayed-acceptance runs")
     ap.add_argument("--no-screen", action="store_true", help="skip the config-2 batched screen")
+    ap.add_argument("--no-postmc", action="store_true",
+                    help="skip the post_mc clustering of the timed run's records")
     ap.add_argument("--tile", default="", help="replicas_per_cta,chunk_points[,unroll] (default: tuned)")
     ap.add_argument("--profile-da", action="store_true",
                     help="only a short delayed-acceptance sequence on the config-1 system (20 "

@@ -19,12 +19,16 @@
  * Every float operation is the reference's, in its order: the distance sums the squared
  * coordinate differences dimension by dimension (no fused multiply-add); a centre sums its
  * members' coordinates in shuffled order and divides by the member count. One thread per
- * object assigns; one thread per cluster walks its segment in order to sum members.
+ * object assigns. For small segments one thread per cluster walks its segment in order to sum
+ * its members; for large ones (the pooled second stage) a stable radix sort of the objects by
+ * cluster (CUB) lists each cluster's members in order and one thread per (cluster,
+ * coordinate) sums them.
  * A segment stops iterating on its own criterion; the host polls one counter per pass.
  */
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cub/device/device_radix_sort.cuh>
 #include <vector>
 
 #include "gd_kmeans.cuh"
@@ -160,6 +164,44 @@ __global__ void update_kernel(const float *__restrict__ sh, const Seg *__restric
   }
 }
 
+__global__ void cluster_key_kernel(const Seg *__restrict__ seg, const int *__restrict__ seg_of,
+                                   const int *__restrict__ mem, int n_obj, int *__restrict__ key,
+                                   int *__restrict__ pos) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n_obj) return;
+  const int m = mem[p];
+  key[p] = m >= 0 ? seg[seg_of[p]].cbase + m : 0x7fffffff;
+  pos[p] = p;
+}
+
+/* first / one-past-last index of each cluster in the sorted key array */
+__global__ void bounds_kernel(const int *__restrict__ key, int n_obj, int n_cl,
+                              int *__restrict__ begin, int *__restrict__ end) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_obj) return;
+  const int k = key[i];
+  if (k >= n_cl) return;
+  if (i == 0 || key[i - 1] != k) begin[k] = i;
+  if (i == n_obj - 1 || key[i + 1] != k) end[k] = i + 1;
+}
+
+/* centre = in-order sum of its members / count, one thread per (cluster, coordinate) */
+__global__ void update_sorted_kernel(const float *__restrict__ sh, int dim,
+                                     const int *__restrict__ cseg,
+                                     const unsigned char *__restrict__ act, int n_cl,
+                                     const int *__restrict__ begin, const int *__restrict__ end,
+                                     const int *__restrict__ pos, float *__restrict__ cen) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n_cl * dim) return;
+  const int c = t / dim, j = t - c * dim;
+  if (!act[cseg[c]]) return;
+  const int b = begin[c], e = end[c];
+  if (e <= b) return;
+  float s = 0.0f;
+  for (int i = b; i < e; ++i) s = __fadd_rn(s, sh[(size_t)pos[i] * dim + j]);
+  cen[(size_t)c * dim + j] = __fdiv_rn(s, (float)(e - b));
+}
+
 /* per segment: delta = changed / n (float); keep iterating while delta > threshold and the
  * pass counter (post-incremented, as `loop++ < 500`) is below max_iter */
 __global__ void step_kernel(const Seg *__restrict__ seg, int n_seg, int *__restrict__ changed,
@@ -269,6 +311,24 @@ int kmeans_device(const KmeansJob &job, KmeansResult &res, std::string &err) {
   ok(dmalloc(&n_act, 1));
   ok(dmalloc(&medoid, n_cl));
   ok(dmalloc(&size, n_cl));
+  int max_n = 0;
+  for (const Seg &g : seg) max_n = g.n > max_n ? g.n : max_n;
+  const bool sorted = max_n > 8192;
+  int *key = nullptr, *key2 = nullptr, *pos = nullptr, *pos2 = nullptr, *cb = nullptr,
+      *ce = nullptr;
+  void *tmp = nullptr;
+  size_t tmp_bytes = 0;
+  if (sorted) {
+    ok(dmalloc(&key, n_obj));
+    ok(dmalloc(&key2, n_obj));
+    ok(dmalloc(&pos, n_obj));
+    ok(dmalloc(&pos2, n_obj));
+    ok(dmalloc(&cb, n_cl));
+    ok(dmalloc(&ce, n_cl));
+    ok(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, key, key2, pos, pos2, n_obj, 0, 31,
+                                       st));
+    ok(cudaMalloc(&tmp, tmp_bytes ? tmp_bytes : 1));
+  }
   if (e == cudaSuccess) {
     std::vector<unsigned char> a0(n_seg);
     for (int s = 0; s < n_seg; ++s) a0[s] = seg[s].k > 0 && job.k[s] <= seg[s].n;
@@ -287,7 +347,19 @@ int kmeans_device(const KmeansJob &job, KmeansResult &res, std::string &err) {
     ok(cudaGetLastError());
     for (int pass = 0; e == cudaSuccess; ++pass) {
       assign_kernel<9><<<bo, T, 0, st>>>(sh, dseg, dseg_of, act, n_obj, cen, mem, changed);
-      update_kernel<9><<<bc, T, 0, st>>>(sh, dseg, dcseg, act, n_cl, mem, cen);
+      if (sorted) {
+        /* stable by key: each cluster's members in shuffled order */
+        cluster_key_kernel<<<bo, T, 0, st>>>(dseg, dseg_of, mem, n_obj, key, pos);
+        ok(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, key, key2, pos, pos2, n_obj, 0, 31,
+                                           st));
+        ok(cudaMemsetAsync(cb, 0, sizeof(int) * n_cl, st));
+        ok(cudaMemsetAsync(ce, 0, sizeof(int) * n_cl, st));
+        bounds_kernel<<<bo, T, 0, st>>>(key2, n_obj, n_cl, cb, ce);
+        update_sorted_kernel<<<(n_cl * D + T - 1) / T, T, 0, st>>>(sh, D, dcseg, act, n_cl, cb,
+                                                                     ce, pos2, cen);
+      } else {
+        update_kernel<9><<<bc, T, 0, st>>>(sh, dseg, dcseg, act, n_cl, mem, cen);
+      }
       ok(cudaMemsetAsync(n_act, 0, sizeof(int), st));
       step_kernel<<<bs, T, 0, st>>>(dseg, n_seg, changed, loops, act, job.threshold,
                                     job.max_iter, n_act);
@@ -308,7 +380,7 @@ int kmeans_device(const KmeansJob &job, KmeansResult &res, std::string &err) {
     ok(cudaStreamSynchronize(st));
   }
   void *ps[] = {obj, sh, cen, dseg, dseg_of, dcseg, perm, mem, orig, changed, loops, act, n_act,
-                medoid, size};
+                medoid, size, key, key2, pos, pos2, cb, ce, tmp};
   for (void *p : ps)
     if (p) cudaFree(p);
   if (e != cudaSuccess) {

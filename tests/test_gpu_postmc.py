@@ -39,7 +39,8 @@ def test_kmeans_matches_oracle_ragged_segments():
 
 
 def test_kmeans_matches_oracle_large_k():
-    _check_segments([5000], 500, seed=3, rng=np.random.default_rng(2))
+    """9,000 objects: above the size where members are listed by a radix sort"""
+    _check_segments([9000], 500, seed=3, rng=np.random.default_rng(2))
 
 
 def test_kmeans_batch_properties_at_scale():
