@@ -464,11 +464,12 @@ def post_mc_measure(eng, cx, args):
     n_rec = int(nxt.sum())
     postmc.post_mc(recs[:8], seed=1)  # warm-up (module load, allocations)
     t0 = time.perf_counter()
-    med, size = postmc.post_mc(recs, seed=1)
+    med, size = postmc.post_mc_steps(steps, nxt, seed=1)
     gpu_s = time.perf_counter() - t0
     out = {"records": n_rec, "replicas": cx.n_rep, "representatives": int(med.shape[0]),
            "gpu_s": gpu_s, "records_per_s": n_rec / gpu_s,
-           "scope": "postmc.post_mc: upload, batched k-means (50 per replica), pooled k-means "
+           "scope": "postmc.post_mc_steps on the records as downloaded: upload, batched k-means "
+                    "(50 per replica), pooled k-means "
                     "(500), host wall clock"}
     if not args.no_cpu:
         from oracle import kmeans as ok

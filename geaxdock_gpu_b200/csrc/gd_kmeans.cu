@@ -106,23 +106,39 @@ __global__ void init_centres(const float *__restrict__ sh, int dim, const Seg *_
     cen[(size_t)c * dim + j] = sh[(size_t)(g.off + (c - g.cbase)) * dim + j];
 }
 
+/* Nearest centre of each object. The centres of the clusters of every segment the block's
+ * objects belong to (a contiguous range) are staged in shared memory when they fit (SMEM_CL
+ * clusters), so that the 9 x k loads per object are shared-memory broadcasts. */
+constexpr int SMEM_CL = 1024;
+
 template <int D>
-__global__ void assign_kernel(const float *__restrict__ sh, const Seg *__restrict__ seg,
-                              const int *__restrict__ seg_of, const unsigned char *__restrict__ act,
-                              int n_obj, const float *__restrict__ cen, int *__restrict__ mem,
-                              int *__restrict__ changed) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(256) assign_kernel(
+    const float *__restrict__ sh, const Seg *__restrict__ seg, const int *__restrict__ seg_of,
+    const unsigned char *__restrict__ act, int n_obj, const float *__restrict__ cen,
+    int *__restrict__ mem, int *__restrict__ changed) {
+  __shared__ float sc[SMEM_CL * D];
+  const int p0 = blockIdx.x * blockDim.x;
+  const int pl = min(p0 + (int)blockDim.x, n_obj) - 1;
+  const int c0 = seg[seg_of[p0]].cbase;
+  const Seg gl = seg[seg_of[pl]];
+  const int nc = gl.cbase + gl.k - c0;
+  const bool staged = nc <= SMEM_CL;
+  if (staged)
+    for (int i = threadIdx.x; i < nc * D; i += blockDim.x) sc[i] = cen[(size_t)c0 * D + i];
+  __syncthreads();
+  const int p = p0 + threadIdx.x;
   if (p >= n_obj) return;
   const int s = seg_of[p];
   if (!act[s]) return;
   const Seg g = seg[s];
+  const float *cb = staged ? sc + (size_t)(g.cbase - c0) * D : cen + (size_t)g.cbase * D;
   float o[D];
 #pragma unroll
   for (int j = 0; j < D; ++j) o[j] = sh[(size_t)p * D + j];
   int best = 0;
   float best_d = 0.0f;
   for (int c = 0; c < g.k; ++c) {
-    const float *q = cen + (size_t)(g.cbase + c) * D;
+    const float *q = cb + (size_t)c * D;
     float d = 0.0f;
 #pragma unroll
     for (int j = 0; j < D; ++j) {
@@ -198,6 +214,8 @@ __global__ void update_sorted_kernel(const float *__restrict__ sh, int dim,
   const int b = begin[c], e = end[c];
   if (e <= b) return;
   float s = 0.0f;
+  /* unrolled so that the gathers run ahead of the (ordered) additions */
+#pragma unroll 8
   for (int i = b; i < e; ++i) s = __fadd_rn(s, sh[(size_t)pos[i] * dim + j]);
   cen[(size_t)c * dim + j] = __fdiv_rn(s, (float)(e - b));
 }
@@ -216,6 +234,18 @@ __global__ void step_kernel(const Seg *__restrict__ seg, int n_seg, int *__restr
     if (more) atomicAdd(n_active, 1);
   }
   changed[s] = 0;
+}
+
+/* the same from the sorted member lists (last member = the largest position in the list) */
+__global__ void medoid_sorted_kernel(int n_cl, const int *__restrict__ begin,
+                                     const int *__restrict__ end, const int *__restrict__ pos,
+                                     const int *__restrict__ perm, int *__restrict__ medoid,
+                                     int *__restrict__ size) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n_cl) return;
+  const int b = begin[c], e = end[c];
+  medoid[c] = e > b ? perm[pos[e - 1]] : -1;
+  size[c] = e > b ? e - b : 0;
 }
 
 __global__ void medoid_kernel(const Seg *__restrict__ seg, const int *__restrict__ cseg, int n_cl,
@@ -368,7 +398,17 @@ int kmeans_device(const KmeansJob &job, KmeansResult &res, std::string &err) {
       ok(cudaStreamSynchronize(st));
       if (h_act == 0 || pass > job.max_iter + 1) break;
     }
-    medoid_kernel<<<bc, T, 0, st>>>(dseg, dcseg, n_cl, mem, perm, medoid, size);
+    if (sorted) {
+      /* member lists of the final memberships */
+      cluster_key_kernel<<<bo, T, 0, st>>>(dseg, dseg_of, mem, n_obj, key, pos);
+      ok(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, key, key2, pos, pos2, n_obj, 0, 31, st));
+      ok(cudaMemsetAsync(cb, 0, sizeof(int) * n_cl, st));
+      ok(cudaMemsetAsync(ce, 0, sizeof(int) * n_cl, st));
+      bounds_kernel<<<bo, T, 0, st>>>(key2, n_obj, n_cl, cb, ce);
+      medoid_sorted_kernel<<<bc, T, 0, st>>>(n_cl, cb, ce, pos2, perm, medoid, size);
+    } else {
+      medoid_kernel<<<bc, T, 0, st>>>(dseg, dcseg, n_cl, mem, perm, medoid, size);
+    }
     unshuffle_kernel<<<bo, T, 0, st>>>(perm, mem, n_obj, orig);
     ok(cudaGetLastError());
     ok(cudaMemcpyAsync(res.membership.data(), orig, sizeof(int) * n_obj, cudaMemcpyDeviceToHost,

@@ -54,23 +54,37 @@ def permutation(seed: int, segment: int, n: int) -> np.ndarray:
     return out
 
 
-def _representatives(records: np.ndarray, seg_off, k, med, size, base):
+def _order(E: np.ndarray, seg_off, k, med, size):
     """Per segment: its clusters' representatives (empty clusters dropped), sorted by total
-    energy (stable) when the segment was clustered, in record order when it was not."""
-    out_rec, out_sz = [], []
-    for s in range(len(seg_off) - 1):
-        n_s = seg_off[s + 1] - seg_off[s]
-        cnt = min(k[s], n_s)
-        m = med[base[s]:base[s] + cnt]
-        z = size[base[s]:base[s] + cnt]
-        ok = m >= 0
-        r, z = records[m[ok]], z[ok]
-        if n_s >= k[s]:
-            o = np.argsort(r["energy"]["e"][:, abi.MAXWEI - 1], kind="stable")
-            r, z = r[o], z[o]
-        out_rec.append(r)
-        out_sz.append(z)
-    return out_rec, out_sz
+    energy (stable) when the segment was clustered, in record order when it was not; all
+    segments in segment order. Returns (object indices into E, cluster sizes)."""
+    off = np.asarray(seg_off, np.int64)
+    kk = np.asarray(k, np.int64)
+    n_s = np.diff(off)
+    cnt = np.minimum(kk, n_s)
+    seg = np.repeat(np.arange(cnt.shape[0]), cnt)
+    ok = med >= 0
+    m = med[ok].astype(np.int64)
+    clustered = (n_s >= kk)[seg[ok]]
+    energy = np.where(clustered, E[m, abi.MAXWEI - 1], np.float32(0.0))
+    order = np.lexsort((np.flatnonzero(ok), energy, seg[ok]))  # segment, energy, cluster
+    return m[order], np.asarray(size)[ok][order]
+
+
+def post_mc_indices(E: np.ndarray, seg_off, seed: int = 0, k1: int = 50, k2: int = 500,
+                    device: int = 0) -> Tuple[np.ndarray, np.ndarray]:
+    """post_mc on the energy rows E [n][10] of all records, segment s = the records of replica
+    s: (indices into E of the representatives, sorted by total energy; cluster sizes)."""
+    E = np.asarray(E, np.float32)
+    off = np.asarray(seg_off, np.int32)
+    k = [k1] * (off.shape[0] - 1)
+    _, med, size, _, _ = kmeans(E[:, :DIM], off, k, seed, device=device)
+    pool, _ = _order(E, off, k, med, size)
+    off2 = np.asarray([0, pool.shape[0]], np.int32)
+    Ep = E[pool]
+    _, med2, size2, _, _ = kmeans(Ep[:, :DIM], off2, [k2], seed + 1, device=device)
+    fin, sz = _order(Ep, off2, [k2], med2, size2)
+    return pool[fin], sz
 
 
 def post_mc(replica_records: Dict[int, np.ndarray] | List[np.ndarray], seed: int = 0,
@@ -80,17 +94,26 @@ def post_mc(replica_records: Dict[int, np.ndarray] | List[np.ndarray], seed: int
     recs = [replica_records[i] for i in range(len(replica_records))]
     if not recs:
         return np.zeros(0, abi.RECORD_DTYPE), np.zeros(0, np.int32)
-    allrec = np.concatenate(recs)
-    off = np.concatenate([[0], np.cumsum([r.shape[0] for r in recs])]).astype(np.int32)
-    k = [k1] * len(recs)
-    _, med, size, _, base = kmeans(allrec["energy"]["e"][:, :DIM], off, k, seed, device=device)
-    pool_r, _ = _representatives(allrec, off, k, med, size, base)
-    pool = np.concatenate(pool_r)
-    off2 = np.asarray([0, pool.shape[0]], np.int32)
-    _, med2, size2, _, base2 = kmeans(pool["energy"]["e"][:, :DIM], off2, [k2], seed + 1,
-                                      device=device)
-    r, z = _representatives(pool, off2, [k2], med2, size2, base2)
-    return r[0], z[0]
+    off = np.concatenate([[0], np.cumsum([r.shape[0] for r in recs])]).astype(np.int64)
+    E = np.concatenate([r["energy"]["e"] for r in recs])
+    idx, sz = post_mc_indices(E, off, seed, k1, k2, device)
+    rep = np.searchsorted(off, idx, side="right") - 1
+    out = np.array([recs[r][i - off[r]] for r, i in zip(rep, idx)], dtype=abi.RECORD_DTYPE)
+    return out.reshape(-1), sz
+
+
+def post_mc_steps(steps: np.ndarray, next_ptr: np.ndarray, seed: int = 0, k1: int = 50,
+                  k2: int = 500, device: int = 0) -> Tuple[np.ndarray, np.ndarray]:
+    """post_mc on Engine.records() output directly (steps [n_rep][m], the first next_ptr[r]
+    of row r filled), without building per-replica arrays."""
+    n, m = steps.shape
+    nxt = np.asarray(next_ptr, np.int64)
+    fi = np.flatnonzero((np.arange(m)[None, :] < nxt[:, None]).ravel())
+    flat = steps.reshape(-1)
+    E = flat["energy"]["e"][fi]
+    off = np.concatenate([[0], np.cumsum(nxt)])
+    idx, sz = post_mc_indices(E, off, seed, k1, k2, device)
+    return flat[fi[idx]], sz
 
 
 def write_states(records: np.ndarray, path: str):

@@ -75,3 +75,5 @@ def test_post_mc_matches_oracle_on_run_records():
     want_r, want_z = ok.post_mc(recs, seed=21)
     assert got_r.shape == want_r.shape and got_r.tobytes() == want_r.tobytes()
     assert np.array_equal(got_z, want_z)
+    st_r, st_z = postmc.post_mc_steps(steps, nxt, seed=21)
+    assert st_r.tobytes() == want_r.tobytes() and np.array_equal(st_z, want_z)
