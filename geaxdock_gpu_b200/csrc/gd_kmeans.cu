@@ -214,9 +214,19 @@ __global__ void update_sorted_kernel(const float *__restrict__ sh, int dim,
   const int b = begin[c], e = end[c];
   if (e <= b) return;
   float s = 0.0f;
-  /* unrolled so that the gathers run ahead of the (ordered) additions */
-#pragma unroll 8
-  for (int i = b; i < e; ++i) s = __fadd_rn(s, sh[(size_t)pos[i] * dim + j]);
+  /* 16 gathers in flight ahead of the (ordered) additions */
+  int i = b;
+  for (; i + 16 <= e; i += 16) {
+    int q[16];
+    float v[16];
+#pragma unroll
+    for (int u = 0; u < 16; ++u) q[u] = pos[i + u];
+#pragma unroll
+    for (int u = 0; u < 16; ++u) v[u] = sh[(size_t)q[u] * dim + j];
+#pragma unroll
+    for (int u = 0; u < 16; ++u) s = __fadd_rn(s, v[u]);
+  }
+  for (; i < e; ++i) s = __fadd_rn(s, sh[(size_t)pos[i] * dim + j]);
   cen[(size_t)c * dim + j] = __fdiv_rn(s, (float)(e - b));
 }
 
