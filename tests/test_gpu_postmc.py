@@ -77,3 +77,20 @@ def test_post_mc_matches_oracle_on_run_records():
     assert np.array_equal(got_z, want_z)
     st_r, st_z = postmc.post_mc_steps(steps, nxt, seed=21)
     assert st_r.tobytes() == want_r.tobytes() and np.array_equal(st_z, want_z)
+
+
+def test_post_mc_edge_cases():
+    """Replicas without records, replicas with fewer records than clusters, and no records
+    at all."""
+    rng = np.random.default_rng(8)
+    recs = []
+    for n in (0, 3, 0, 120, 49, 50):
+        r = np.zeros(n, abi.RECORD_DTYPE)
+        r["energy"]["e"] = rng.normal(0, 1, (n, 10)).astype(np.float32)
+        r["step"] = np.arange(n)
+        recs.append(r)
+    got_r, got_z = postmc.post_mc(recs, seed=4)
+    want_r, want_z = ok.post_mc(recs, seed=4)
+    assert got_r.tobytes() == want_r.tobytes() and np.array_equal(got_z, want_z)
+    e_r, e_z = postmc.post_mc([np.zeros(0, abi.RECORD_DTYPE)] * 3, seed=4)
+    assert e_r.shape == (0,) and e_z.shape == (0,)
