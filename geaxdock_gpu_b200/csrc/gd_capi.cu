@@ -11,7 +11,10 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
+#include <condition_variable>
+#include <deque>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -163,6 +166,118 @@ struct gd_ctx {
   int chain_gen = -1;
   GdTileDesc *d_chain_tiles = nullptr;
   int chain_tiles_cap = 0;
+  /* record streaming into host memory (gd_records_stream) */
+  struct RecStream *rs = nullptr;
+};
+
+/* rows [start[r], start[r] + off[r+1] - off[r]) of every replica's records, packed at off[r] */
+__global__ void rs_gather_kernel(const gd_record_step *__restrict__ rec, int rec_cap,
+                                 const int *__restrict__ start, const int *__restrict__ off,
+                                 int n_rep, gd_record_step *__restrict__ out) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n_rep) return;
+  const gd_record_step *src = rec + (size_t)r * rec_cap + start[r];
+  for (int i = 0, n = off[r + 1] - off[r]; i < n; ++i) out[off[r] + i] = src[i];
+}
+
+/* The worker of gd_records_stream. After each record-writing call the calling thread copies the
+ * record counters into a snapshot slot on the context's stream and queues the slot; the worker
+ * waits for the snapshot, packs every replica's records written since its previous snapshot
+ * (records are appended only, so they are complete) with a small gather kernel on its own
+ * stream, downloads the packed rows into a reused host staging buffer and copies them into the
+ * caller's array, all while the context's stream runs the next work. */
+struct RecStream {
+  static constexpr int NSNAP = 4;
+  gd_record_step *host = nullptr;
+  int cap = 0, n_rep = 0, rec_cap = 0, device = 0;
+  const gd_record_step *d_rec = nullptr;
+  cudaStream_t cs = nullptr;
+  int *d_snap[NSNAP] = {};
+  cudaEvent_t ev[NSNAP] = {};
+  bool busy[NSNAP] = {};
+  int *d_start = nullptr, *d_off = nullptr; /* [n_rep], [n_rep + 1] */
+  gd_record_step *d_pack = nullptr;
+  size_t pack_cap = 0;
+  std::deque<int> queue;
+  std::mutex mu;
+  std::condition_variable cv;
+  bool stop = false;
+  std::vector<int> prev; /* counters of the previous snapshot (0 after a restart) */
+  std::vector<int> snap; /* the latest snapshot copied */
+  cudaError_t err = cudaSuccess;
+  std::thread th;
+
+  cudaError_t one(const std::vector<int> &v, std::vector<int> &start, std::vector<int> &off,
+                  std::vector<gd_record_step> &stage) {
+    off[0] = 0;
+    for (int r = 0; r < n_rep; ++r) {
+      const int a = std::min(prev[r], cap), b = std::min(v[r], cap);
+      start[r] = a;
+      off[r + 1] = off[r] + std::max(0, b - a);
+    }
+    const size_t total = (size_t)off[n_rep];
+    if (total == 0) return cudaSuccess;
+    cudaError_t e = cudaSuccess;
+    if (total > pack_cap) {
+      if (d_pack) cudaFree(d_pack);
+      d_pack = nullptr;
+      pack_cap = 0;
+      e = cudaMalloc(&d_pack, total * sizeof(gd_record_step));
+      if (e != cudaSuccess) return e;
+      pack_cap = total;
+    }
+    if (stage.size() < total) stage.resize(total);
+    e = cudaMemcpyAsync(d_start, start.data(), sizeof(int) * n_rep, cudaMemcpyHostToDevice, cs);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(d_off, off.data(), sizeof(int) * (n_rep + 1), cudaMemcpyHostToDevice,
+                          cs);
+    if (e != cudaSuccess) return e;
+    rs_gather_kernel<<<(n_rep + 127) / 128, 128, 0, cs>>>(d_rec, rec_cap, d_start, d_off, n_rep,
+                                                          d_pack);
+    e = cudaGetLastError();
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(stage.data(), d_pack, total * sizeof(gd_record_step),
+                          cudaMemcpyDeviceToHost, cs);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(cs);
+    if (e != cudaSuccess) return e;
+    for (int r = 0; r < n_rep; ++r)
+      if (off[r + 1] > off[r])
+        memcpy(host + (size_t)r * cap + start[r], stage.data() + off[r],
+               sizeof(gd_record_step) * (size_t)(off[r + 1] - off[r]));
+    return cudaSuccess;
+  }
+
+  void worker() {
+    cudaSetDevice(device);
+    std::vector<int> v(n_rep), start(n_rep), off(n_rep + 1);
+    std::vector<gd_record_step> stage;
+    for (;;) {
+      int k;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        cv.wait(lk, [&] { return stop || !queue.empty(); });
+        if (queue.empty()) return;
+        k = queue.front();
+      }
+      cudaError_t e = cudaEventSynchronize(ev[k]);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(v.data(), d_snap[k], sizeof(int) * n_rep, cudaMemcpyDeviceToHost, cs);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(cs);
+      if (e == cudaSuccess) e = one(v, start, off, stage);
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        if (e == cudaSuccess) {
+          prev = v;
+          snap = v;
+        } else if (err == cudaSuccess) {
+          err = e;
+        }
+        queue.pop_front();
+        busy[k] = false;
+      }
+      cv.notify_all();
+    }
+  }
 };
 
 namespace {
@@ -193,6 +308,84 @@ cudaError_t d2h_rows(void *dst, size_t hpitch, const void *src, size_t dpitch, s
     for (auto &x : th) x.join();
   }
   return cudaMemcpy2D(dst, hpitch, src, dpitch, width, n, cudaMemcpyDeviceToHost);
+}
+
+/* queues a snapshot of the record counters taken after the work queued on the context's
+ * stream so far (no-op without gd_records_stream) */
+int rs_enqueue(gd_ctx *c) {
+  RecStream *r = c->rs;
+  if (!r) return GD_OK;
+  int k = -1;
+  {
+    std::unique_lock<std::mutex> lk(r->mu);
+    r->cv.wait(lk, [&] {
+      if (r->err != cudaSuccess) return true;
+      for (int i = 0; i < RecStream::NSNAP; ++i)
+        if (!r->busy[i]) return true;
+      return false;
+    });
+    if (r->err != cudaSuccess)
+      return fail(GD_ERR_CUDA, "record stream: %s", cudaGetErrorString(r->err));
+    for (int i = 0; i < RecStream::NSNAP && k < 0; ++i)
+      if (!r->busy[i]) k = i;
+    r->busy[k] = true;
+  }
+  cudaError_t e = cudaMemcpyAsync(r->d_snap[k], c->d_rec_next, sizeof(int) * c->n_rep,
+                                  cudaMemcpyDeviceToDevice, c->stream);
+  if (e == cudaSuccess) e = cudaEventRecord(r->ev[k], c->stream);
+  {
+    std::lock_guard<std::mutex> lk(r->mu);
+    if (e != cudaSuccess) {
+      r->busy[k] = false;
+      return fail(GD_ERR_CUDA, "record stream: %s", cudaGetErrorString(e));
+    }
+    r->queue.push_back(k);
+  }
+  r->cv.notify_all();
+  return GD_OK;
+}
+
+/* one more snapshot after everything queued, then wait for every copy: the host buffer then
+ * mirrors the device records */
+int rs_flush(gd_ctx *c) {
+  RecStream *r = c->rs;
+  if (!r) return GD_OK;
+  int rc = rs_enqueue(c);
+  if (rc) return rc;
+  std::unique_lock<std::mutex> lk(r->mu);
+  r->cv.wait(lk, [&] { return r->queue.empty(); });
+  if (r->err != cudaSuccess)
+    return fail(GD_ERR_CUDA, "record stream: %s", cudaGetErrorString(r->err));
+  return GD_OK;
+}
+
+/* after a flush, before the counters restart: the next copies start from record 0 */
+void rs_restart(gd_ctx *c) {
+  if (!c->rs) return;
+  std::lock_guard<std::mutex> lk(c->rs->mu);
+  std::fill(c->rs->prev.begin(), c->rs->prev.end(), 0);
+}
+
+/* stops the worker after the queued copies and frees the stream's resources */
+void rs_stop(gd_ctx *c) {
+  RecStream *r = c->rs;
+  if (!r) return;
+  {
+    std::lock_guard<std::mutex> lk(r->mu);
+    r->stop = true;
+  }
+  r->cv.notify_all();
+  if (r->th.joinable()) r->th.join();
+  for (int i = 0; i < RecStream::NSNAP; ++i) {
+    if (r->d_snap[i]) cudaFree(r->d_snap[i]);
+    if (r->ev[i]) cudaEventDestroy(r->ev[i]);
+  }
+  if (r->d_start) cudaFree(r->d_start);
+  if (r->d_off) cudaFree(r->d_off);
+  if (r->d_pack) cudaFree(r->d_pack);
+  if (r->cs) cudaStreamDestroy(r->cs);
+  delete r;
+  c->rs = nullptr;
 }
 
 template <class T>
@@ -629,6 +822,7 @@ int gd_destroy(gd_ctx *c) {
   if (!c) return GD_OK;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  rs_stop(c);
   drop_graphs(c);
   da_free(c);
   for (void *p : c->allocs) cudaFree(p);
@@ -1198,11 +1392,13 @@ int gd_mc_init(gd_ctx *c) {
   a.n_steps = 1;
   CK(cudaMemsetAsync(c->d_acs, 0, sizeof(int) * c->n_rep, c->stream));
   CK(cudaMemsetAsync(c->d_err, 0, sizeof(unsigned), c->stream));
+  if ((rc = rs_flush(c))) return rc;
+  rs_restart(c);
   rc = launch_mc(c, a, c->d_tiles, n, c->d_counters);
   if (rc) return rc;
   c->initialized = true;
   c->exchange_calls = 0;
-  return GD_OK;
+  return rs_enqueue(c);
 }
 
 int gd_reset_records(gd_ctx *c, int r0, int r1) {
@@ -1210,6 +1406,8 @@ int gd_reset_records(gd_ctx *c, int r0, int r1) {
   int rc = check_range(c, r0, r1);
   if (rc) return rc;
   const int n = r1 - r0 + 1;
+  if ((rc = rs_flush(c))) return rc;
+  rs_restart(c);
   gd::gd_reset_records_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(c->d_rec_next, r0, r1);
   CK(cudaGetLastError());
   return GD_OK;
@@ -1227,7 +1425,8 @@ int gd_mc_run(gd_ctx *c, int r0, int r1, int s1, int s2) {
   a.mode = 0;
   a.n_steps = c->mc.steps_per_exchange;
   a.step0 = s1 + s2;
-  return launch_mc(c, a, c->d_tiles, n, c->d_counters);
+  if ((rc = launch_mc(c, a, c->d_tiles, n, c->d_counters))) return rc;
+  return rs_enqueue(c);
 }
 
 int gd_exchange(gd_ctx *c, int mode_l, int mode_t) {
@@ -1303,7 +1502,7 @@ int gd_mc_run_fused(gd_ctx *c, int s1, int n_steps, int exchange) {
                      c->stream));
   CK(cudaGraphLaunch(it->second, c->stream));
   if (exchange) c->exchange_calls += chunks;
-  return GD_OK;
+  return rs_enqueue(c);
 }
 
 int gd_sync(gd_ctx *c) {
@@ -1360,6 +1559,55 @@ int gd_get_record_counts(gd_ctx *c, int *next_ptr, int r0, int r1) {
   CK(cudaStreamSynchronize(c->stream));
   CK(cudaMemcpy(next_ptr, c->d_rec_next + r0, sizeof(int) * (r1 - r0 + 1),
                 cudaMemcpyDeviceToHost));
+  return GD_OK;
+}
+
+int gd_records_stream(gd_ctx *c, gd_record_step *steps, int cap) {
+  if (!c) return fail(GD_ERR_INVALID, "null context");
+  if (c->rs) {
+    const int rc = rs_flush(c);
+    rs_stop(c);
+    if (rc) return rc;
+  }
+  if (!steps) return GD_OK;
+  if (!c->mc.record || !c->d_rec) return fail(GD_ERR_STATE, "records are disabled");
+  if (cap < 1 || cap > c->rec_cap)
+    return fail(GD_ERR_INVALID, "cap %d outside 1..record capacity %d", cap, c->rec_cap);
+  CK(cudaSetDevice(c->device));
+  RecStream *r = new RecStream;
+  r->host = steps;
+  r->cap = cap;
+  r->n_rep = c->n_rep;
+  r->rec_cap = c->rec_cap;
+  r->device = c->device;
+  r->d_rec = c->d_rec;
+  r->snap.assign(c->n_rep, 0);
+  r->prev.assign(c->n_rep, 0);
+  cudaError_t e = cudaStreamCreateWithFlags(&r->cs, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMalloc(&r->d_start, sizeof(int) * (size_t)c->n_rep);
+  if (e == cudaSuccess) e = cudaMalloc(&r->d_off, sizeof(int) * ((size_t)c->n_rep + 1));
+  for (int i = 0; i < RecStream::NSNAP && e == cudaSuccess; ++i) {
+    e = cudaMalloc(&r->d_snap[i], sizeof(int) * (size_t)c->n_rep);
+    if (e == cudaSuccess)
+      e = cudaEventCreateWithFlags(&r->ev[i], cudaEventDisableTiming | cudaEventBlockingSync);
+  }
+  c->rs = r;
+  if (e != cudaSuccess) {
+    rs_stop(c);
+    return fail(GD_ERR_CUDA, "gd_records_stream: %s", cudaGetErrorString(e));
+  }
+  r->th = std::thread([r] { r->worker(); });
+  return rs_enqueue(c);
+}
+
+int gd_records_stream_flush(gd_ctx *c, int *next_ptr) {
+  if (!c || !c->rs) return fail(GD_ERR_STATE, "gd_records_stream is not active");
+  const int rc = rs_flush(c);
+  if (rc) return rc;
+  if (next_ptr) {
+    std::lock_guard<std::mutex> lk(c->rs->mu);
+    std::copy(c->rs->snap.begin(), c->rs->snap.end(), next_ptr);
+  }
   return GD_OK;
 }
 
@@ -2277,7 +2525,7 @@ int gd_sur_collect(gd_ctx *c, int s1, int n_steps, int exchange) {
   if (rc) return rc;
   if (d->smp_hi != g0) d->smp_lo = g0; /* not contiguous with the earlier samples */
   d->smp_hi = g0 + (long long)n_steps * c->n_rep;
-  return GD_OK;
+  return rs_enqueue(c);
 }
 
 int gd_sur_train(gd_ctx *c, int iterations, float *losses) {
@@ -2327,6 +2575,7 @@ int gd_sur_train(gd_ctx *c, int iterations, float *losses) {
 int gd_da_run(gd_ctx *c, int s1, int n_steps, int exchange) {
   int rc = da_run_steps(c, s1, n_steps, exchange, false);
   if (rc) return rc;
+  if ((rc = rs_enqueue(c))) return rc;
   DaState *d = c->da;
   const bool controller = d->prm.fallback_accept > 0.0f;
   if (!controller && d->prm.split > 0) return GD_OK;

@@ -60,6 +60,8 @@ def lib() -> C.CDLL:
         "gd_get_records": [vp, vp, C.c_int, C.c_int],
         "gd_get_records_raw": [vp, vp, vp, C.c_int, C.c_int, C.c_int],
         "gd_get_record_counts": [vp, vp, C.c_int, C.c_int],
+        "gd_records_stream": [vp, vp, C.c_int],
+        "gd_records_stream_flush": [vp, vp],
         "gd_get_etotal": [vp, fp, C.c_int, C.c_int],
         "gd_get_replicas": [vp, vp, C.c_int, C.c_int],
         "gd_get_state": [vp, vp, C.c_int, C.c_int],
@@ -154,11 +156,13 @@ class Engine:
             check(lib().gd_replica_offset(self.h, k, C.byref(o)))
             self.offsets.append(o.value)
         self.cap = params.steps_per_dump + 1
+        self._stream_buf = None
 
     def close(self):
         if getattr(self, "h", None):
             lib().gd_destroy(self.h)
             self.h = None
+        self._stream_buf = None
 
     def __del__(self):
         try:
@@ -239,6 +243,24 @@ class Engine:
         steps = np.empty((n, m), abi.RECORD_DTYPE)
         check(lib().gd_get_records_raw(self.h, _p(steps), _p(nxt), r0, r1, m))
         return steps, nxt
+
+    def stream_records(self, cap: int) -> np.ndarray:
+        """Starts gd_records_stream into a new host array [n_rep][cap] (RECORD_DTYPE): the
+        records are copied while the run proceeds; stream_flush() completes and returns it."""
+        buf = np.empty((self.n_rep, cap), abi.RECORD_DTYPE)
+        check(lib().gd_records_stream(self.h, _p(buf), cap))
+        self._stream_buf = buf
+        return buf
+
+    def stream_flush(self):
+        """(steps [n_rep][cap], next_ptr [n_rep]) mirroring the device records now."""
+        nxt = np.empty(self.n_rep, np.int32)
+        check(lib().gd_records_stream_flush(self.h, _p(nxt)))
+        return self._stream_buf, nxt
+
+    def stream_stop(self):
+        check(lib().gd_records_stream(self.h, None, 0))
+        self._stream_buf = None
 
     def lig_records(self, r0=0, r1=None) -> bytes:
         """LigRecord array bytes (reference layout, src/dock.h:377-381)."""

@@ -265,6 +265,18 @@ int gd_get_records_raw(gd_ctx *ctx, gd_record_step *steps, int *next_ptr, int re
                        int rep_end, int cap);
 /* Records held per replica (next_ptr) for rep_begin..rep_end. */
 int gd_get_record_counts(gd_ctx *ctx, int *next_ptr, int rep_begin, int rep_end);
+/* The records downloaded while the run proceeds, instead of all at the end (the reference
+ * copies the whole LigRecord array after each dump window, src/kernel_cuda_lancher_siglegpu.cu:
+ * 36-46). From this call on, every call that writes records (gd_mc_init, gd_mc_run,
+ * gd_mc_run_fused, gd_sur_collect, gd_da_run) also has a host worker thread copy, on its own
+ * CUDA stream and while the next work runs, the record rows written so far into
+ * steps[r * cap + i] (all replicas, the first `cap` records each; pageable or pinned memory,
+ * which must stay valid until streaming stops). gd_records_stream_flush waits for the copies
+ * of everything queued so far and returns the counts (next_ptr[n_rep]); the buffer then holds
+ * what gd_get_records_raw with the same cap would return. gd_reset_records and gd_mc_init
+ * flush first (read the window before resetting it). steps = NULL flushes and stops. */
+int gd_records_stream(gd_ctx *ctx, gd_record_step *steps, int cap);
+int gd_records_stream_flush(gd_ctx *ctx, int *next_ptr);
 int gd_get_etotal(gd_ctx *ctx, float *etotal, int rep_begin, int rep_end);
 int gd_get_replicas(gd_ctx *ctx, gd_replica *replicas, int rep_begin, int rep_end);
 int gd_get_state(gd_ctx *ctx, gd_replica_state *state, int rep_begin, int rep_end);

@@ -1,0 +1,79 @@
+"""Record streaming (gd_records_stream): the host buffer filled while the run proceeds equals,
+after each flush, the records downloaded at that point (gd_get_records_raw), through plain
+steps, the fused loop, a records reset, delayed-acceptance collect steps, and a stream started
+before gd_mc_init."""
+import numpy as np
+import pytest
+
+from geaxdock_gpu_b200 import abi, engine
+from tests.conftest import have_gpu
+from tests.golden.fixtures import load_ref
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not have_gpu(), reason="needs a B200")]
+
+
+def _same(e, buf, nxt):
+    steps, n2 = e.records()
+    assert np.array_equal(nxt, n2)
+    for r in range(e.n_rep):
+        assert buf[r, :nxt[r]].tobytes() == steps[r, :nxt[r]].tobytes(), r
+
+
+@pytest.fixture(scope="module")
+def cx_ff():
+    z, cx, ff = load_ref("1a07C1")
+    return cx, ff
+
+
+def test_stream_matches_downloads(cx_ff):
+    cx, ff = cx_ff
+    params = abi.mc_params(steps_per_exchange=10, steps_per_dump=200, seed=3)
+    with engine.Engine(ff, [cx], params) as e:
+        e.mc_init()
+        buf = e.stream_records(201)
+        for it in range(5):
+            e.mc_run(0, it * 10)
+            e.exchange(int(not (it % 2)))
+        b, nxt = e.stream_flush()
+        assert b is buf and nxt.max() > 1
+        _same(e, buf, nxt)
+        e.run_fused(50, 50, exchange=True)
+        _same(e, *e.stream_flush())
+        e.reset_records()
+        for it in range(3):
+            e.mc_run(200, it * 10)
+        _same(e, *e.stream_flush())
+        e.stream_stop()
+        e.mc_run(200, 30)
+        steps, n2 = e.records()
+        assert n2.max() > 0
+
+
+def test_stream_before_init_and_small_cap(cx_ff):
+    cx, ff = cx_ff
+    params = abi.mc_params(steps_per_exchange=10, steps_per_dump=200, seed=4)
+    with engine.Engine(ff, [cx], params) as e:
+        buf = e.stream_records(25)
+        e.mc_init()
+        for it in range(4):
+            e.mc_run(0, it * 10)
+        b, nxt = e.stream_flush()
+        steps, n2 = e.records()
+        assert np.array_equal(nxt, n2)
+        for r in range(e.n_rep):
+            m = min(25, nxt[r])
+            assert b[r, :m].tobytes() == steps[r, :m].tobytes()
+
+
+def test_stream_delayed_acceptance_collect(cx_ff):
+    cx, ff = cx_ff
+    params = abi.mc_params(steps_per_exchange=10, steps_per_dump=400, seed=5,
+                           move_kind=abi.MOVE_GAUSSIAN)
+    with engine.Engine(ff, [cx], params) as e:
+        e.mc_init()
+        sur = engine.Surrogate(e, hidden=128, batch=256, sample_cap=1 << 14)
+        buf = e.stream_records(401)
+        sur.collect(0, 40, exchange=True)
+        sur.train(5)
+        sur.run(40, 40, exchange=True)
+        _same(e, *e.stream_flush())
