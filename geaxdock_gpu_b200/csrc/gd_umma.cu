@@ -28,6 +28,7 @@
  */
 #include <cuda.h> /* CUtensorMap and its enums; the encoder is fetched from the driver at run time */
 
+#include <atomic>
 #include <cstdint>
 
 #include "gd_mlp.cuh"
@@ -291,15 +292,16 @@ typedef CUresult (*EncodeTiled)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, 
                                 CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
 EncodeTiled encoder() {
-  static EncodeTiled fn = nullptr;
-  if (!fn) {
+  /* looked up once (thread-safe static initialisation) */
+  static const EncodeTiled fn = [] {
     void *p = nullptr;
     cudaDriverEntryPointQueryResult q;
     if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
             cudaSuccess &&
         q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<EncodeTiled>(p);
-  }
+      return reinterpret_cast<EncodeTiled>(p);
+    return (EncodeTiled) nullptr;
+  }();
   return fn;
 }
 
@@ -326,14 +328,18 @@ int make_map(CUtensorMap *m, const UmmaOperand &o, int box_rows) {
 template <int BN>
 int launch(const UmmaOperand &A, const UmmaOperand &B, int M, int N, int K, int splits,
            const UmmaEpilogue &e, int *err, cudaStream_t s) {
-  static bool attr = false;
+  /* the shared-memory limit is a per-device attribute: set once per device */
+  static std::atomic<unsigned long long> attr_set{0};
   const size_t smem =
       tile_bytes(A.mn_major, BM, K) + tile_bytes(B.mn_major, BN, K) + STAGE_BYTES + 1024;
-  if (!attr) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return -2;
+  const unsigned long long bit = 1ull << (dev & 63);
+  if (!(attr_set.load() & bit)) {
     if (cudaFuncSetAttribute(umma_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              256 * 256 + BN * 512 + STAGE_BYTES + 1024) != cudaSuccess)
       return -2;
-    attr = true;
+    attr_set.fetch_or(bit);
   }
   CUtensorMap ta, tb;
   int rc;
