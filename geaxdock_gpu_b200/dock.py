@@ -12,7 +12,8 @@ records of all replicas reach steps_per_dump x n_rep; then post_mc clustering (p
 the table of the 500 representatives (printStates) in the --csv file, and a run summary.
 Options of this implementation: --device, --seed (Monte Carlo and clustering), --dump-dir
 (write every dump window's LigRecord array, records.py), --gaussian (Gaussian moves instead
-of the reference's uniform ones).
+of the reference's uniform ones), --surrogate (delayed acceptance with the learned surrogate,
+trained on the first window's plain steps).
 """
 from __future__ import annotations
 
@@ -44,6 +45,12 @@ def parse(argv=None):
                     "reference seeds its generators")
     ap.add_argument("--dump-dir", default="", help="write each dump window's records here")
     ap.add_argument("--gaussian", action="store_true")
+    ap.add_argument("--surrogate", action="store_true",
+                    help="delayed acceptance with the learned energy surrogate: the first dump "
+                         "window's plain steps train it (one pass of Adam over their proposals), "
+                         "later windows run delayed-acceptance steps")
+    ap.add_argument("--train-iterations", type=int, default=0,
+                    help="--surrogate: Adam steps (default: one pass over the samples)")
     ap.add_argument("--max-dumps", type=int, default=1000,
                     help="stop after this many dump windows even if records are short")
     return ap.parse_args(argv)
@@ -68,16 +75,28 @@ def run(a) -> int:
     have = 0
     s1 = 0
     t_mc = 0.0
+    t_train = 0.0
     with engine.Engine(ff, [cx], params, device=a.device) as e:
         e.mc_init()
+        sur = engine.Surrogate(e, sample_cap=n_rep * spd) if a.surrogate else None
         dump = 0
         while have < est and dump < a.max_dumps:
             if s1 != 0:
                 e.reset_records()
             t0 = time.perf_counter()
-            e.run_fused(s1, spd, exchange=True)
+            if sur is None:
+                e.run_fused(s1, spd, exchange=True)
+            elif dump == 0:
+                sur.collect(s1, spd, exchange=True)  # plain steps; their proposals are samples
+            else:
+                sur.run(s1, spd, exchange=True)
             e.sync()
             t_mc += time.perf_counter() - t0
+            if sur is not None and dump == 0:
+                t0 = time.perf_counter()
+                iters = a.train_iterations or max(1, n_rep * spd // 8192)
+                sur.train(iters)
+                t_train = time.perf_counter() - t0
             steps, nxt = e.records()
             for i in range(n_rep):
                 per_rep[i].append(steps[i, :nxt[i]])
@@ -87,6 +106,7 @@ def run(a) -> int:
                 records.write_dump(e, a.dump_dir, a.id, s1 // spd)
             s1 += spd
             dump += 1
+        sur_stats = sur.stats() if sur is not None else None
     recs = [np.concatenate(r) if r else np.zeros(0, abi.RECORD_DTYPE) for r in per_rep]
     t0 = time.perf_counter()
     medoids, sizes = postmc.post_mc(recs, seed=seed & 0xFFFFFFFF, device=a.device)
@@ -104,6 +124,11 @@ def run(a) -> int:
     print("rotational scale\t\t%.8f %.8f %.8f" % (a.r, a.r, a.r))
     print("temperatures\t\t\t%d (%.4f .. %.4f)" % (a.nt, a.floor_temp, a.ceiling_temp))
     print("acceptance ratio\t\t%.5f" % (have / trials if trials else 0.0))
+    if a.surrogate:
+        st = sur_stats[0] if sur_stats else {}
+        print("surrogate\t\t\tproposed %d passed %d accepted %d rmse %.4f (training %.3f s)"
+              % (st.get("proposed", 0), st.get("passed", 0), st.get("accepted", 0),
+                 st.get("rmse", 0.0), t_train))
     print("representatives\t\t\t%d" % medoids.shape[0])
     print("Monte Carlo time (s)\t\t%.3f\npost-processing time (s)\t%.3f\ntotal time (s)\t\t\t%.3f"
           % (t_mc, t_post, time.perf_counter() - t_start))

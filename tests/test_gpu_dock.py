@@ -102,3 +102,20 @@ def test_dock_command_line(tmp_path, capsys):
     assert np.all(np.diff(body[:, -1]) >= 0)  # sorted by total energy
     d0 = records.read_dump(str(tmp_path / "dumps" / "synth_0000.bin"))
     assert d0.shape[0] == 4 * 2 * 3 and d0["next_ptr"].max() > 0
+
+
+def test_dock_command_line_with_surrogate(tmp_path, capsys):
+    rng = np.random.default_rng(6)
+    _write_complex(tmp_path, rng)
+    z, _, _ = load_ref("1a07C1")
+    _write_paras(tmp_path / "paras", abi.enepara_raw_from_array(z["enepara_raw"]))
+    out = tmp_path / "out.csv"
+    rc = dock.main(["-p", str(tmp_path / "p.pdb"), "-l", str(tmp_path / "l.sdf"),
+                    "-s", str(tmp_path / "p.ff"), "--para", str(tmp_path / "paras"),
+                    "-i", "synth", "-o", str(out), "--nt", "2", "--seed", "7",
+                    "--max-dumps", "2", "--gaussian", "--surrogate", "--train-iterations", "20"])
+    assert rc == 0
+    text = capsys.readouterr().out
+    assert "surrogate" in text and "proposed" in text
+    body = np.array([[float(v) for v in l.split()] for l in out.read_text().splitlines()[1:]])
+    assert body.shape[0] >= 1 and np.all(np.isfinite(body))
