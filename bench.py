@@ -679,6 +679,24 @@ def profile_da(args):
         print(json.dumps({"profile_da": sur.stats()[0]}), flush=True)
 
 
+def profile_mc(args):
+    """A short plain run on a 128-replica subset of the config-1 system (8 ligand conformers,
+    2 protein conformers, 8 temperatures, no records): four 10-step launches, small enough for
+    multi-pass profiler captures."""
+    from geaxdock_gpu_b200 import engine
+    w = workload(42)
+    cx = w.complexes[0].subset(n_lig=8, n_prt=2, n_tmp=8)
+    params = w.params
+    params.record = 0
+    with engine.Engine(w.ff, [cx], params) as e:
+        e.set_tile(6, 1024, 2)
+        e.mc_init()
+        for it in range(4):
+            e.mc_run(0, it * params.steps_per_exchange)
+        e.sync()
+    print(json.dumps({"profile_mc": {"replicas": cx.n_rep, "launches": 4}}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -698,6 +716,9 @@ def main():
                          "profiler launch lists; prints its statistics")
     ap.add_argument("--move-mult", type=float, default=1.0,
                     help="--profile-da / --screen-da: move scales multiplied by this factor")
+    ap.add_argument("--profile-mc", action="store_true",
+                    help="only a short plain run on a 128-replica subset of the config-1 system "
+                         "(four 10-step launches), for multi-pass profiler captures")
     ap.add_argument("--screen-da", action="store_true",
                     help="only the config-4 run (delayed acceptance on the config-2 screen); "
                          "prints its own JSON line")
@@ -707,6 +728,9 @@ def main():
         return
     if args.profile_da:
         profile_da(args)
+        return
+    if args.profile_mc:
+        profile_mc(args)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
