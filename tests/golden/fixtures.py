@@ -22,3 +22,9 @@ def load_ref(name="1a07C1"):
         mcs_x=z["mcs_x"], mcs_y=z["mcs_y"], mcs_z=z["mcs_z"], mcs_tcc=z["mcs_tcc"], temp=temp)
     ff = abi.enepara_from_array(z["enepara"])
     return z, cx, ff
+
+
+def load_trajectory():
+    """The reference's sample trajectory of 1a07C1 (see make_trajectory.py): float64 rows of
+    PrtIdx, LigIdx, the six move-vector entries, cms and the weighted total energy."""
+    return np.load(os.path.join(HERE, "trajectory_1a07C1.npz"))["rows"]

@@ -371,3 +371,21 @@ def test_autotune_picks_a_tile_and_keeps_the_chains(raw, tmp_path):
         eng.sync()
         again = autotune.tune(eng, cache_path=str(tmp_path / "cache.json"))
         assert again["cached"] and again["tile"] == res["tile"]
+
+
+def test_eval_energy_reproduces_reference_trajectory():
+    """The library's energy kernel on every accepted step of the reference's own sample
+    trajectory of 1a07C1 (data/trajectory.out, printed with %f by printLigandTrajectories,
+    src/util.C:2041-2056): weighted total within 1e-5 and cms within 2e-6 of the printed
+    values, the bounds the FP64 oracle meets on the same rows."""
+    from tests.golden.fixtures import load_trajectory
+    rows = load_trajectory()
+    z, cx, ff = load_ref("1a07C1")
+    with engine.Engine(ff, [cx], abi.mc_params()) as eng:
+        for ip, il in {(int(a), int(b)) for a, b in rows[:, :2]}:
+            sel = (rows[:, 0] == ip) & (rows[:, 1] == il)
+            got = eng.eval_energy(0, ip, il, rows[sel, 2:8].astype(np.float32))
+            de = np.abs(got["e"][:, 9].astype(np.float64) - rows[sel, 9])
+            dc = np.abs(got["cms"].astype(np.float64) - rows[sel, 8])
+            assert de.max() <= 1e-5, (ip, il, int(de.argmax()), de.max())
+            assert dc.max() <= 2e-6, (ip, il, int(dc.argmax()), dc.max())

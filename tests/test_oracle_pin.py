@@ -215,3 +215,30 @@ def test_fp32_baseline_agrees_with_fp64(ref):
         o64 = po.pose_energy(ff, cx, ip, il, z["pose_mm"][i], rm, 64)
         o32 = po.pose_energy(ff, cx, ip, il, z["pose_mm"][i], rm, 32)
         assert rel_errors(o32["e"], o64, ff).max() <= 2e-5
+
+
+# The reference's sample trajectory prints each value with %f (6 decimals, +-5e-7) after an
+# FP32 evaluation on the GPU: the weighted total is held to 1e-5, the contact fraction to 2e-6.
+TRAJ_E_TOL = 1e-5
+TRAJ_CMS_TOL = 2e-6
+
+
+def test_oracle_reproduces_reference_trajectory():
+    """Every accepted step of data/trajectory.out (1a07C1, written by printLigandTrajectories,
+    src/util.C:2041-2056) re-evaluated from its protein/ligand index and move vector with the
+    reference's own parameter file and .ff: the weighted total and cms come back to the
+    printed precision, which pins the loaders, the parameter fold and CalcEnergy_d together
+    on data the reference produced itself."""
+    from tests.golden.fixtures import load_trajectory
+    rows = load_trajectory()
+    z, cx, ff = load_ref("1a07C1")
+    rm = po.ref_map(ff, cx)
+    assert rows.shape == (2666, 10)
+    de = np.zeros(rows.shape[0])
+    dc = np.zeros(rows.shape[0])
+    for i, r in enumerate(rows):
+        o = po.pose_energy(ff, cx, int(r[0]), int(r[1]), r[2:8].astype(np.float32), rm, 64)
+        de[i] = abs(o["e"][9] - r[9])
+        dc[i] = abs(o["cms"] - r[8])
+    assert de.max() <= TRAJ_E_TOL, (int(de.argmax()), de.max())
+    assert dc.max() <= TRAJ_CMS_TOL, (int(dc.argmax()), dc.max())
