@@ -1762,6 +1762,54 @@ int gd_eval_energy(gd_ctx *c, int ci, int prt_conf, int lig_conf, const float *m
   return GD_OK;
 }
 
+/* One thread per (pose, atom): the rotation of the pose and the placed atom, with the same
+ * gd_rotation / gd_place_atom the Monte Carlo kernel places its ligands with. */
+__global__ void gd_place_kernel(const GdDevComplex *cxs, int ci, int lig_conf, const float *mm,
+                                int n, float *xyz) {
+  const GdDevComplex &cx = cxs[ci];
+  const int L = cx.lna;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)n * L) return;
+  const int pose = (int)(i / L), l = (int)(i % L);
+  float m[6], rot[9];
+  for (int k = 0; k < 6; ++k) m[k] = mm[pose * 6 + k];
+  gd_rotation(m, rot);
+  const float *lc = cx.lig_center + lig_conf * 3;
+  const float4 o = cx.lig_pos[lig_conf * L + l];
+  gd_place_atom(rot, GD_ADD(m[0], lc[0]), GD_ADD(m[1], lc[1]), GD_ADD(m[2], lc[2]), o.x, o.y,
+                o.z, &xyz[i * 3], &xyz[i * 3 + 1], &xyz[i * 3 + 2]);
+}
+
+int gd_place_ligand(gd_ctx *c, int ci, int lig_conf, const float *mm, int n, float *xyz) {
+  if (!c || (n > 0 && (!mm || !xyz))) return fail(GD_ERR_INVALID, "null argument");
+  if (ci < 0 || ci >= c->n_complex) return fail(GD_ERR_INVALID, "bad complex index");
+  const ComplexInfo &x = c->info[ci];
+  if (lig_conf < 0 || lig_conf >= x.n_lig)
+    return fail(GD_ERR_INVALID, "ligand conformer %d out of range [0, %d)", lig_conf, x.n_lig);
+  if (n < 0) return fail(GD_ERR_INVALID, "negative pose count");
+  if (n == 0) return GD_OK;
+  CK(cudaSetDevice(c->device));
+  const size_t out_bytes = sizeof(float) * 3 * (size_t)x.lna * n;
+  float *d_mm = nullptr, *d_xyz = nullptr;
+  CK(cudaStreamSynchronize(c->stream));
+  cudaError_t e = cudaMalloc(&d_mm, sizeof(float) * 6 * (size_t)n);
+  if (e == cudaSuccess) e = cudaMalloc(&d_xyz, out_bytes);
+  if (e == cudaSuccess) e = cudaMemcpy(d_mm, mm, sizeof(float) * 6 * (size_t)n,
+                                       cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    const long long total = (long long)n * x.lna;
+    gd_place_kernel<<<(unsigned)((total + 255) / 256), 256, 0, c->stream>>>(c->d_cx, ci, lig_conf,
+                                                                           d_mm, n, d_xyz);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e == cudaSuccess) e = cudaMemcpy(xyz, d_xyz, out_bytes, cudaMemcpyDeviceToHost);
+  cudaFree(d_mm);
+  cudaFree(d_xyz);
+  if (e != cudaSuccess) return fail(GD_ERR_CUDA, "gd_place_ligand: %s", cudaGetErrorString(e));
+  return GD_OK;
+}
+
 int gd_trace_enable(gd_ctx *c, int max_steps) {
   if (!c || max_steps < 0) return fail(GD_ERR_INVALID, "bad argument");
   CK(cudaStreamSynchronize(c->stream));

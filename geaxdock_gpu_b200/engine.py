@@ -68,6 +68,7 @@ def lib() -> C.CDLL:
         "gd_set_state": [vp, vp, C.c_int, C.c_int],
         "gd_get_device_error": [vp, ip],
         "gd_eval_energy": [vp, C.c_int, C.c_int, C.c_int, fp, C.c_int, vp],
+        "gd_place_ligand": [vp, C.c_int, C.c_int, fp, C.c_int, fp],
         "gd_trace_enable": [vp, C.c_int],
         "gd_trace_get": [vp, fp, ip, ip],
         "gd_get_stream": [vp, C.POINTER(vp)],
@@ -302,6 +303,15 @@ class Engine:
         out = np.zeros(mm.shape[0], abi.ENERGY_DTYPE)
         check(lib().gd_eval_energy(self.h, complex_index, prt_conf, lig_conf, abi.fptr(mm),
                                    mm.shape[0], _p(out)))
+        return out
+
+    def place_ligand(self, complex_index: int, lig_conf: int,
+                     movematrix: np.ndarray) -> np.ndarray:
+        """Placed ligand atoms of each pose, [n_poses, lna, 3] (PlaceLigand, src/util.C:457)."""
+        mm = np.ascontiguousarray(movematrix, np.float32).reshape(-1, 6)
+        out = np.zeros((mm.shape[0], self.complexes[complex_index].lna, 3), np.float32)
+        check(lib().gd_place_ligand(self.h, complex_index, lig_conf, abi.fptr(mm), mm.shape[0],
+                                    abi.fptr(out)))
         return out
 
     def trace_enable(self, max_steps: int):

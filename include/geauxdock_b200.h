@@ -305,6 +305,13 @@ int gd_eval_energy(gd_ctx *ctx, int complex_index, int prt_conf, int lig_conf,
 int gd_eval_energy_noalloc(gd_ctx *ctx, int complex_index, int prt_conf, int lig_conf,
                            const float *d_movematrix, int n_poses, gd_energy *d_out);
 
+/* Laboratory-frame ligand coordinates of n_poses poses (movematrix[6] each) of one ligand
+ * conformer: xyz[(pose * lna + atom) * 3 + {0, 1, 2}], placed on the device by the transform
+ * the Monte Carlo kernel applies. Replaces PlaceLigand (src/util.C:457-502) as the trace tool
+ * calls it (src/trace.C:104-105); n_poses = 0 is a no-op. */
+int gd_place_ligand(gd_ctx *ctx, int complex_index, int lig_conf, const float *movematrix,
+                    int n_poses, float *xyz);
+
 /* Per-step trace for bit-exact replay: when enabled, gd_mc_run logs for each replica and
  * step the proposal's total energy and the accept flag; trace[(r * max_steps) + s]. */
 int gd_trace_enable(gd_ctx *ctx, int max_steps);
