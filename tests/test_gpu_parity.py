@@ -389,3 +389,31 @@ def test_eval_energy_reproduces_reference_trajectory():
             dc = np.abs(got["cms"].astype(np.float64) - rows[sel, 8])
             assert de.max() <= 1e-5, (ip, il, int(de.argmax()), de.max())
             assert dc.max() <= 2e-6, (ip, il, int(dc.argmax()), dc.max())
+
+
+def test_eval_energy_soft_core_poses():
+    """Poses that put one ligand atom 0.4-1.9 A from a protein point, inside the soft core of
+    the electrostatic term (r < 1 / el1), where the kernel adds the near-field terms after
+    each segment's pair loop: every term within 1e-5 of the FP64 oracle."""
+    z, cx, ff = load_ref("1a07C1")
+    rm = z["ref_matrix"].astype(np.uint8)
+    rng = np.random.default_rng(12)
+    L, P = cx.lna, cx.pnp
+    mm = np.zeros((24, 6), np.float32)
+    for i in range(mm.shape[0]):
+        l, p = int(rng.integers(L)), int(rng.integers(P))
+        d = rng.normal(size=3)
+        d *= rng.uniform(0.4, 1.9) / np.linalg.norm(d)
+        orig = np.array([cx.lig_x[0, l], cx.lig_y[0, l], cx.lig_z[0, l]], np.float64)
+        target = np.array([cx.prt_x[0, p], cx.prt_y[0, p], cx.prt_z[0, p]], np.float64) + d
+        mm[i, :3] = target - orig - cx.lig_center[0]
+    near = 1.0 / ff.el1
+    for i in range(mm.shape[0]):
+        xyz, _ = po.place_f64(cx, 0, mm[i])
+        dmin = min(np.min((xyz[0][:, None] - cx.prt_x[0][None]) ** 2
+                          + (xyz[1][:, None] - cx.prt_y[0][None]) ** 2
+                          + (xyz[2][:, None] - cx.prt_z[0][None]) ** 2) ** 0.5, 9.0)
+        assert dmin < near, (i, dmin)
+    with engine.Engine(ff, [cx], abi.mc_params()) as eng:
+        worst = _energy_check(eng, ff, cx, 0, 0, 0, mm, rm)
+    assert worst.max() <= TOL, worst
