@@ -294,14 +294,15 @@ def delayed_acceptance(w, dev, tile, scale_mult, intervals, burn=2000, iters=166
         split_used = sur.split()
         fa, fb = a.state(), b.state()
         del flush
-    # null reference for the KS test: plain steps from the same start with another seed
+    # null reference for the KS test: plain steps from the same start with another seed, the
+    # same warm-up interval plus `intervals` intervals as the two arms
     p2 = type(p).from_buffer_copy(p)
     p2.seed = p.seed + 1
     with engine.Engine(ff, [cx], p2, device=dev) as c2:
         c2.set_tile(*tile)
         c2.mc_init()
         c2.set_state(start)
-        c2.run_fused(burn + spe, spe * intervals, exchange=True)
+        c2.run_fused(burn, spe * (intervals + 1), exchange=True)
         c2.sync()
         fc = c2.state()
     ea, eb = fa["energy_old"]["e"][:, 9], fb["energy_old"]["e"][:, 9]
@@ -322,7 +323,7 @@ def delayed_acceptance(w, dev, tile, scale_mult, intervals, burn=2000, iters=166
             "surrogate_rmse": st["rmse"], "target_mu_sigma": [info["mu"], info["sigma"]],
             "surrogate_active": st["active"],
             "ks_min_p": min(ks), "ks_p_per_temperature": ks,
-            "ks_null_min_p": min(ks_null),
+            "ks_null_min_p": min(ks_null), "ks_null_p_per_temperature": ks_null,
             "ks_note": "final states, 341 independent chains per temperature; ks_null: plain vs "
                        "plain with another seed from the same start (what equal distributions "
                        "give for the smallest of 20 p-values)",
@@ -659,6 +660,40 @@ def run_ours(args, rank, world, local_rank):
     print(json.dumps(out), flush=True)
 
 
+def da_ks_seeds(seeds, move_mult):
+    """The delayed-acceptance comparison of the config-3 workload repeated with several Philox
+    seeds: every per-temperature KS p-value of DA against plain (final states of the 341
+    independent chains per temperature), pooled, and the same for plain against plain with
+    another seed. Both arms of a comparison start from one state, and DA draws the plain
+    chain's moves and accept uniforms, so the arms are positively coupled and p-values lean
+    high; a difference between their distributions would instead make small p-values too
+    frequent, which the one-sided uniformity test (small_p_excess_ks_p) measures."""
+    from scipy import stats
+    pooled, null, rows = [], [], []
+    for sd in seeds:
+        w = workload(42)
+        w.params.seed = sd
+        r = delayed_acceptance(w, 0, (6, 1024, 2), move_mult, 100)
+        pooled += r["ks_p_per_temperature"]
+        null += r["ks_null_p_per_temperature"]
+        rows.append({"seed": sd, "ks_min_p": r["ks_min_p"], "ks_null_min_p": r["ks_null_min_p"],
+                     "speedup_vs_plain": r["speedup_vs_plain"],
+                     "stage1_pass": r["stage1_pass"]})
+    def summary(v):
+        v = np.asarray(v)
+        # "greater": the p-values' CDF lies above the uniform one, i.e. small p-values are
+        # too frequent, which a difference between the chains' distributions would cause
+        return {"p_values": len(v), "mean": float(v.mean()),
+                "frac_below_0.01": float((v < 0.01).mean()),
+                "frac_below_0.05": float((v < 0.05).mean()),
+                "uniformity_ks_p": float(stats.kstest(v, "uniform").pvalue),
+                "small_p_excess_ks_p": float(stats.kstest(v, "uniform",
+                                                          alternative="greater").pvalue),
+                "values": [round(float(x), 4) for x in v]}
+    return {"da_ks": {"move_mult": move_mult, "runs": rows, "da_vs_plain": summary(pooled),
+                      "plain_vs_plain": summary(null)}}
+
+
 def profile_da(args):
     from geaxdock_gpu_b200 import engine
     w = workload(42)
@@ -714,6 +749,9 @@ def main():
                     help="only a short delayed-acceptance sequence on the config-1 system (20 "
                          "collect steps, 20 Adam steps, 20 DA steps, 10 plain steps), for "
                          "profiler launch lists; prints its statistics")
+    ap.add_argument("--da-ks", default="",
+                    help="only the delayed-acceptance KS comparison at --move-mult, once per "
+                         "Philox seed of this comma-separated list, p-values pooled")
     ap.add_argument("--move-mult", type=float, default=1.0,
                     help="--profile-da / --screen-da: move scales multiplied by this factor")
     ap.add_argument("--profile-mc", action="store_true",
@@ -725,6 +763,10 @@ def main():
     args = ap.parse_args()
     if args.screen_da:
         print(json.dumps(screen_da(0, args.move_mult)), flush=True)
+        return
+    if args.da_ks:
+        print(json.dumps(da_ks_seeds([int(v) for v in args.da_ks.split(",")], args.move_mult)),
+              flush=True)
         return
     if args.profile_da:
         profile_da(args)
