@@ -170,87 +170,131 @@ struct gd_ctx {
   struct RecStream *rs = nullptr;
 };
 
-/* rows [start[r], start[r] + off[r+1] - off[r]) of every replica's records, packed at off[r] */
-__global__ void rs_gather_kernel(const gd_record_step *__restrict__ rec, int rec_cap,
-                                 const int *__restrict__ start, const int *__restrict__ off,
-                                 int n_rep, gd_record_step *__restrict__ out) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= n_rep) return;
-  const gd_record_step *src = rec + (size_t)r * rec_cap + start[r];
-  for (int i = 0, n = off[r + 1] - off[r]; i < n; ++i) out[off[r] + i] = src[i];
+/* Copy plan of one record-stream snapshot, one block: for every replica the rows written since
+ * the previous snapshot (counters in prev, clamped to the host array's cap) start at start[r]
+ * and go to off[r] of the packed buffer; off[n_rep] is the total. prev takes the new counters,
+ * cnt keeps them for the host. *overflow is set when the total exceeds the packed buffer's
+ * pack_rows (then nothing is gathered). */
+__global__ void rs_plan_kernel(const int *__restrict__ cur, int *__restrict__ prev, int n_rep,
+                               int cap, long long pack_rows, int *__restrict__ start,
+                               int *__restrict__ off, int *__restrict__ cnt, int *overflow) {
+  __shared__ int part[1024];
+  const int T = blockDim.x, t = threadIdx.x;
+  const int per = (n_rep + T - 1) / T, r0 = min(n_rep, t * per), r1 = min(n_rep, r0 + per);
+  int sum = 0;
+  for (int r = r0; r < r1; ++r)
+    sum += max(0, min(cur[r], cap) - min(prev[r], cap));
+  part[t] = sum;
+  __syncthreads();
+  for (int o = 1; o < T; o <<= 1) {
+    const int v = t >= o ? part[t - o] : 0;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  int base = t ? part[t - 1] : 0;
+  for (int r = r0; r < r1; ++r) {
+    const int c = cur[r], a = min(prev[r], cap);
+    start[r] = a;
+    off[r] = base;
+    base += max(0, min(c, cap) - a);
+    prev[r] = c;
+    cnt[r] = c;
+  }
+  if (t == T - 1) {
+    off[n_rep] = part[T - 1];
+    *overflow = (long long)part[T - 1] > pack_rows ? 1 : 0;
+  }
 }
 
-/* The worker of gd_records_stream. After each record-writing call the calling thread copies the
- * record counters into a snapshot slot on the context's stream and queues the slot; the worker
- * waits for the snapshot, packs every replica's records written since its previous snapshot
- * (records are appended only, so they are complete) with a small gather kernel on its own
- * stream, downloads the packed rows into a reused host staging buffer and copies them into the
- * caller's array, all while the context's stream runs the next work. */
+/* rows [start[r], start[r] + off[r+1] - off[r]) of every replica's records packed at off[r],
+ * one warp per replica copying 4-byte words */
+__global__ void rs_gather_kernel(const gd_record_step *__restrict__ rec, int rec_cap,
+                                 const int *__restrict__ start, const int *__restrict__ off,
+                                 int n_rep, long long pack_rows, gd_record_step *__restrict__ out) {
+  const int w = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (w >= n_rep || (long long)off[n_rep] > pack_rows) return;
+  constexpr int WORDS = sizeof(gd_record_step) / 4;
+  const uint32_t *src =
+      reinterpret_cast<const uint32_t *>(rec + (size_t)w * rec_cap + start[w]);
+  uint32_t *dst = reinterpret_cast<uint32_t *>(out + off[w]);
+  const int n = (off[w + 1] - off[w]) * WORDS;
+  for (int i = lane; i < n; i += 32) dst[i] = src[i];
+}
+
+/* The record stream of gd_records_stream. After each record-writing call the calling thread
+ * queues, on the context's stream, the copy plan and the gather of every replica's rows
+ * written since the previous snapshot into a packed device buffer of a free snapshot slot
+ * (records are appended only, so they are complete); stream order keeps the gather off the
+ * SMs while the Monte Carlo kernels run. A worker thread waits for the slot, downloads the plan
+ * and the packed rows into page-locked host memory on its own stream (a copy engine, no SMs)
+ * and copies them into the caller's array, while the context's stream runs the next work. */
 struct RecStream {
   static constexpr int NSNAP = 4;
   gd_record_step *host = nullptr;
   int cap = 0, n_rep = 0, rec_cap = 0, device = 0;
   const gd_record_step *d_rec = nullptr;
   cudaStream_t cs = nullptr;
-  int *d_snap[NSNAP] = {};
+  int *d_prev = nullptr;                           /* [n_rep] counters of the last snapshot */
+  int *d_plan[NSNAP] = {};                         /* start [n_rep], off [n_rep+1], cnt [n_rep],
+                                                      overflow [1] */
+  gd_record_step *d_pack[NSNAP] = {};
+  long long pack_rows[NSNAP] = {};
   cudaEvent_t ev[NSNAP] = {};
   bool busy[NSNAP] = {};
-  int *d_start = nullptr, *d_off = nullptr; /* [n_rep], [n_rep + 1] */
-  gd_record_step *d_pack = nullptr;
-  size_t pack_cap = 0;
+  int *h_plan = nullptr;                           /* page-locked copy of one slot's plan */
+  gd_record_step *h_stage = nullptr;               /* page-locked packed rows */
+  size_t stage_cap = 0;
   std::deque<int> queue;
   std::mutex mu;
   std::condition_variable cv;
   bool stop = false;
-  std::vector<int> prev; /* counters of the previous snapshot (0 after a restart) */
-  std::vector<int> snap; /* the latest snapshot copied */
+  std::vector<int> snap; /* the counters of the latest snapshot copied */
   cudaError_t err = cudaSuccess;
+  bool overflow = false;
   std::thread th;
 
-  cudaError_t one(const std::vector<int> &v, std::vector<int> &start, std::vector<int> &off,
-                  std::vector<gd_record_step> &stage) {
-    off[0] = 0;
-    for (int r = 0; r < n_rep; ++r) {
-      const int a = std::min(prev[r], cap), b = std::min(v[r], cap);
-      start[r] = a;
-      off[r + 1] = off[r] + std::max(0, b - a);
-    }
-    const size_t total = (size_t)off[n_rep];
-    if (total == 0) return cudaSuccess;
-    cudaError_t e = cudaSuccess;
-    if (total > pack_cap) {
-      if (d_pack) cudaFree(d_pack);
-      d_pack = nullptr;
-      pack_cap = 0;
-      e = cudaMalloc(&d_pack, total * sizeof(gd_record_step));
-      if (e != cudaSuccess) return e;
-      pack_cap = total;
-    }
-    if (stage.size() < total) stage.resize(total);
-    e = cudaMemcpyAsync(d_start, start.data(), sizeof(int) * n_rep, cudaMemcpyHostToDevice, cs);
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(d_off, off.data(), sizeof(int) * (n_rep + 1), cudaMemcpyHostToDevice,
-                          cs);
-    if (e != cudaSuccess) return e;
-    rs_gather_kernel<<<(n_rep + 127) / 128, 128, 0, cs>>>(d_rec, rec_cap, d_start, d_off, n_rep,
-                                                          d_pack);
-    e = cudaGetLastError();
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(stage.data(), d_pack, total * sizeof(gd_record_step),
-                          cudaMemcpyDeviceToHost, cs);
+  size_t plan_ints() const { return 3 * (size_t)n_rep + 2; }
+
+  /* downloads slot k's rows into the caller's array */
+  cudaError_t one(int k) {
+    int *start = h_plan, *off = h_plan + n_rep, *cnt = off + n_rep + 1, *ovf = cnt + n_rep;
+    cudaError_t e = cudaMemcpyAsync(h_plan, d_plan[k], sizeof(int) * plan_ints(),
+                                    cudaMemcpyDeviceToHost, cs);
     if (e == cudaSuccess) e = cudaStreamSynchronize(cs);
     if (e != cudaSuccess) return e;
-    for (int r = 0; r < n_rep; ++r)
-      if (off[r + 1] > off[r])
-        memcpy(host + (size_t)r * cap + start[r], stage.data() + off[r],
-               sizeof(gd_record_step) * (size_t)(off[r + 1] - off[r]));
+    if (*ovf) {
+      overflow = true;
+      return cudaSuccess;
+    }
+    const size_t total = (size_t)off[n_rep];
+    if (total > 0) {
+      if (total > stage_cap) {
+        if (h_stage) cudaFreeHost(h_stage);
+        h_stage = nullptr;
+        stage_cap = 0;
+        const size_t want = total + total / 4;
+        e = cudaHostAlloc(&h_stage, want * sizeof(gd_record_step), cudaHostAllocDefault);
+        if (e != cudaSuccess) return e;
+        stage_cap = want;
+      }
+      e = cudaMemcpyAsync(h_stage, d_pack[k], total * sizeof(gd_record_step),
+                          cudaMemcpyDeviceToHost, cs);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(cs);
+      if (e != cudaSuccess) return e;
+      for (int r = 0; r < n_rep; ++r)
+        if (off[r + 1] > off[r])
+          memcpy(host + (size_t)r * cap + start[r], h_stage + off[r],
+                 sizeof(gd_record_step) * (size_t)(off[r + 1] - off[r]));
+    }
+    std::lock_guard<std::mutex> lk(mu);
+    snap.assign(cnt, cnt + n_rep);
     return cudaSuccess;
   }
 
   void worker() {
     cudaSetDevice(device);
-    std::vector<int> v(n_rep), start(n_rep), off(n_rep + 1);
-    std::vector<gd_record_step> stage;
     for (;;) {
       int k;
       {
@@ -260,18 +304,10 @@ struct RecStream {
         k = queue.front();
       }
       cudaError_t e = cudaEventSynchronize(ev[k]);
-      if (e == cudaSuccess)
-        e = cudaMemcpyAsync(v.data(), d_snap[k], sizeof(int) * n_rep, cudaMemcpyDeviceToHost, cs);
-      if (e == cudaSuccess) e = cudaStreamSynchronize(cs);
-      if (e == cudaSuccess) e = one(v, start, off, stage);
+      if (e == cudaSuccess) e = one(k);
       {
         std::lock_guard<std::mutex> lk(mu);
-        if (e == cudaSuccess) {
-          prev = v;
-          snap = v;
-        } else if (err == cudaSuccess) {
-          err = e;
-        }
+        if (e != cudaSuccess && err == cudaSuccess) err = e;
         queue.pop_front();
         busy[k] = false;
       }
@@ -310,28 +346,50 @@ cudaError_t d2h_rows(void *dst, size_t hpitch, const void *src, size_t dpitch, s
   return cudaMemcpy2D(dst, hpitch, src, dpitch, width, n, cudaMemcpyDeviceToHost);
 }
 
-/* queues a snapshot of the record counters taken after the work queued on the context's
- * stream so far (no-op without gd_records_stream) */
-int rs_enqueue(gd_ctx *c) {
+/* queues a snapshot taken after the work queued on the context's stream so far: the copy plan
+ * and the gather of the rows written since the previous snapshot, at most rows_per_rep per
+ * replica (the steps of the call that wrote them). No-op without gd_records_stream. */
+int rs_enqueue(gd_ctx *c, int rows_per_rep) {
   RecStream *r = c->rs;
   if (!r) return GD_OK;
   int k = -1;
   {
     std::unique_lock<std::mutex> lk(r->mu);
     r->cv.wait(lk, [&] {
-      if (r->err != cudaSuccess) return true;
+      if (r->err != cudaSuccess || r->overflow) return true;
       for (int i = 0; i < RecStream::NSNAP; ++i)
         if (!r->busy[i]) return true;
       return false;
     });
     if (r->err != cudaSuccess)
       return fail(GD_ERR_CUDA, "record stream: %s", cudaGetErrorString(r->err));
+    if (r->overflow) return fail(GD_ERR_STATE, "record stream: more rows than the writing calls queued");
     for (int i = 0; i < RecStream::NSNAP && k < 0; ++i)
       if (!r->busy[i]) k = i;
     r->busy[k] = true;
   }
-  cudaError_t e = cudaMemcpyAsync(r->d_snap[k], c->d_rec_next, sizeof(int) * c->n_rep,
-                                  cudaMemcpyDeviceToDevice, c->stream);
+  const long long need = (long long)r->n_rep * std::min(r->cap, std::max(0, rows_per_rep));
+  cudaError_t e = cudaSuccess;
+  if (need > r->pack_rows[k]) {
+    /* the slot is idle: no copy reads its buffer */
+    if (r->d_pack[k]) cudaFree(r->d_pack[k]);
+    r->d_pack[k] = nullptr;
+    r->pack_rows[k] = 0;
+    e = cudaMalloc(&r->d_pack[k], (size_t)need * sizeof(gd_record_step));
+    if (e == cudaSuccess) r->pack_rows[k] = need;
+  }
+  int *plan = r->d_plan[k], n = r->n_rep;
+  if (e == cudaSuccess) {
+    rs_plan_kernel<<<1, 1024, 0, c->stream>>>(c->d_rec_next, r->d_prev, n, r->cap,
+                                              r->pack_rows[k], plan, plan + n, plan + 2 * n + 1,
+                                              plan + 3 * n + 1);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess && r->pack_rows[k] > 0) {
+    rs_gather_kernel<<<(unsigned)((n + 7) / 8), 256, 0, c->stream>>>(
+        r->d_rec, r->rec_cap, plan, plan + n, n, r->pack_rows[k], r->d_pack[k]);
+    e = cudaGetLastError();
+  }
   if (e == cudaSuccess) e = cudaEventRecord(r->ev[k], c->stream);
   {
     std::lock_guard<std::mutex> lk(r->mu);
@@ -345,25 +403,25 @@ int rs_enqueue(gd_ctx *c) {
   return GD_OK;
 }
 
-/* one more snapshot after everything queued, then wait for every copy: the host buffer then
- * mirrors the device records */
+/* one more snapshot after everything queued (every record-writing call has queued its own, so
+ * it finds no new rows), then wait for every copy: the host array mirrors the device records */
 int rs_flush(gd_ctx *c) {
   RecStream *r = c->rs;
   if (!r) return GD_OK;
-  int rc = rs_enqueue(c);
+  int rc = rs_enqueue(c, 0);
   if (rc) return rc;
   std::unique_lock<std::mutex> lk(r->mu);
   r->cv.wait(lk, [&] { return r->queue.empty(); });
   if (r->err != cudaSuccess)
     return fail(GD_ERR_CUDA, "record stream: %s", cudaGetErrorString(r->err));
+  if (r->overflow) return fail(GD_ERR_STATE, "record stream: more rows than the writing calls queued");
   return GD_OK;
 }
 
 /* after a flush, before the counters restart: the next copies start from record 0 */
 void rs_restart(gd_ctx *c) {
   if (!c->rs) return;
-  std::lock_guard<std::mutex> lk(c->rs->mu);
-  std::fill(c->rs->prev.begin(), c->rs->prev.end(), 0);
+  cudaMemsetAsync(c->rs->d_prev, 0, sizeof(int) * (size_t)c->rs->n_rep, c->stream);
 }
 
 /* stops the worker after the queued copies and frees the stream's resources */
@@ -377,12 +435,13 @@ void rs_stop(gd_ctx *c) {
   r->cv.notify_all();
   if (r->th.joinable()) r->th.join();
   for (int i = 0; i < RecStream::NSNAP; ++i) {
-    if (r->d_snap[i]) cudaFree(r->d_snap[i]);
+    if (r->d_plan[i]) cudaFree(r->d_plan[i]);
+    if (r->d_pack[i]) cudaFree(r->d_pack[i]);
     if (r->ev[i]) cudaEventDestroy(r->ev[i]);
   }
-  if (r->d_start) cudaFree(r->d_start);
-  if (r->d_off) cudaFree(r->d_off);
-  if (r->d_pack) cudaFree(r->d_pack);
+  if (r->d_prev) cudaFree(r->d_prev);
+  if (r->h_plan) cudaFreeHost(r->h_plan);
+  if (r->h_stage) cudaFreeHost(r->h_stage);
   if (r->cs) cudaStreamDestroy(r->cs);
   delete r;
   c->rs = nullptr;
@@ -1398,7 +1457,7 @@ int gd_mc_init(gd_ctx *c) {
   if (rc) return rc;
   c->initialized = true;
   c->exchange_calls = 0;
-  return rs_enqueue(c);
+  return rs_enqueue(c, 1);
 }
 
 int gd_reset_records(gd_ctx *c, int r0, int r1) {
@@ -1426,7 +1485,7 @@ int gd_mc_run(gd_ctx *c, int r0, int r1, int s1, int s2) {
   a.n_steps = c->mc.steps_per_exchange;
   a.step0 = s1 + s2;
   if ((rc = launch_mc(c, a, c->d_tiles, n, c->d_counters))) return rc;
-  return rs_enqueue(c);
+  return rs_enqueue(c, c->mc.steps_per_exchange);
 }
 
 int gd_exchange(gd_ctx *c, int mode_l, int mode_t) {
@@ -1502,7 +1561,7 @@ int gd_mc_run_fused(gd_ctx *c, int s1, int n_steps, int exchange) {
                      c->stream));
   CK(cudaGraphLaunch(it->second, c->stream));
   if (exchange) c->exchange_calls += chunks;
-  return rs_enqueue(c);
+  return rs_enqueue(c, n_steps);
 }
 
 int gd_sync(gd_ctx *c) {
@@ -1582,12 +1641,12 @@ int gd_records_stream(gd_ctx *c, gd_record_step *steps, int cap) {
   r->device = c->device;
   r->d_rec = c->d_rec;
   r->snap.assign(c->n_rep, 0);
-  r->prev.assign(c->n_rep, 0);
   cudaError_t e = cudaStreamCreateWithFlags(&r->cs, cudaStreamNonBlocking);
-  if (e == cudaSuccess) e = cudaMalloc(&r->d_start, sizeof(int) * (size_t)c->n_rep);
-  if (e == cudaSuccess) e = cudaMalloc(&r->d_off, sizeof(int) * ((size_t)c->n_rep + 1));
+  if (e == cudaSuccess) e = cudaMalloc(&r->d_prev, sizeof(int) * (size_t)c->n_rep);
+  if (e == cudaSuccess) e = cudaMemsetAsync(r->d_prev, 0, sizeof(int) * (size_t)c->n_rep, c->stream);
+  if (e == cudaSuccess) e = cudaHostAlloc(&r->h_plan, sizeof(int) * r->plan_ints(), 0);
   for (int i = 0; i < RecStream::NSNAP && e == cudaSuccess; ++i) {
-    e = cudaMalloc(&r->d_snap[i], sizeof(int) * (size_t)c->n_rep);
+    e = cudaMalloc(&r->d_plan[i], sizeof(int) * r->plan_ints());
     if (e == cudaSuccess)
       e = cudaEventCreateWithFlags(&r->ev[i], cudaEventDisableTiming | cudaEventBlockingSync);
   }
@@ -1596,8 +1655,19 @@ int gd_records_stream(gd_ctx *c, gd_record_step *steps, int cap) {
     rs_stop(c);
     return fail(GD_ERR_CUDA, "gd_records_stream: %s", cudaGetErrorString(e));
   }
+  /* the first snapshot copies the rows written before the stream started */
+  std::vector<int> cnt(c->n_rep);
+  e = cudaStreamSynchronize(c->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(cnt.data(), c->d_rec_next, sizeof(int) * cnt.size(), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) {
+    rs_stop(c);
+    return fail(GD_ERR_CUDA, "gd_records_stream: %s", cudaGetErrorString(e));
+  }
+  int rows = 0;
+  for (int v : cnt) rows = std::max(rows, std::min(v, cap));
   r->th = std::thread([r] { r->worker(); });
-  return rs_enqueue(c);
+  return rs_enqueue(c, rows);
 }
 
 int gd_records_stream_flush(gd_ctx *c, int *next_ptr) {
@@ -2573,7 +2643,7 @@ int gd_sur_collect(gd_ctx *c, int s1, int n_steps, int exchange) {
   if (rc) return rc;
   if (d->smp_hi != g0) d->smp_lo = g0; /* not contiguous with the earlier samples */
   d->smp_hi = g0 + (long long)n_steps * c->n_rep;
-  return rs_enqueue(c);
+  return rs_enqueue(c, n_steps);
 }
 
 int gd_sur_train(gd_ctx *c, int iterations, float *losses) {
@@ -2623,7 +2693,7 @@ int gd_sur_train(gd_ctx *c, int iterations, float *losses) {
 int gd_da_run(gd_ctx *c, int s1, int n_steps, int exchange) {
   int rc = da_run_steps(c, s1, n_steps, exchange, false);
   if (rc) return rc;
-  if ((rc = rs_enqueue(c))) return rc;
+  if ((rc = rs_enqueue(c, n_steps))) return rc;
   DaState *d = c->da;
   const bool controller = d->prm.fallback_accept > 0.0f;
   if (!controller && d->prm.split > 0) return GD_OK;

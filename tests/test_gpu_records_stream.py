@@ -77,3 +77,25 @@ def test_stream_delayed_acceptance_collect(cx_ff):
         sur.train(5)
         sur.run(40, 40, exchange=True)
         _same(e, *e.stream_flush())
+
+
+def test_stream_started_mid_window(cx_ff):
+    """A stream started after records exist copies those rows with its first snapshot, then
+    the rows of every later call; a second stream on the same context restarts from row 0."""
+    cx, ff = cx_ff
+    params = abi.mc_params(steps_per_exchange=10, steps_per_dump=200, seed=6)
+    with engine.Engine(ff, [cx], params) as e:
+        e.mc_init()
+        for it in range(3):
+            e.mc_run(0, it * 10)
+        buf = e.stream_records(201)
+        for it in range(3, 6):
+            e.mc_run(0, it * 10)
+        b, nxt = e.stream_flush()
+        assert b is buf and nxt.max() > 30
+        _same(e, buf, nxt)
+        buf2 = e.stream_records(201)
+        e.run_fused(60, 20, exchange=True)
+        b2, nxt2 = e.stream_flush()
+        assert b2 is buf2
+        _same(e, buf2, nxt2)
