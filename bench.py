@@ -666,6 +666,29 @@ def run_ours(args, rank, world, local_rank):
     print(json.dumps(out), flush=True)
 
 
+def profile_aux(args):
+    """The small kernels around the Monte Carlo kernel, on a 128-replica subset of the config-1
+    system: a record stream over four 10-step intervals (copy plan + gather per interval), the
+    exchange after each, and the placement of 4,096 poses (gd_place_ligand)."""
+    from geaxdock_gpu_b200 import engine
+    w = workload(42)
+    cx = w.complexes[0].subset(n_lig=8, n_prt=2, n_tmp=8)
+    params = w.params
+    with engine.Engine(w.ff, [cx], params) as e:
+        e.set_tile(6, 1024, 2)
+        e.mc_init()
+        e.stream_records(64)
+        for it in range(4):
+            e.mc_run(0, it * params.steps_per_exchange)
+            e.exchange(int(not (it % 2)))
+        steps, nxt = e.stream_flush()
+        mm = np.random.default_rng(1).normal(0, 1, (4096, 6)).astype(np.float32)
+        xyz = e.place_ligand(0, 0, mm)
+        e.stream_stop()
+    print(json.dumps({"profile_aux": {"replicas": cx.n_rep, "records": int(nxt.sum()),
+                                      "poses": int(xyz.shape[0])}}), flush=True)
+
+
 def da_ks_seeds(seeds, move_mult):
     """The delayed-acceptance comparison of the config-3 workload repeated with several Philox
     seeds: every per-temperature KS p-value of DA against plain (final states of the 341
@@ -755,6 +778,9 @@ def main():
                     help="only a short delayed-acceptance sequence on the config-1 system (20 "
                          "collect steps, 20 Adam steps, 20 DA steps, 10 plain steps), for "
                          "profiler launch lists; prints its statistics")
+    ap.add_argument("--profile-aux", action="store_true",
+                    help="only the record-stream, exchange and placement kernels on a small "
+                         "case, for profiler captures")
     ap.add_argument("--da-ks", default="",
                     help="only the delayed-acceptance KS comparison at --move-mult, once per "
                          "Philox seed of this comma-separated list, p-values pooled")
@@ -769,6 +795,9 @@ def main():
     args = ap.parse_args()
     if args.screen_da:
         print(json.dumps(screen_da(0, args.move_mult)), flush=True)
+        return
+    if args.profile_aux:
+        profile_aux(args)
         return
     if args.da_ks:
         print(json.dumps(da_ks_seeds([int(v) for v in args.da_ks.split(",")], args.move_mult)),
