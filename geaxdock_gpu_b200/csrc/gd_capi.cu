@@ -257,17 +257,16 @@ struct RecStream {
 
   size_t plan_ints() const { return 3 * (size_t)n_rep + 2; }
 
-  /* downloads slot k's rows into the caller's array */
-  cudaError_t one(int k) {
-    int *start = h_plan, *off = h_plan + n_rep, *cnt = off + n_rep + 1, *ovf = cnt + n_rep;
+  /* downloads slot k's rows into the caller's array; *ovf: the slot's rows exceeded its
+   * packed buffer and nothing was gathered */
+  cudaError_t one(int k, bool *ovf) {
+    int *start = h_plan, *off = h_plan + n_rep, *cnt = off + n_rep + 1;
     cudaError_t e = cudaMemcpyAsync(h_plan, d_plan[k], sizeof(int) * plan_ints(),
                                     cudaMemcpyDeviceToHost, cs);
     if (e == cudaSuccess) e = cudaStreamSynchronize(cs);
     if (e != cudaSuccess) return e;
-    if (*ovf) {
-      overflow = true;
-      return cudaSuccess;
-    }
+    *ovf = cnt[n_rep] != 0;
+    if (*ovf) return cudaSuccess;
     const size_t total = (size_t)off[n_rep];
     if (total > 0) {
       if (total > stage_cap) {
@@ -303,11 +302,13 @@ struct RecStream {
         if (queue.empty()) return;
         k = queue.front();
       }
+      bool ovf = false;
       cudaError_t e = cudaEventSynchronize(ev[k]);
-      if (e == cudaSuccess) e = one(k);
+      if (e == cudaSuccess) e = one(k, &ovf);
       {
         std::lock_guard<std::mutex> lk(mu);
         if (e != cudaSuccess && err == cudaSuccess) err = e;
+        if (ovf) overflow = true;
         queue.pop_front();
         busy[k] = false;
       }
@@ -419,9 +420,10 @@ int rs_flush(gd_ctx *c) {
 }
 
 /* after a flush, before the counters restart: the next copies start from record 0 */
-void rs_restart(gd_ctx *c) {
-  if (!c->rs) return;
-  cudaMemsetAsync(c->rs->d_prev, 0, sizeof(int) * (size_t)c->rs->n_rep, c->stream);
+int rs_restart(gd_ctx *c) {
+  if (!c->rs) return GD_OK;
+  CK(cudaMemsetAsync(c->rs->d_prev, 0, sizeof(int) * (size_t)c->rs->n_rep, c->stream));
+  return GD_OK;
 }
 
 /* stops the worker after the queued copies and frees the stream's resources */
@@ -1452,7 +1454,7 @@ int gd_mc_init(gd_ctx *c) {
   CK(cudaMemsetAsync(c->d_acs, 0, sizeof(int) * c->n_rep, c->stream));
   CK(cudaMemsetAsync(c->d_err, 0, sizeof(unsigned), c->stream));
   if ((rc = rs_flush(c))) return rc;
-  rs_restart(c);
+  if ((rc = rs_restart(c))) return rc;
   rc = launch_mc(c, a, c->d_tiles, n, c->d_counters);
   if (rc) return rc;
   c->initialized = true;
@@ -1466,7 +1468,7 @@ int gd_reset_records(gd_ctx *c, int r0, int r1) {
   if (rc) return rc;
   const int n = r1 - r0 + 1;
   if ((rc = rs_flush(c))) return rc;
-  rs_restart(c);
+  if ((rc = rs_restart(c))) return rc;
   gd::gd_reset_records_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(c->d_rec_next, r0, r1);
   CK(cudaGetLastError());
   return GD_OK;
