@@ -564,32 +564,6 @@ def run_ours(args, rank, world, local_rank):
     eng.close()
     del flush
 
-    if rank != 0:
-        return
-    mc_avg_ms = sum(mc_ms) / len(mc_ms)
-    flops_launch = flops_rs * rs_per_step
-    achieved = flops_launch / (mc_avg_ms * 1e-3) / 1e12
-    peak = None
-    try:
-        import ctypes as C
-        v = C.c_double()
-        if engine.lib().gd_probe_fp32_peak(dev, 5, C.byref(v)) == 0:
-            peak = v.value
-    except Exception:
-        peak = None
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "gd_mc_kernel_config1_traffic.json")
-    if os.path.exists(tpath):
-        try:
-            traffic = json.load(open(tpath)).get("bytes_per_launch")
-        except Exception:
-            traffic = None
-    roofline = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": (achieved / peak) if peak else None, "traffic": traffic,
-                "kernel": "gd_mc_kernel", "launch_ms": mc_avg_ms,
-                "flop_per_replica_step": flops_rs,
-                "peak_source": "measured FP32 FMA probe (gd_probe_fp32_peak), same run"}
-
     # ---------------- end to end through the C ABI (host buffers) ----------------
     e2e = None
     if not args.no_e2e:
@@ -601,6 +575,8 @@ def run_ours(args, rank, world, local_rank):
                      "mcs_z", "mcs_tcc", "temp"):
             h2d += getattr(cx, name).nbytes
         h2d += C.sizeof(abi.EnePara)
+        if dist:
+            dist.barrier()
         t0 = time.perf_counter()
         e = engine.Engine(ff, [cx], params, device=dev)
         e.set_tile(*tile_used)
@@ -627,12 +603,42 @@ def run_ours(args, rank, world, local_rank):
         d2h += download()
         e.close()
         dt = time.perf_counter() - t0
-        e2e = {"value": rs_per_step * args.steps / dt, "unit": UNIT,
+        if dist:
+            from geaxdock_gpu_b200.shard import max_over_ranks
+            dt = max_over_ranks(dt, dist)
+        e2e = {"value": world * rs_per_step * args.steps / dt, "unit": UNIT,
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                "scope": "gd_create + gd_mc_init + K x (gd_mc_run + gd_exchange + "
                         "gd_get_etotal) + the filled record rows of every dump window "
                         "(gd_get_record_counts + gd_get_records_raw, as the reference's launcher "
-                        "downloads LigRecord per dump) + gd_destroy, host wall clock"}
+                        "downloads LigRecord per dump) + gd_destroy, host wall clock, every rank "
+                        "its own shard, slowest rank"}
+
+    if rank != 0:
+        return
+    mc_avg_ms = sum(mc_ms) / len(mc_ms)
+    flops_launch = flops_rs * rs_per_step
+    achieved = flops_launch / (mc_avg_ms * 1e-3) / 1e12
+    peak = None
+    try:
+        import ctypes as C
+        v = C.c_double()
+        if engine.lib().gd_probe_fp32_peak(dev, 5, C.byref(v)) == 0:
+            peak = v.value
+    except Exception:
+        peak = None
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "gd_mc_kernel_config1_traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get("bytes_per_launch")
+        except Exception:
+            traffic = None
+    roofline = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": (achieved / peak) if peak else None, "traffic": traffic,
+                "kernel": "gd_mc_kernel", "launch_ms": mc_avg_ms,
+                "flop_per_replica_step": flops_rs,
+                "peak_source": "measured FP32 FMA probe (gd_probe_fp32_peak), same run"}
 
     da = None
     if world == 1 and not args.no_da:
