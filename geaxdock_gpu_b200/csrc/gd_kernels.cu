@@ -103,8 +103,8 @@ __device__ __forceinline__ float dist2(float ax, float ay, float az, float px, f
 
 struct Acc {
   float2 vdw, ele, pmf, hdb, hsum;
+  float2 ncon; /* contact counts (exact small integers) */
   float psp;
-  int ncon;
 };
 
 /* Per-segment pair parameters, splatted over the two lanes of an FP32x2 register pair. */
@@ -160,12 +160,12 @@ __device__ __forceinline__ void pair_body(const float4 A, const float4 B,
    * Its maximum over r is log2(e) (12 - pmf0)^2 / 8 < 100 for pmf0 > -10 (checked when the
    * force field is loaded), so den stays finite and p4 den does wherever p4 does. */
   const float2 tt = __ffma2_rn(q.b2, r, __ffma2_rn(f2(-0.5f * LOG2E_F), d2, q.c2));
-  const float2 den = __fadd2_rn(one, make_float2(ex2_a(tt.x), ex2_a(tt.y)));
-  /* one reciprocal for both quotients: num / p4 = num den / (p4 den),
-   * pmf1 / den = pmf1 p4 / (p4 den) */
-  const float2 pd = __fmul2_rn(p4, den);
+  const float2 ee = make_float2(ex2_a(tt.x), ex2_a(tt.y));
+  /* one reciprocal for both quotients, den = 1 + ee: num / p4 = num den / (p4 den),
+   * pmf1 / den = pmf1 p4 / (p4 den), with p4 den = p4 + p4 ee and num den = num + num ee */
+  const float2 pd = __ffma2_rn(p4, ee, p4);
   const float2 inv = make_float2(rcp_a(pd.x), rcp_a(pd.y));
-  const float2 vn = __fmul2_rn(num, den);
+  const float2 vn = __ffma2_rn(num, ee, num);
   const float2 pn = __fmul2_rn(q.pmf1, p4);
   if constexpr (PAIR) {
     a.vdw = __ffma2_rn(vn, inv, a.vdw);
@@ -174,9 +174,13 @@ __device__ __forceinline__ void pair_body(const float4 A, const float4 B,
     a.vdw.x = __fmaf_rn(vn.x, inv.x, a.vdw.x);
     a.pmf.x = __fmaf_rn(pn.x, inv.x, a.pmf.x);
   }
-  /* contacts (mcc, psp): sqrtf(d2) <= pmf0  <=>  d2 <= thr */
+  /* contacts (mcc, psp): sqrtf(d2) <= pmf0  <=>  d2 <= thr, counted as 1.0 / 0.0 */
   const bool c0 = d2.x <= q.thr, c1 = PAIR && d2.y <= q.thr;
-  a.ncon += (int)c0 + (int)c1;
+  if constexpr (PAIR) {
+    a.ncon = __fadd2_rn(a.ncon, make_float2(c0 ? 1.0f : 0.0f, c1 ? 1.0f : 0.0f));
+  } else {
+    a.ncon.x += c0 ? 1.0f : 0.0f;
+  }
   if (KIND & 2) {
     const float4 X = PX[m];
     if (c0) a.psp += __ldg(psprow + __float_as_int(X.z));
@@ -526,7 +530,7 @@ __global__ void __launch_bounds__(GD_MAX_TPB, GD_MIN_BLOCKS(UNROLL))
             pq.pmf1 = f2(q1.y); pq.hc1 = f2(q1.z); pq.hc0 = f2(q1.w);
             pq.hs = f2(q2.x); pq.b2 = f2(q2.z); pq.c2 = f2(q2.w);
             const float2 z2 = f2(0.0f);
-            Acc acc = {z2, z2, z2, z2, z2, 0.0f, 0};
+            Acc acc = {z2, z2, z2, z2, z2, z2, 0.0f};
             pair_dispatch<UNROLL>(g.w, PA, PB, PX, i0, i1, ax, ay, az, pq, psprow, f, acc);
             part[0 * T + tid] += (double)acc.vdw.x + (double)acc.vdw.y;
             part[1 * T + tid] += (double)acc.ele.x + (double)acc.ele.y;
@@ -534,7 +538,7 @@ __global__ void __launch_bounds__(GD_MAX_TPB, GD_MIN_BLOCKS(UNROLL))
             part[3 * T + tid] += (double)acc.psp;
             part[4 * T + tid] += (double)acc.hdb.x + (double)acc.hdb.y;
             part[5 * T + tid] += (double)acc.hsum.x + (double)acc.hsum.y;
-            ncon += acc.ncon;
+            ncon += (int)(acc.ncon.x + acc.ncon.y);
           }
         }
         if (!resident) {
