@@ -419,10 +419,11 @@ int rs_flush(gd_ctx *c) {
   return GD_OK;
 }
 
-/* after a flush, before the counters restart: the next copies start from record 0 */
-int rs_restart(gd_ctx *c) {
+/* after a flush, before the counters of replicas [r0, r1] restart: their next copies start
+ * from record 0 */
+int rs_restart(gd_ctx *c, int r0, int r1) {
   if (!c->rs) return GD_OK;
-  CK(cudaMemsetAsync(c->rs->d_prev, 0, sizeof(int) * (size_t)c->rs->n_rep, c->stream));
+  CK(cudaMemsetAsync(c->rs->d_prev + r0, 0, sizeof(int) * (size_t)(r1 - r0 + 1), c->stream));
   return GD_OK;
 }
 
@@ -1454,7 +1455,7 @@ int gd_mc_init(gd_ctx *c) {
   CK(cudaMemsetAsync(c->d_acs, 0, sizeof(int) * c->n_rep, c->stream));
   CK(cudaMemsetAsync(c->d_err, 0, sizeof(unsigned), c->stream));
   if ((rc = rs_flush(c))) return rc;
-  if ((rc = rs_restart(c))) return rc;
+  if ((rc = rs_restart(c, 0, c->n_rep - 1))) return rc;
   rc = launch_mc(c, a, c->d_tiles, n, c->d_counters);
   if (rc) return rc;
   c->initialized = true;
@@ -1468,7 +1469,7 @@ int gd_reset_records(gd_ctx *c, int r0, int r1) {
   if (rc) return rc;
   const int n = r1 - r0 + 1;
   if ((rc = rs_flush(c))) return rc;
-  if ((rc = rs_restart(c))) return rc;
+  if ((rc = rs_restart(c, r0, r1))) return rc;
   gd::gd_reset_records_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(c->d_rec_next, r0, r1);
   CK(cudaGetLastError());
   return GD_OK;

@@ -99,3 +99,22 @@ def test_stream_started_mid_window(cx_ff):
         b2, nxt2 = e.stream_flush()
         assert b2 is buf2
         _same(e, buf2, nxt2)
+
+
+def test_stream_partial_reset(cx_ff):
+    """Resetting the records of some replicas restarts only their copies: the host array
+    still equals the device records afterwards."""
+    cx, ff = cx_ff
+    params = abi.mc_params(steps_per_exchange=10, steps_per_dump=200, seed=7)
+    with engine.Engine(ff, [cx], params) as e:
+        e.mc_init()
+        buf = e.stream_records(201)
+        for it in range(3):
+            e.mc_run(0, it * 10)
+        half = e.n_rep // 2
+        e.reset_records(0, half - 1)
+        for it in range(3, 5):
+            e.mc_run(0, it * 10)
+        b, nxt = e.stream_flush()
+        assert b is buf and nxt[:half].max() <= 20 < nxt[half:].max()
+        _same(e, buf, nxt)
