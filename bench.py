@@ -10,7 +10,8 @@ synthetic data. One bench step = one exchange interval: 10 MC steps of every rep
 ours:      device time from CUDA events recorded on the library's own stream around each
            step, L2 flushed between steps (outside the events), max over ranks; `e2e` is a
            whole run through the C ABI from host buffers (gd_create uploads, init, K steps,
-           record download) timed on the host; `cpu_baseline` is the reference's own step code
+           record download per dump window) timed on the host, on every rank (the slowest
+           rank's time); `cpu_baseline` is the reference's own step code
            on the host cores (as the reference arm) on a bounded sample (rank 0, N = 1).
 reference: the reference's own MonteCarlo_d step functions (Move_d, CalcEnergy_d, CalcMcc_d,
            Accept_d, RecordLigand_d) compiled for the CPU from its sources (oracle/_ref/refpin),
