@@ -226,6 +226,21 @@ class Protein:
         return self.x.shape[0]
 
 
+def load_weights(path: str) -> np.ndarray:
+    """loadWeight (src/load.C:1762-1794): one term weight per line, the number at the start of
+    its first 30 characters (0 where there is none)."""
+    out = []
+    for line in _lines(path):
+        tok = line[:30].split()
+        v = np.float32(0.0)
+        if tok:
+            m = re.match(r"[+-]?(\d+\.?\d*|\.\d+)([eE][+-]?\d+)?", tok[0])
+            if m:
+                v = np.float32(float(m.group(0)))
+        out.append(v)
+    return np.asarray(out, F32)
+
+
 def _pdb_points(lines: Sequence[str]):
     """The point list of the first model (src/load.C:965-1060)."""
     r, t, d, c, seq3 = [], [], [], [], []
@@ -355,16 +370,63 @@ def _sdf_sections(lines: Sequence[str]) -> List[List[str]]:
     return secs
 
 
-def _tag_value(sect: Sequence[str], key: str, start: int) -> Optional[str]:
-    val = None
-    for i in range(start, len(sect)):
-        if key in sect[i] and i + 1 < len(sect):
-            val = sect[i + 1]
-    return val
+def sdf_records(path: str) -> List[List[str]]:
+    """readLigandSections (src/load.C:428-446): the file's records, each the lines up to and
+    including its `$$$$`."""
+    return _sdf_sections(_lines(path))
 
 
-def _centre(x: np.ndarray, y: np.ndarray, z: np.ndarray):
-    """moveLigand2ItsCenterFrame (src/load.C:232-253): float sums, float means, subtract."""
+def ligand_header(sect: Sequence[str]) -> Tuple[int, int]:
+    """writeLigProperty's counts (src/load.C:388-426): atoms and bonds from the counts line."""
+    if len(sect) < 4:
+        raise LoadError("truncated SDF header")
+    return c_atoi(sect[3][0:3]), c_atoi(sect[3][3:6])
+
+
+def atom_block(sect: Sequence[str], lna: int):
+    """writeDefaultLigAtomCoord (src/load.C:302-320): the atom block's coordinates as read
+    (columns 1-30)."""
+    if lna < 1 or 4 + lna > len(sect):
+        raise LoadError("bad atom count %d" % lna)
+    return (np.asarray([_f(sect[4 + i][0:10]) for i in range(lna)], F32),
+            np.asarray([_f(sect[4 + i][10:20]) for i in range(lna)], F32),
+            np.asarray([_f(sect[4 + i][20:30]) for i in range(lna)], F32))
+
+
+def ensemble(sect: Sequence[str]) -> Tuple[List[float], List[str]]:
+    """getLigEnsembleRmsd / getLigEnsembleCoords (src/load.C:108-156): the ENSEMBLE_RMSD values
+    (the lines after the tag while they start with a digit) and the ENSEMBLE_COORDS rows (the
+    lines after the tag up to an empty one)."""
+    rmsds: List[float] = []
+    coords: List[str] = []
+    for i, line in enumerate(sect):
+        if "ENSEMBLE_RMSD" in line:
+            j = i + 1
+            while j < len(sect) and sect[j][:1].isdigit():
+                rmsds += [c_atof(tok) for tok in sect[j].split()]
+                j += 1
+        if "ENSEMBLE_COORDS" in line:
+            j = i + 1
+            while j < len(sect) and sect[j] != "":
+                coords.append(sect[j])
+                j += 1
+    return rmsds, coords
+
+
+def ensemble_coords(row: str, lna: int):
+    """writeEnsAtomCoord (src/load.C:284-300): one ENSEMBLE_COORDS row as x y z triples
+    (missing atoms at 0)."""
+    v = [_f(tok) for tok in row.split()]
+    if len(v) % 3:
+        raise LoadError("an ENSEMBLE_COORDS row is not x y z triples")
+    xs = np.zeros(lna, F32); ys = np.zeros(lna, F32); zs = np.zeros(lna, F32)
+    for k in range(min(len(v) // 3, lna)):
+        xs[k], ys[k], zs[k] = v[3 * k], v[3 * k + 1], v[3 * k + 2]
+    return xs, ys, zs
+
+
+def centre(x: np.ndarray, y: np.ndarray, z: np.ndarray):
+    """moveLigand2ItsCenterFrame (src/load.C:239-260): float sums, float means, subtract."""
     lna = x.shape[0]
     sx = sy = sz = F32(0.0)
     for i in range(lna):
@@ -374,20 +436,61 @@ def _centre(x: np.ndarray, y: np.ndarray, z: np.ndarray):
             np.asarray([F32(v - cz) for v in z], F32))
 
 
+def ensemble_total(sect: Sequence[str]) -> int:
+    """getLigEnsembleTotal (src/load.C:262-279): the integer on the line after the last
+    ENSEMBLE_TOTAL tag (a record without one is an error, where the reference exits)."""
+    tot = -1
+    for i, line in enumerate(sect):
+        if "ENSEMBLE_TOTAL" in line:
+            tot = c_atoi(sect[i + 1] if i + 1 < len(sect) else "")
+    if tot == -1:
+        raise LoadError("no ENSEMBLE_TOTAL")
+    return tot
+
+
+def pocket_center(path: str) -> np.ndarray:
+    """loadPocketCenter (src/load.C:1326-1343): x y z of the last line holding CENTER."""
+    center_line = None
+    for line in _lines(path):
+        if "CENTER" in line:
+            center_line = line
+    if center_line is None:
+        raise LoadError("%s: no CENTER line" % path)
+    tok = center_line.split()
+    if len(tok) < 4:
+        raise LoadError("%s: CENTER line with fewer than three values" % path)
+    return np.asarray([_f(tok[1]), _f(tok[2]), _f(tok[3])], F32)
+
+
+def ligand_conformers(sect: Sequence[str], lna: int) -> List[Tuple[np.ndarray, ...]]:
+    """loadOneLigand's conformers as read, before centring (src/load.C:200-227): the atom
+    block, then every ENSEMBLE_COORDS row whose ENSEMBLE_RMSD is above 0.1 A."""
+    confs = [atom_block(sect, lna)]
+    rmsds, coords = ensemble(sect)
+    if len(rmsds) != len(coords):
+        raise LoadError("%d ENSEMBLE_RMSD values for %d ENSEMBLE_COORDS rows" %
+                        (len(rmsds), len(coords)))
+    for rm, row in zip(rmsds, coords):
+        # rmsd values are compared as floats against the double threshold
+        if float(F32(rm)) > MINLIGRMSD:
+            confs.append(ensemble_coords(row, lna))
+    return confs
+
+
 def load_ligand(path: str) -> Ligand:
     """loadLigand / loadOneLigand (src/load.C:157-230): the first SDF record; conformer 0 is
     the atom block, the others are the ENSEMBLE_COORDS rows whose ENSEMBLE_RMSD is above
     0.1 A; every conformer is centred on its own centroid."""
-    secs = _sdf_sections(_lines(path))
+    secs = sdf_records(path)
     if not secs:
         raise LoadError("%s: no SDF record ($$$$)" % path)
     sect = secs[0]
-    if len(sect) < 4:
-        raise LoadError("%s: truncated SDF header" % path)
-    lna = c_atoi(sect[3][0:3])
-    lnb = c_atoi(sect[3][3:6])
-    if lna < 1 or 4 + lna > len(sect):
-        raise LoadError("%s: bad atom count %d" % (path, lna))
+    try:
+        lna, lnb = ligand_header(sect)
+        if lna < 1 or 4 + lna > len(sect):
+            raise LoadError("bad atom count %d" % lna)
+    except LoadError as ex:
+        raise LoadError("%s: %s" % (path, ex))
     start = 4 + lna + lnb
     types: List[int] = []
     charges: List[np.float32] = []
@@ -406,38 +509,11 @@ def load_ligand(path: str) -> Ligand:
     if len(types) < lna or len(charges) < lna:
         raise LoadError("%s: OB_ATOM_TYPES / OB_ATOMIC_CHARGES shorter than %d atoms" %
                         (path, lna))
-    x0 = np.asarray([_f(sect[4 + i][0:10]) for i in range(lna)], F32)
-    y0 = np.asarray([_f(sect[4 + i][10:20]) for i in range(lna)], F32)
-    z0 = np.asarray([_f(sect[4 + i][20:30]) for i in range(lna)], F32)
-    confs = [(x0, y0, z0)]
-    # ENSEMBLE_RMSD: the following lines while they start with a digit
-    rmsds: List[float] = []
-    coords: List[str] = []
-    for i, line in enumerate(sect):
-        if "ENSEMBLE_RMSD" in line:
-            j = i + 1
-            while j < len(sect) and sect[j][:1].isdigit():
-                rmsds += [c_atof(tok) for tok in sect[j].split()]
-                j += 1
-        if "ENSEMBLE_COORDS" in line:
-            j = i + 1
-            while j < len(sect) and sect[j] != "":
-                coords.append(sect[j])
-                j += 1
-    if len(rmsds) != len(coords):
-        raise LoadError("%s: %d ENSEMBLE_RMSD values for %d ENSEMBLE_COORDS rows" %
-                        (path, len(rmsds), len(coords)))
-    for rm, row in zip(rmsds, coords):
-        # rmsd values are compared as floats against the double threshold
-        if float(F32(rm)) > MINLIGRMSD:
-            v = [_f(tok) for tok in row.split()]
-            if len(v) % 3:
-                raise LoadError("%s: an ENSEMBLE_COORDS row is not x y z triples" % path)
-            xs = np.zeros(lna, F32); ys = np.zeros(lna, F32); zs = np.zeros(lna, F32)
-            for k in range(min(len(v) // 3, lna)):
-                xs[k], ys[k], zs[k] = v[3 * k], v[3 * k + 1], v[3 * k + 2]
-            confs.append((xs, ys, zs))
-    cx = [_centre(*cf) for cf in confs]
+    try:
+        confs = ligand_conformers(sect, lna)
+    except LoadError as ex:
+        raise LoadError("%s: %s" % (path, ex))
+    cx = [centre(*cf) for cf in confs]
     return Ligand(t=np.asarray(types[:lna], np.int32), c=np.asarray(charges[:lna], F32),
                   n=np.arange(lna, dtype=np.int32),
                   x=np.stack([a for a, _, _ in cx]), y=np.stack([b for _, b, _ in cx]),

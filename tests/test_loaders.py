@@ -3,6 +3,9 @@
 * On the reference's own input files (when its tree is present), every array of the complex
   and the raw and folded energy parameters equal, bit for bit, the fixtures that the
   reference's loaders and folds produced (tests/golden/make_golden.py, via oracle/refpin).
+* The reference's own loader tests (src/load_test.C), restated on the same files: record and
+  ensemble counts, atom/bond counts, coordinates as read and after centring, the pocket
+  centre, the weight file against the parameter file.
 * On small files written here, the parsing rules the reference applies: ensemble conformers
   kept only above 0.1 A RMSD and centred on their own centroid, effective points of each
   residue, one conformation per ENDMDL/TER block, both MCS line formats, unknown ligand types,
@@ -201,3 +204,91 @@ def test_unknown_residue_is_an_error(tmp_path):
     atoms = _residue("ALA", 1, 0.0, []) + [("CA", "XYZ", 2, 5.0, 0.0, 0.0)]
     with pytest.raises(loaders.LoadError):
         loaders.load_protein(_pdb(tmp_path, [atoms]))
+
+
+# ------------------------------------------------------------------------------------------
+# the reference's own loader tests (src/load_test.C), restated on the same files
+
+
+def _data(*parts):
+    p = os.path.join(DATA, *parts)
+    if not os.path.exists(p):
+        pytest.skip("the reference's input files are not present")
+    return p
+
+
+def _almost(want, got, ulps=4):
+    """gtest's FloatingPoint<float>::AlmostEquals: within 4 units in the last place."""
+    a, b = np.float32(want), np.float32(got)
+
+    def key(v):
+        i = int(np.array(v, np.float32).view(np.int32))
+        return i if i >= 0 else -(i & 0x7FFFFFFF)
+    return abs(key(a) - key(b)) <= ulps
+
+
+def test_load_test_weights():
+    """loadWeight/parameters (src/load_test.C:15-30): the term weights of the parameter file
+    and of the separate weight file agree within 1e-4."""
+    w = loaders.load_weights(_data("parameters", "08ff_opt"))
+    raw = loaders.load_enepara(_data("parameters", "paras"))
+    assert w.shape[0] == 9
+    for i in range(w.shape[0]):
+        assert abs(float(raw.w[i]) - float(w[i])) < 1e-4, i
+
+
+def test_load_test_ligand_1a07C1():
+    """Load_Ligands/1a07C1 (src/load_test.C:71-111): one record whose ENSEMBLE_TOTAL matches
+    its coordinate rows and RMSD values, 21 conformers after the RMSD filter, conformer 0 atom
+    0 x = 45.6740, conformer 2 atom 0 y = -5.2246 (as read)."""
+    secs = loaders.sdf_records(_data("1a07C1", "1a07C1.sdf"))
+    assert len(secs) == 1
+    total = loaders.ensemble_total(secs[0])
+    rmsds, rows = loaders.ensemble(secs[0])
+    assert len(rows) == total and len(rmsds) == total
+    lna, _ = loaders.ligand_header(secs[0])
+    confs = loaders.ligand_conformers(secs[0], lna)
+    assert len(confs) == 21
+    assert _almost(45.6740, confs[0][0][0])
+    assert _almost(-5.2246, confs[2][1][0])
+    assert loaders.load_ligand(_data("1a07C1", "1a07C1.sdf")).n_conf == 21
+
+
+def test_load_test_ligands_1b9v():
+    """Load_Ligands/1b9vA (src/load_test.C:113-180): six records, 50 ensemble conformers with
+    50 RMSD values, 23 atoms and 23 bonds; atom 1 x of the atom block -0.0184, of ensemble row
+    0 2.1011, atom 1 z of row 2 -2.2202; atom 0 x after centring -3.6306739; pocket centre
+    y -9.590."""
+    secs = loaders.sdf_records(_data("edud", "1b9v_4.sdf"))
+    assert len(secs) == 6
+    sect = secs[0]
+    assert loaders.ensemble_total(sect) == 50
+    rmsds, rows = loaders.ensemble(sect)
+    assert len(rows) == 50 and len(rmsds) == 50
+    lna, lnb = loaders.ligand_header(sect)
+    assert (lna, lnb) == (23, 23)
+    x, y, z = loaders.atom_block(sect, lna)
+    assert _almost(-0.0184, x[1])
+    assert _almost(2.1011, loaders.ensemble_coords(rows[0], lna)[0][1])
+    assert _almost(-2.2202, loaders.ensemble_coords(rows[2], lna)[2][1])
+    assert _almost(-3.6306739, loaders.centre(x, y, z)[0][0])
+    assert _almost(-9.590, loaders.pocket_center(_data("edud", "1b9v_4.ff"))[1])
+
+
+def test_load_test_ligands_1e66():
+    """Load_Ligands/1e66 (src/load_test.C:183-213): six records, 50 ensemble conformers,
+    28 atoms and 31 bonds."""
+    secs = loaders.sdf_records(_data("edud", "1e66_4.sdf"))
+    assert len(secs) == 6
+    assert loaders.ensemble_total(secs[0]) == 50
+    rmsds, rows = loaders.ensemble(secs[0])
+    assert len(rmsds) == len(rows) == 50
+    assert loaders.ligand_header(secs[0]) == (28, 31)
+
+
+def test_load_test_10gs():
+    """Load_Ligands/10gsA00 and Load_Protein/10gsA00 (src/load_test.C:216-239): the ligand
+    file loads; the protein has one conformation."""
+    loaders.load_ligand(_data("10gs", "10gs_ligand.sdf"))
+    loaders.pocket_center(_data("10gs", "10gsA00.ff"))
+    assert loaders.load_protein(_data("10gs", "10gsA00.pdb")).n_conf == 1
