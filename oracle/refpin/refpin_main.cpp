@@ -259,8 +259,41 @@ static int bench_main(int argc, char **argv) {
   return 0;
 }
 
+/* the reference's k-means module (src/kmeans.h:68,71) */
+extern "C" float **seq_kmeans(float **, int, int, int, float, int *, int *);
+extern "C" float **file_read(int, char *, int *, int *);
+
+/* --kmeans file --k N --out f.gdfx: the run of cluster_test (src/cluster_test.C:23-66) --
+ * the reference's file_read of a text data file (an id, then the coordinates, per line) and
+ * its seq_kmeans with threshold 0.001 -- written as objects, membership, centres, loops. */
+static int kmeans_main(int argc, char **argv) {
+  char path[4096];
+  snprintf(path, sizeof(path), "%s", arg(argc, argv, "--kmeans", ""));
+  const int k = atoi(arg(argc, argv, "--k", "10"));
+  int n = 0, d = 0;
+  float **obj = file_read(0, path, &n, &d);
+  if (!obj || n < k || k < 1) { fprintf(stderr, "cannot read %s\n", path); return 2; }
+  std::vector<float> objects(obj[0], obj[0] + (size_t)n * d);
+  std::vector<int> mem(n);
+  int loops = 0;
+  float **cen = seq_kmeans(obj, d, n, k, 0.001f, mem.data(), &loops);
+  {
+    Writer w(arg(argc, argv, "--out", "kmeans.gdfx"));
+    w.put("objects", 'f', {(uint64_t)n, (uint64_t)d}, objects.data(), 4);
+    w.put("membership", 'i', {(uint64_t)n}, mem.data(), 4);
+    w.put("centres", 'f', {(uint64_t)k, (uint64_t)d}, cen[0], 4);
+    w.put("loops", 'i', {1}, &loops, 4);
+  }
+  free(obj[0]);
+  free(obj);
+  free(cen[0]);
+  free(cen);
+  return 0;
+}
+
 int main(int argc, char **argv) {
   if (strcmp(arg(argc, argv, "--bench", ""), "")) return bench_main(argc, argv);
+  if (strcmp(arg(argc, argv, "--kmeans", ""), "")) return kmeans_main(argc, argv);
   InputFiles in = InputFiles();
   in.prt_file.path = arg(argc, argv, "--pdb", "");
   in.lig_file.path = arg(argc, argv, "--sdf", "");

@@ -1,8 +1,9 @@
 """Generate the golden fixtures under tests/golden/ from the reference's own code.
 
-Builds oracle/_ref/refpin (the reference's loaders, host folds and kernel source compiled for
-the CPU; see oracle/refpin/) and runs it on the reference's real complexes. Each run writes a
-.gdfx container that this script converts to a compressed .npz:
+Builds oracle/_ref/refpin (the reference's loaders, host folds, kernel source and k-means
+module compiled for the CPU; see oracle/refpin/) and runs it on the reference's real complexes
+and on the k-means module's sample data. Each run writes a .gdfx container that this script
+converts to a compressed .npz:
 
   python tests/golden/make_golden.py [--reference /path/to/geaxdock_gpu]
 
@@ -45,6 +46,12 @@ def read_gdfx(path):
     return out
 
 
+# cluster_test's run (src/cluster_test.C:23-66) on the vendored k-means module's text data:
+# name -> (data file under src/modules/kmeans-master/Image_data, clusters)
+KMEANS = {"edge100": ("edge100.txt", 10), "color100": ("color100.txt", 10),
+          "texture100": ("texture100.txt", 10)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
@@ -64,6 +71,17 @@ def main():
         dst = os.path.join(HERE, "ref_%s.npz" % name)
         np.savez_compressed(dst, **arrs)
         print(name, os.path.getsize(dst), "bytes", file=sys.stderr)
+    km = {}
+    for name, (fname, k) in KMEANS.items():
+        tmp = os.path.join(REPO, "oracle", "_ref", "kmeans_%s.gdfx" % name)
+        src = os.path.join(a.reference, "src", "modules", "kmeans-master", "Image_data", fname)
+        subprocess.run([binp, "--kmeans", src, "--k", str(k), "--out", tmp], check=True,
+                       stdout=subprocess.DEVNULL)
+        for key, v in read_gdfx(tmp).items():
+            km["%s_%s" % (name, key)] = v
+    dst = os.path.join(HERE, "kmeans_ref.npz")
+    np.savez_compressed(dst, **km)
+    print("kmeans", os.path.getsize(dst), "bytes", file=sys.stderr)
 
 
 if __name__ == "__main__":

@@ -94,3 +94,22 @@ def test_post_mc_edge_cases():
     assert got_r.tobytes() == want_r.tobytes() and np.array_equal(got_z, want_z)
     e_r, e_z = postmc.post_mc([np.zeros(0, abi.RECORD_DTYPE)] * 3, seed=4)
     assert e_r.shape == (0,) and e_z.shape == (0,)
+
+
+def test_gpu_kmeans_is_the_references_seq_kmeans():
+    """The library's k-means on the reference's own k-means run (src/seq_kmeans.c on the
+    k-means module's 9-coordinate sample, 10 clusters, threshold 0.001; fixture from
+    tests/golden/make_golden.py), the objects laid out so that the seeded shuffle restores the
+    file's order: the reference's membership, cluster sizes and pass count."""
+    import os
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "kmeans_ref.npz"))
+    obj, ref = z["color100_objects"], z["color100_membership"]
+    n = obj.shape[0]
+    for seed in (0, 5):
+        perm = postmc.permutation(seed, 0, n)
+        objp = np.empty_like(obj)
+        objp[perm] = obj
+        mem, med, size, passes, base = postmc.kmeans(objp, [0, n], [10], seed)
+        assert np.array_equal(mem[perm], ref)
+        assert size.tolist() == np.bincount(ref, minlength=10).tolist()
+        assert int(passes[0]) == int(z["color100_loops"][0])

@@ -76,3 +76,37 @@ def test_write_states_format(tmp_path):
                         "vdw ele pmf psp hdb hpc kde lhm edst ener")
     f = lines[1].split(" ")
     assert f[:4] == ["3", "1", "0.5000", "1.2346"] and len(f) == 20 and f[-1] == "4.0000"
+
+
+def _kmeans_ref():
+    import os
+    return np.load(os.path.join(os.path.dirname(__file__), "golden", "kmeans_ref.npz"))
+
+
+@pytest.mark.parametrize("name", ["edge100", "color100", "texture100"])
+def test_oracle_seq_kmeans_is_the_references(name):
+    """The oracle's seq_kmeans against the reference's own (src/seq_kmeans.c, run as
+    src/cluster_test.C:23-66 runs it: 10 clusters, threshold 0.001, on the k-means module's
+    sample data; fixtures from tests/golden/make_golden.py): the same membership, the same
+    centres bit for bit, the same number of passes."""
+    z = _kmeans_ref()
+    obj, cen = z[name + "_objects"], z[name + "_centres"]
+    mem, c, passes = ok.seq_kmeans(obj, cen.shape[0], 0.001)
+    assert np.array_equal(np.asarray(mem), z[name + "_membership"])
+    assert np.array_equal(np.asarray(c, np.float32).view(np.uint32), cen.view(np.uint32))
+    assert passes == int(z[name + "_loops"][0])
+
+
+@pytest.mark.parametrize("seed", [0, 5, 2 ** 33 + 1])
+def test_oracle_shuffled_kmeans_reproduces_the_reference_order(seed):
+    """Objects laid out so that the seeded shuffle puts them back in the file's order give
+    clusterByKmeans the reference's seq_kmeans run on that order (membership and sizes)."""
+    z = _kmeans_ref()
+    obj, ref = z["color100_objects"], z["color100_membership"]
+    perm = ok.permutation(seed, 0, obj.shape[0])
+    objp = np.empty_like(obj)
+    objp[perm] = obj
+    mem, _, size, passes = ok.cluster_by_kmeans(objp, 10, seed, 0)
+    assert np.array_equal(np.asarray(mem)[perm], ref)
+    assert np.asarray(size).tolist() == np.bincount(ref, minlength=10).tolist()
+    assert passes == int(z["color100_loops"][0])
