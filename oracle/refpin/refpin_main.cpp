@@ -19,6 +19,7 @@
 #include <cstdint>
 #include <cstring>
 #include <ctime>
+#include <list>
 #include <map>
 #include <string>
 #include <vector>
@@ -357,6 +358,32 @@ int main(int argc, char **argv) {
   xp.num_temp = nt;
   SetTemperature(temp, &xp);
   SetReplica(replica, lig, cs);
+
+  /* --trace rows.txt: the trace program's loop (src/trace.C:90-122) -- the rows of a
+   * trajectory file as its read2D reads them (src/load.C:80-105), each placed by PlaceLigand
+   * (conformer int(row[1]), move vector row[2..7]) and written by replaceLigandCoords
+   * (src/util.C:457-545) -- every row's SDF text into `out`, each after a line ">>>> row k". */
+  const char *trace_rows = arg(argc, argv, "--trace", "");
+  if (trace_rows[0]) {
+    TraceFile tf;
+    tf.path = trace_rows;
+    std::vector<std::vector<float> > rows = read2D(&tf);
+    FILE *fo = fopen(out, "w");
+    if (!fo) { perror(out); return 2; }
+    int k = 0;
+    for (auto &row : rows) {
+      if (row.size() < 8 || (int)row[1] < 0 || (int)row[1] >= cs.n_lig) break;
+      float mv[6];
+      for (int i = 0; i < 6; ++i) mv[i] = row[2 + i];
+      Ligand *my = &lig[(int)row[1]];
+      PlaceLigand(my, mv);
+      std::list<std::string> sdf = replaceLigandCoords(&in.lig_file, my);
+      fprintf(fo, ">>>> row %d\n", k++);
+      for (auto &line : sdf) fprintf(fo, "%s\n", line.c_str());
+    }
+    fclose(fo);
+    return 0;
+  }
 
   Writer w(out);
   {

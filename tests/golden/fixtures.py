@@ -28,3 +28,10 @@ def load_trajectory():
     """The reference's sample trajectory of 1a07C1 (see make_trajectory.py): float64 rows of
     PrtIdx, LigIdx, the six move-vector entries, cms and the weighted total energy."""
     return np.load(os.path.join(HERE, "trajectory_1a07C1.npz"))["rows"]
+
+
+def load_trajectory_trace():
+    """(rows, picked row indices, placed atoms [picked, lna, 3] in A) of the reference's trace
+    program on every 13th trajectory row (see make_trajectory.py)."""
+    z = np.load(os.path.join(HERE, "trajectory_1a07C1.npz"))
+    return z["rows"], z["trace_rows"], z["trace_xyz"].astype(np.float64) * 1e-4

@@ -69,3 +69,17 @@ def test_trace_tool_writes_the_placed_ligands(tmp_path, capsys):
                                                           np.float32(r[2:8])))
         got = (tmp_path / ("pose_%d.sdf" % k)).read_text()
         assert got == "\n".join(want) + "\n", k
+
+
+def test_place_ligand_is_the_reference_trace():
+    """The library's placement against the reference's trace program on every 13th row of its
+    sample trajectory (fixture from tests/golden/make_trajectory.py): every atom within the SDF
+    lines' printed precision (5e-5 rounding, 1.5e-4 allowed)."""
+    from tests.golden.fixtures import load_trajectory_trace
+    rows, pick, ref = load_trajectory_trace()
+    z, cx, ff = load_ref("1a07C1")
+    with engine.Engine(ff, [cx], abi.mc_params()) as e:
+        for lc in np.unique(rows[pick, 1]).astype(int):
+            sel = np.nonzero(rows[pick, 1] == lc)[0]
+            got = e.place_ligand(0, int(lc), rows[pick[sel], 2:8].astype(np.float32))
+            assert np.max(np.abs(got.astype(np.float64) - ref[sel])) <= 1.5e-4, lc

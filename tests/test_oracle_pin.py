@@ -242,3 +242,19 @@ def test_oracle_reproduces_reference_trajectory():
         dc[i] = abs(o["cms"] - r[8])
     assert de.max() <= TRAJ_E_TOL, (int(de.argmax()), de.max())
     assert dc.max() <= TRAJ_CMS_TOL, (int(dc.argmax()), dc.max())
+
+
+def test_oracle_placement_is_the_reference_trace():
+    """The reference's trace program (read2D, PlaceLigand, replaceLigandCoords; src/trace.C:90-122,
+    run by tests/golden/make_trajectory.py through oracle/_ref/refpin on every 13th row of
+    data/trajectory.out): the oracle places every atom of those rows within the SDF lines'
+    printed precision (5e-5 rounding, 1.1e-4 allowed) in FP64 and in FP32."""
+    from tests.golden.fixtures import load_trajectory_trace
+    rows, pick, ref = load_trajectory_trace()
+    z, cx, ff = load_ref("1a07C1")
+    assert ref.shape == (pick.shape[0], cx.lna, 3)
+    for k, i in enumerate(pick):
+        lc, mm = int(rows[i, 1]), rows[i, 2:8].astype(np.float32)
+        for place in (po.place_f64, po.place_f32):
+            xyz, _ = place(cx, lc, mm)
+            assert np.max(np.abs(np.asarray(xyz, np.float64).T - ref[k])) <= 1.1e-4, (k, place)
