@@ -292,9 +292,25 @@ static int kmeans_main(int argc, char **argv) {
   return 0;
 }
 
+/* --states records.bin --out table.txt: the reference's printStates (src/util.C:1504-1545) on
+ * the LigRecordSingleStep array of a raw file (the product's gd_record_step layout). */
+static int states_main(int argc, char **argv) {
+  const char *in = arg(argc, argv, "--states", "");
+  FILE *f = fopen(in, "rb");
+  if (!f) { perror(in); return 2; }
+  std::vector<LigRecordSingleStep> steps;
+  LigRecordSingleStep s;
+  while (fread(&s, sizeof(s), 1, f) == 1) steps.push_back(s);
+  fclose(f);
+  std::string out = arg(argc, argv, "--out", "states.txt");
+  printStates(steps, out);
+  return 0;
+}
+
 int main(int argc, char **argv) {
   if (strcmp(arg(argc, argv, "--bench", ""), "")) return bench_main(argc, argv);
   if (strcmp(arg(argc, argv, "--kmeans", ""), "")) return kmeans_main(argc, argv);
+  if (strcmp(arg(argc, argv, "--states", ""), "")) return states_main(argc, argv);
   InputFiles in = InputFiles();
   in.prt_file.path = arg(argc, argv, "--pdb", "");
   in.lig_file.path = arg(argc, argv, "--sdf", "");

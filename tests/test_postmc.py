@@ -110,3 +110,15 @@ def test_oracle_shuffled_kmeans_reproduces_the_reference_order(seed):
     assert np.array_equal(np.asarray(mem)[perm], ref)
     assert np.asarray(size).tolist() == np.bincount(ref, minlength=10).tolist()
     assert passes == int(z["color100_loops"][0])
+
+
+def test_write_states_is_the_references_print_states(tmp_path):
+    """The trajectory table against the reference's own printStates (src/util.C:1504-1545) on
+    300 records with signed zeros, values rounding to zero from below and rounding ties
+    (fixture from tests/golden/make_states.py): byte for byte."""
+    import os
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "states_ref.npz"))
+    rec = np.frombuffer(z["records"].tobytes(), abi.RECORD_DTYPE)
+    p = tmp_path / "states.csv"
+    postmc.write_states(rec, str(p))
+    assert p.read_bytes() == z["table"].tobytes()
