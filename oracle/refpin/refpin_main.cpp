@@ -16,6 +16,7 @@
  */
 #include "refpin_shim.h"
 
+#include <cstddef>
 #include <cstdint>
 #include <cstring>
 #include <ctime>
@@ -39,6 +40,24 @@ static_assert(sizeof(Energy) == sizeof(gd_energy), "Energy layout");
 static_assert(sizeof(LigRecordSingleStep) == sizeof(gd_record_step), "record layout");
 static_assert(sizeof(LigRecord) == sizeof(gd_lig_record), "LigRecord layout");
 static_assert(sizeof(Temp) == sizeof(gd_temp), "Temp layout");
+/* field by field: the record structs that the reference's dumps and readers use */
+#define GD_SAME_OFFSET(R, G, f) static_assert(offsetof(R, f) == offsetof(G, f), #R "." #f)
+GD_SAME_OFFSET(Replica, gd_replica, idx_rep);
+GD_SAME_OFFSET(Replica, gd_replica, idx_prt);
+GD_SAME_OFFSET(Replica, gd_replica, idx_tmp);
+GD_SAME_OFFSET(Replica, gd_replica, idx_lig);
+GD_SAME_OFFSET(Energy, gd_energy, e);
+GD_SAME_OFFSET(Energy, gd_energy, cms);
+GD_SAME_OFFSET(Energy, gd_energy, rmsd);
+GD_SAME_OFFSET(LigRecordSingleStep, gd_record_step, replica);
+GD_SAME_OFFSET(LigRecordSingleStep, gd_record_step, energy);
+GD_SAME_OFFSET(LigRecordSingleStep, gd_record_step, movematrix);
+GD_SAME_OFFSET(LigRecordSingleStep, gd_record_step, step);
+GD_SAME_OFFSET(LigRecord, gd_lig_record, step);
+GD_SAME_OFFSET(LigRecord, gd_lig_record, next_ptr);
+static_assert(sizeof(((LigRecord *)0)->step) == sizeof(((gd_lig_record *)0)->step),
+              "LigRecord steps per dump");
+#undef GD_SAME_OFFSET
 
 /* ---------------- named-array container ---------------- */
 struct Writer {
