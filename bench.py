@@ -52,9 +52,27 @@ def load_raw():
     return abi.enepara_raw_from_array(z["enepara_raw"])
 
 
-def workload(seed):
+def workload(seed, fold=None):
     from geaxdock_gpu_b200 import system
-    return system.config(1, load_raw(), seed=seed)
+    return system.config(1, load_raw(), seed=seed, fold=fold)
+
+
+def bench_config(world):
+    """The workload object both arms print (the same system, moves and step at every N)."""
+    return {"workload": "config1: P=3000 x 11 conf, L=40 x 31 conf, T=20, 6820 replicas per "
+                        "GPU, gaussian moves 0.1 A / 0.05 rad, exchange/10",
+            "step": "10 MC steps of every replica + 1 exchange",
+            "l2": "flushed between steps (256 MB write)",
+            "parallelism": "replica shards, no collective" if world > 1 else "1 GPU"}
+
+
+def product_library_mapped():
+    """True when this process has the product's CUDA library mapped (Linux /proc maps)."""
+    try:
+        with open("/proc/self/maps") as f:
+            return any("libgeauxdock_b200" in ln for ln in f)
+    except OSError:
+        return False
 
 
 class ClockSampler:
@@ -168,11 +186,14 @@ def cpu_baseline_sample(w, seconds=12.0, nthreads=0):
 def run_reference(args, rank, world):
     """The reference arm: the reference's own MonteCarlo_d step code on the host cores
     (oracle/_ref/refpin, one process per core; the oracle's FP32 OpenMP port when that build is
-    absent), each bench step a bounded replica sample x 10 MC steps of the config-1 system."""
+    absent), each bench step a bounded replica sample x 10 MC steps of the config-1 system with
+    the configured Gaussian moves. The force field is folded by the oracle's OptimizeEnepara
+    restatement (bit-identical to the reference's and the library's folds), so this process
+    never loads the product's library; it checks that before printing."""
     if rank != 0:
         return
     from oracle import pyoracle as po, refbench
-    w = workload(42)
+    w = workload(42, fold=po.fold_enepara)
     cx, ff, params = w.complexes[0], w.ff, w.params
     params.record = 0
     nt = po.max_threads()
@@ -210,20 +231,21 @@ def run_reference(args, rank, world):
     tot = sum(times)
     value = done / tot
     kind = "reference" if use_ref else "port"
-    sample = ("%d replicas x 10 MC steps per bench step through the reference's MonteCarlo_d step "
-              "functions compiled for the CPU (oracle/_ref/refpin), one process per core" % n_rep
+    sample = ("%d of 6820 replicas x 10 MC steps (configured Gaussian moves) per bench step "
+              "through the reference's MonteCarlo_d step functions compiled for the CPU "
+              "(oracle/_ref/refpin), one process per core; the exchange (< 0.2 %% of a step) "
+              "not timed" % n_rep
               if use_ref else "%d of 6820 replicas x 10 MC steps per bench step (oracle FP32 "
               "OpenMP port)" % n_rep)
+    if product_library_mapped():
+        raise RuntimeError("the reference arm loaded the product's library")
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
            "data": "synthetic (seeded, config-1 shapes)", "impl": "reference",
-           "config": {"workload": "config1: P=3000 x 11 conf, L=40 x 31 conf, T=20, 6820 "
-                                  "replicas (reference: its own uniform moves; the exchange, "
-                                  "< 0.2 % of a step, not timed)",
-                      "replicas_sampled": n_rep},
+           "config": bench_config(world),
            "cpu_baseline": {"value": value, "unit": UNIT, "cores": nt, "kind": kind,
-                            "sample": sample},
+                            "sample": sample, "replicas_sampled": n_rep},
            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
@@ -659,14 +681,10 @@ def run_ours(args, rank, world, local_rank):
            "warmup": args.warmup, "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
            "data": "synthetic (seeded, config-1 shapes)",
-           "config": {"workload": "config1: P=3000 x 11 conf, L=40 x 31 conf, T=20, 6820 "
-                                  "replicas per GPU, gaussian moves, exchange/10",
-                      "step": "10 MC steps + 1 exchange, all replicas",
-                      "l2": "flushed between steps (256 MB write)",
-                      "tile": {"replicas_per_cta": tile_used[0], "chunk_points": tile_used[1],
-                               "unroll": tile_used[2], "split": tile_used[3],
-                               "threads": tile_used[4], "source": tile_source},
-                      "parallelism": "replica shards, no collective" if world > 1 else "1 GPU"},
+           "config": bench_config(world),
+           "tile": {"replicas_per_cta": tile_used[0], "chunk_points": tile_used[1],
+                    "unroll": tile_used[2], "split": tile_used[3], "threads": tile_used[4],
+                    "source": tile_source},
            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
            "gpu_launches": 2 * args.steps + args.steps // max(1, intervals_per_dump),
            "delayed_acceptance": da, "batched_screen": screen, "post_mc": post}

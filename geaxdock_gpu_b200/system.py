@@ -119,14 +119,17 @@ def _chain(rng, n, n_conf):
     return out
 
 
-def forcefield(raw: abi.EneParaRaw, seed: int) -> abi.EnePara:
-    """Raw parameters with pmf1 ~ N(0, 1), folded by the library (OptimizeEnepara)."""
-    from .engine import fold_enepara
+def forcefield(raw: abi.EneParaRaw, seed: int, fold=None) -> abi.EnePara:
+    """Raw parameters with pmf1 ~ N(0, 1), folded by `fold` (OptimizeEnepara, src/util.C:717-760);
+    the library's gd_fold_enepara when None. A caller that must not load the library passes
+    another fold with the same arithmetic."""
+    if fold is None:
+        from .engine import fold_enepara as fold
     rng = np.random.default_rng(seed)
     r = abi.EneParaRaw.from_buffer_copy(bytes(raw))
     pmf = np.ctypeslib.as_array(r.pmf)  # [30][24][2] view
     pmf[:N_PROT_TYPES, :N_LIG_TYPES, 1] = rng.normal(0.0, 1.0, (N_PROT_TYPES, N_LIG_TYPES))
-    return fold_enepara(r)
+    return fold(r)
 
 
 def make_complex(rng, ff: abi.EnePara, L: int, n_lig: int, P: int, n_prt: int, n_tmp: int,
@@ -189,10 +192,11 @@ def make_protein(rng, ff: abi.EnePara, P: int, n_prt: int, center):
 
 
 def config(cfg: int, raw: abi.EneParaRaw, seed: int = 42, n_ligands: Optional[int] = None,
-           n_steps: Optional[int] = None) -> Workload:
-    """The benchmark configurations 0, 1, 2 (n_ligands shrinks config 2 for tests)."""
+           n_steps: Optional[int] = None, fold=None) -> Workload:
+    """The benchmark configurations 0, 1, 2 (n_ligands shrinks config 2 for tests); `fold` as
+    in forcefield()."""
     rng = np.random.default_rng(seed)
-    ff = forcefield(raw, seed)
+    ff = forcefield(raw, seed, fold)
     params = abi.mc_params(steps_per_exchange=10, steps_per_dump=abi.STEPS_PER_DUMP,
                            move_scale=(0.1, 0.1, 0.1, 0.05, 0.05, 0.05),
                            move_kind=abi.MOVE_GAUSSIAN, record=1, seed=seed)

@@ -45,7 +45,7 @@ def write_gdfx(path: str, arrays: Dict[str, np.ndarray]):
 
 
 def complex_container(path: str, cx: abi.ComplexArrays, ff: abi.EnePara, params: abi.McParams):
-    """The complex, the folded force field, the temperatures and the move scales."""
+    """The complex, the folded force field, the temperatures, the move scales and kind."""
     sizes = np.array([cx.n_lig, cx.n_prt, cx.n_tmp, cx.lna, cx.pnp, cx.pnk, cx.pos, 0], np.int32)
     arrays = {"sizes": sizes}
     for name in ("lig_x", "lig_y", "lig_z", "lig_center", "lig_t", "lig_c", "lig_n", "prt_x",
@@ -56,6 +56,7 @@ def complex_container(path: str, cx: abi.ComplexArrays, ff: abi.EnePara, params:
     arrays["temp"] = np.frombuffer(np.ascontiguousarray(cx.temp).tobytes(), np.float32)
     arrays["enepara"] = np.frombuffer(bytes(ff), np.float32)
     arrays["move_scale"] = np.array([params.move_scale[i] for i in range(6)], np.float32)
+    arrays["move_kind"] = np.array([params.move_kind], np.int32)
     write_gdfx(path, arrays)
 
 

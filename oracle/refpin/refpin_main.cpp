@@ -141,8 +141,10 @@ struct Reader {
 /* Timing mode: the reference's own MonteCarlo_d step functions (Move_d, CalcEnergy_d,
  * CalcMcc_d, Accept_d, RecordLigand_d, src/kernel_cuda_l1_montecarlo.cu:95-117) on a complex
  * given as product arrays (--bench file.gdfx), replicas [--r0, --r1), --steps steps each, one
- * thread; prints "replica_steps seconds". Moves: the reference's uniform form with the
- * given scales. */
+ * thread; prints "replica_steps seconds accepted". Moves: the container's move kind drawn from
+ * the product's Philox stream (stream 0, replica r, step) and handed to Move_d as its p, which
+ * the reference scales by move_scale (src/kernel_cuda_l2_move.cu:27): uniform p = 2u - 1 as
+ * MonteCarlo_d draws it, or Gaussian p = z (Box-Muller), the configured N(0, scale) moves. */
 static int bench_main(int argc, char **argv) {
   Reader rd(arg(argc, argv, "--bench", ""));
   if (!rd.ok) { fprintf(stderr, "cannot read the --bench container\n"); return 2; }
@@ -156,6 +158,7 @@ static int bench_main(int argc, char **argv) {
   const int r1 = std::min(cs.n_rep, atoi(arg(argc, argv, "--r1", "1")));
   const int steps = atoi(arg(argc, argv, "--steps", "10"));
   const uint64_t seed = strtoull(arg(argc, argv, "--seed", "42"), 0, 10);
+  const int move_kind = rd.data.count("move_kind") ? rd.i("move_kind")[0] : 0;
   const float *ms = rd.f("move_scale");
   float move_scale[6];
   for (int k = 0; k < 6; ++k) move_scale[k] = ms[k];
@@ -261,8 +264,15 @@ static int bench_main(int argc, char **argv) {
       const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
       const gd_u32x4 a = gd_philox4x32_10((uint32_t)r, (uint32_t)step, 0u, GD_RNG_MOVE, k0, k1);
       const gd_u32x4 b = gd_philox4x32_10((uint32_t)r, (uint32_t)step, 0u, GD_RNG_MOVE2, k0, k1);
-      const float pm[6] = {gd_sym11(a.v[0]), gd_sym11(a.v[1]), gd_sym11(a.v[2]),
-                           gd_sym11(a.v[3]), gd_sym11(b.v[0]), gd_sym11(b.v[1])};
+      float pm[6];
+      if (move_kind == GD_MOVE_GAUSSIAN) {
+        gd_box_muller(a.v[0], a.v[1], &pm[0], &pm[1]);
+        gd_box_muller(a.v[2], a.v[3], &pm[2], &pm[3]);
+        gd_box_muller(b.v[0], b.v[1], &pm[4], &pm[5]);
+      } else {
+        const uint32_t wd[6] = {a.v[0], a.v[1], a.v[2], a.v[3], b.v[0], b.v[1]};
+        for (int k = 0; k < 6; ++k) pm[k] = gd_sym11(wd[k]);
+      }
       move_all(ml, pm);
       CalcEnergy_d(0, ml, mp);
       CalcMcc_d(0, ml, mp);

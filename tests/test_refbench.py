@@ -23,3 +23,20 @@ def test_reference_steps_run_on_the_synthetic_system(tmp_path):
     # small uniform moves (the configured 0.1 A / 0.05 rad as the reference's scales): most
     # proposals are accepted, as in the product
     assert 0.5 < r["accepted"] / r["replica_steps"] <= 1.0
+
+
+def test_reference_steps_take_the_configured_gaussian_moves(tmp_path):
+    """The container's move kind reaches Move_d: Gaussian moves of the configured scales give
+    a different acceptance count from uniform moves of the same scales on the same replicas."""
+    z, _, _ = load_ref("1a07C1")
+    raw = abi.enepara_raw_from_array(z["enepara_raw"])
+    w = system.config(0, raw)
+    cx, ff, p = w.complexes[0], w.ff, w.params
+    assert p.move_kind == abi.MOVE_GAUSSIAN
+    for i in range(6):
+        p.move_scale[i] *= 20.0
+    g = refbench.run(cx, ff, p, n_rep=32, steps=5, procs=4, workdir=str(tmp_path))
+    p.move_kind = abi.MOVE_UNIFORM
+    u = refbench.run(cx, ff, p, n_rep=32, steps=5, procs=4, workdir=str(tmp_path))
+    assert g["replica_steps"] == u["replica_steps"] == 160
+    assert g["accepted"] != u["accepted"]
