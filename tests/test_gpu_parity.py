@@ -11,7 +11,7 @@ import pytest
 from geaxdock_gpu_b200 import abi, engine, system
 from oracle import pyoracle as po
 from tests.golden.fixtures import load_ref
-from tests.tolerance import rel_errors
+from tests.tolerance import plain_rel_errors, rel_errors, report
 
 pytestmark = pytest.mark.gpu
 
@@ -24,12 +24,16 @@ def raw():
     return abi.enepara_raw_from_array(z["enepara_raw"])
 
 
-def _energy_check(eng, ff, cx, ci, ip, il, mm, refmap):
+def _energy_check(eng, ff, cx, ci, ip, il, mm, refmap, plain=None):
+    """Worst sum-of-magnitudes error per term of eng's energies of poses mm; the worst plain
+    relative error per term is folded into `plain` when given."""
     got = eng.eval_energy(ci, ip, il, mm)
     worst = np.zeros(10)
     for i in range(mm.shape[0]):
         o = po.pose_energy(ff, cx, ip, il, mm[i], refmap, 64)
         worst = np.maximum(worst, rel_errors(got["e"][i], o, ff))
+        if plain is not None:
+            np.maximum(plain, plain_rel_errors(got["e"][i], o), out=plain)
         assert abs(got["cms"][i] - o["cms"]) <= 2e-6, (i, got["cms"][i], o["cms"])
         assert abs(got["rmsd"][i] - o["rmsd"]) <= 1e-5 * max(1.0, o["rmsd"])
     return worst
@@ -40,12 +44,15 @@ def test_eval_energy_reference_complexes(name):
     z, cx, ff = load_ref(name)
     rm = z["ref_matrix"].astype(np.uint8)
     with engine.Engine(ff, [cx], abi.mc_params()) as eng:
+        sumabs, plain = np.zeros(10), np.zeros(10)
         for ip in range(min(cx.n_prt, 3)):
             sel = np.nonzero(z["pose_idx"][:, 0] == ip)[0]
             for il in np.unique(z["pose_idx"][sel, 1])[:4]:
                 mm = z["pose_mm"][sel[z["pose_idx"][sel, 1] == il]]
-                worst = _energy_check(eng, ff, cx, 0, ip, int(il), mm, rm)
+                worst = _energy_check(eng, ff, cx, 0, ip, int(il), mm, rm, plain)
+                sumabs = np.maximum(sumabs, worst)
                 assert worst.max() <= TOL, (ip, il, worst)
+    report("GPU gd_eval_energy, %s" % name, sumabs, plain)
 
 
 @pytest.mark.parametrize("cfg", [0, 1])
@@ -55,10 +62,13 @@ def test_eval_energy_synthetic(raw, cfg):
     rm = po.ref_map(ff, cx)
     rng = np.random.default_rng(5)
     mm = np.concatenate([rng.normal(0, 1.5, (24, 3)), rng.uniform(-3.2, 3.2, (24, 3))], 1)
+    sumabs, plain = np.zeros(10), np.zeros(10)
     with engine.Engine(ff, [cx], w.params) as eng:
         for ip in range(min(cx.n_prt, 2)):
-            worst = _energy_check(eng, ff, cx, 0, ip, 1, mm.astype(np.float32), rm)
+            worst = _energy_check(eng, ff, cx, 0, ip, 1, mm.astype(np.float32), rm, plain)
+            sumabs = np.maximum(sumabs, worst)
             assert worst.max() <= TOL, worst
+    report("GPU gd_eval_energy, config %d" % cfg, sumabs, plain)
 
 
 @pytest.mark.parametrize("chunk", [64, 512, 4096])
@@ -417,3 +427,61 @@ def test_eval_energy_soft_core_poses():
     with engine.Engine(ff, [cx], abi.mc_params()) as eng:
         worst = _energy_check(eng, ff, cx, 0, 0, 0, mm, rm)
     assert worst.max() <= TOL, worst
+
+
+def _extreme_batch(raw):
+    """Config-2 complexes at the shape extremes: ligands of 10 and 64 atoms (8 conformers)
+    against pockets of 1,200 and 6,000 points (4 conformers), 16 temperatures each."""
+    rng = np.random.default_rng(2024)
+    ff = system.forcefield(raw, 42)
+    cxs = []
+    for j, P in enumerate((1200, 6000)):
+        center = np.array([100.0 * j, 0.0, 0.0])
+        prot = system.make_protein(rng, ff, P, 4, center)
+        for L in (10, 64):
+            cxs.append(system.make_complex(rng, ff, L=L, n_lig=8, P=P, n_prt=4, n_tmp=16,
+                                           protein=prot, pocket=center))
+    return ff, cxs
+
+
+@pytest.mark.parametrize("chunk", [512, 2048])
+def test_config2_extreme_shapes_against_oracle(raw, chunk):
+    """Energies of the batched kernel at config 2's extremes (L 10 / 64, P 1,200 / 6,000) in
+    one context with the fill tile of 256 threads (25 replicas per CTA at L = 10, 4 at
+    L = 64) and protein chunks smaller than every pocket (streamed): every term, cms and rmsd
+    of given poses (gd_eval_energy) and of the initial poses (gd_mc_init) against the FP64
+    oracle. Both error metrics are printed and the sum-of-magnitudes one is asserted: the
+    synthetic totals here cancel by up to 130x (sum of |w_i e_i| over |e_9|), so a plain 1e-5
+    on them would ask for 8e-8 of the summed magnitudes, below FP32 pair arithmetic."""
+    ff, cxs = _extreme_batch(raw)
+    params = abi.mc_params(steps_per_exchange=10, steps_per_dump=10, seed=7)
+    rng = np.random.default_rng(chunk)
+    sumabs, plain = np.zeros(10), np.zeros(10)
+    with engine.Engine(ff, cxs, params) as eng:
+        eng.set_tile(0, chunk, 0, 1, 256)
+        ks = [eng.replicas_per_cta(i) for i in range(len(cxs))]
+        assert ks == [25, 4, 25, 4], ks
+        for ci, cx in enumerate(cxs):
+            rm = po.ref_map(ff, cx)
+            for ip, il in ((0, 0), (3, 5)):
+                mm = np.zeros((10, 6), np.float32)
+                mm[:, :3] = rng.normal(0, 1.5, (10, 3))
+                mm[:, 3:] = rng.uniform(-3.1, 3.1, (10, 3))
+                w = _energy_check(eng, ff, cx, ci, ip, il, mm, rm, plain)
+                sumabs = np.maximum(sumabs, w)
+        eng.mc_init()
+        eng.sync()
+        st = eng.state()
+        for ci, cx in enumerate(cxs):
+            rm = po.ref_map(ff, cx)
+            off = eng.offsets[ci]
+            for r in range(0, cx.n_rep, 37):
+                p, l = r // (cx.n_tmp * cx.n_lig), r % cx.n_lig
+                o = po.pose_energy(ff, cx, p, l, np.zeros(6, np.float32), rm, 64)
+                got = st["energy_old"][off + r]
+                sumabs = np.maximum(sumabs, rel_errors(got["e"], o, ff))
+                np.maximum(plain, plain_rel_errors(got["e"], o), out=plain)
+                assert abs(got["cms"] - o["cms"]) <= 2e-6
+                assert abs(got["rmsd"] - o["rmsd"]) <= 1e-5 * max(1.0, o["rmsd"])
+    report("config-2 extremes, chunk %d" % chunk, sumabs, plain)
+    assert sumabs.max() <= TOL, sumabs
