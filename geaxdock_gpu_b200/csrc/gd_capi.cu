@@ -905,6 +905,11 @@ int gd_destroy(gd_ctx *c) {
   return GD_OK;
 }
 
+/* set-up of the allocation-free entry point on `device` (defined with it below) */
+namespace {
+int noalloc_prepare(int device);
+}
+
 int gd_create(const gd_enepara *ff, const gd_complex_desc *cxs, int n_complexes,
               const gd_mc_params *mc, int device, gd_ctx **out) {
   if (!out) return fail(GD_ERR_INVALID, "null out");
@@ -937,6 +942,11 @@ int gd_create(const gd_enepara *ff, const gd_complex_desc *cxs, int n_complexes,
     return fail(GD_ERR_NODEVICE, "device %d is sm_%d%d; this library is built for sm_100a",
                 device, prop.major, prop.minor);
   CK(cudaSetDevice(device));
+
+  {
+    const int rc0 = noalloc_prepare(device);
+    if (rc0) return rc0;
+  }
 
   gd_ctx *c = new gd_ctx();
   c->device = device;
@@ -1927,7 +1937,9 @@ int gd_trace_get(gd_ctx *c, float *e_new, int *acc, int *n_steps) {
  * holds up to GD_NOALLOC_MAX_POSES poses, is allocated once when the library is loaded on a
  * device and stays there until the process exits, and is shared by every call in the
  * process: each call rewrites the parts it uses (the queue head is cleared by the fill
- * kernel), and calls whose kernels overlap on the GPU would race on it. */
+ * kernel), and calls whose kernels overlap on the GPU would race on it. Its device address
+ * is looked up by gd_create (which allocates anyway), once per device, so the entry point
+ * itself only reads the cached address. */
 
 namespace {
 
@@ -1961,18 +1973,32 @@ __global__ void gd_noalloc_fill(int complex_index, int prt_conf, int lig_conf, i
 std::mutex g_noalloc_mu;
 void *g_noalloc_addr[64] = {nullptr};
 
-/* Device address of the scratch array on `device` (the current device), looked up once per
- * device: host code cannot use the symbol itself as a device address. */
+/* Set-up on `device` (the current device), once per device, from gd_create: the device
+ * address of the scratch array (host code cannot use the symbol itself as a device address)
+ * and the fill kernel's attributes, which load the module's code and data under lazy module
+ * loading, so that no later call of the entry point loads anything. */
+int noalloc_prepare(int device) {
+  if (device < 0 || device >= 64) return fail(GD_ERR_NODEVICE, "device %d out of range", device);
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (g_noalloc_addr[device]) return GD_OK;
+  void *p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p)
+    return fail(GD_ERR_CUDA, "cudaGetSymbolAddress(scratch) failed: %s", cudaGetErrorString(e));
+  cudaFuncAttributes fa;
+  e = cudaFuncGetAttributes(&fa, gd_noalloc_fill);
+  if (e != cudaSuccess)
+    return fail(GD_ERR_CUDA, "cudaFuncGetAttributes(fill) failed: %s", cudaGetErrorString(e));
+  g_noalloc_addr[device] = p;
+  return GD_OK;
+}
+
+/* The scratch array's device address cached by noalloc_prepare for `device`. */
 int noalloc_scratch(int device, NoallocScratch **out) {
   if (device < 0 || device >= 64) return fail(GD_ERR_NODEVICE, "device %d out of range", device);
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_addr[device]) {
-    void *p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p)
-      return fail(GD_ERR_CUDA, "cudaGetSymbolAddress(scratch) failed: %s", cudaGetErrorString(e));
-    g_noalloc_addr[device] = p;
-  }
+  if (!g_noalloc_addr[device])
+    return fail(GD_ERR_STATE, "allocation-free scratch not set up on device %d", device);
   *out = reinterpret_cast<NoallocScratch *>(g_noalloc_addr[device]);
   return GD_OK;
 }
@@ -1986,7 +2012,8 @@ extern "C" int gd_eval_energy_noalloc(gd_ctx *c, int ci, int prt_conf, int lig_c
   const ComplexInfo &x = c->info[ci];
   if (prt_conf < 0 || prt_conf >= x.n_prt || lig_conf < 0 || lig_conf >= x.n_lig)
     return fail(GD_ERR_INVALID, "conformer index out of range");
-  if (n < 0 || n > GD_NOALLOC_MAX_POSES)
+  if (n < 0) return fail(GD_ERR_INVALID, "gd_eval_energy_noalloc: negative pose count %d", n);
+  if (n > GD_NOALLOC_MAX_POSES)
     return fail(GD_ERR_CAPACITY,
                 "gd_eval_energy_noalloc: %d poses; the allocation-free path holds at most %d "
                 "(split the batch or use gd_eval_energy)",

@@ -296,11 +296,12 @@ int gd_eval_energy(gd_ctx *ctx, int complex_index, int prt_conf, int lig_conf,
  * No counterpart in the reference. d_movematrix (n_poses x 6 floats) and d_out (n_poses
  * gd_energy) are DEVICE pointers the caller owns; the call allocates nothing: its work queue
  * and tile list live in one fixed device array of the library, sized for at most
- * GD_NOALLOC_MAX_POSES poses (larger n_poses returns GD_ERR_CAPACITY). The call only enqueues
- * work on the context's stream; gd_sync (or a stream sync) makes d_out ready. The first call
- * on a device looks up that array's device address; make that first call before any stream
- * capture. Every call in the process shares the array, so calls whose kernels overlap on the
- * GPU (two contexts on different streams) race: serialise them. */
+ * GD_NOALLOC_MAX_POSES poses (larger n_poses returns GD_ERR_CAPACITY, a negative one
+ * GD_ERR_INVALID). The call only enqueues work on the context's stream; gd_sync (or a stream
+ * sync) makes d_out ready. gd_create looks up that array's device address once per device,
+ * so the call itself loads and allocates nothing. Every call in the process shares the
+ * array, so calls whose kernels overlap on the GPU (two contexts on different streams) race:
+ * serialise them. */
 #define GD_NOALLOC_MAX_POSES 16384
 int gd_eval_energy_noalloc(gd_ctx *ctx, int complex_index, int prt_conf, int lig_conf,
                            const float *d_movematrix, int n_poses, gd_energy *d_out);

@@ -3,9 +3,11 @@
 Callers that cannot allocate device memory when they need energies (a framework that owns the
 whole device pool, a callback or real-time context where cudaMalloc is not allowed) pass
 device buffers they already own; the entry point's own scratch lives in a fixed device array
-of the library. These checks call it through the C ABI twice in a row, against the regular
-gd_eval_energy on the same poses, and check its size limit. The file is named to be collected
-last, so that a run stopping at the first failure has run every other test before it.
+of the library. These checks call it through the C ABI several times in a row, against the
+regular gd_eval_energy on the same poses (the same kernel on the same poses, so the results
+must agree bit for bit), at the size limit and past it, and check that a call leaves the
+device's free memory unchanged. The file is named to be collected last, so that a run stopping
+at the first failure has run every other test before it.
 """
 import ctypes as C
 
@@ -27,6 +29,11 @@ def _noalloc_fn():
     return fn
 
 
+def _poses(rng, n):
+    return np.concatenate([rng.normal(0, 1.0, (n, 3)), rng.uniform(-3.1, 3.1, (n, 3))],
+                          axis=1).astype(np.float32)
+
+
 def test_noalloc_matches_eval_energy_on_two_calls():
     import torch
 
@@ -34,9 +41,8 @@ def test_noalloc_matches_eval_energy_on_two_calls():
     z, cx, ff = load_ref("1a07C1")
     rng = np.random.default_rng(11)
     with engine.Engine(ff, [cx], abi.mc_params()) as eng:
-        for call, (ip, il, n) in enumerate([(0, 3, 37), (2, 11, 300)]):
-            mm = np.concatenate([rng.normal(0, 1.0, (n, 3)), rng.uniform(-3.1, 3.1, (n, 3))],
-                                axis=1).astype(np.float32)
+        for call, (ip, il, n) in enumerate([(0, 3, 37), (2, 11, 300), (1, 5, MAX_POSES)]):
+            mm = _poses(rng, n)
             want = eng.eval_energy(0, ip, il, mm)
             # device buffers owned by the caller (allocated here, not by the entry point)
             d_mm = torch.from_numpy(mm).to("cuda")
@@ -46,9 +52,29 @@ def test_noalloc_matches_eval_energy_on_two_calls():
             assert rc == abi.GD_OK, engine.lib().gd_last_error_string()
             eng.sync()
             got = d_out.cpu().numpy().view(abi.ENERGY_DTYPE)
-            for fld in ("e", "cms", "rmsd"):
-                np.testing.assert_allclose(got[fld], want[fld], rtol=1e-6, atol=1e-7,
-                                           err_msg="call %d field %s" % (call, fld))
+            assert got.tobytes() == want.tobytes(), "call %d (%d poses)" % (call, n)
+
+
+def test_noalloc_call_leaves_free_device_memory_unchanged():
+    import torch
+
+    fn = _noalloc_fn()
+    z, cx, ff = load_ref("1a07C1")
+    n = 1000
+    mm = _poses(np.random.default_rng(3), n)
+    with engine.Engine(ff, [cx], abi.mc_params()) as eng:
+        d_mm = torch.from_numpy(mm).to("cuda")
+        d_out = torch.zeros(n * 12, dtype=torch.float32, device="cuda")
+        first = torch.zeros_like(d_out)
+        assert fn(eng.h, 0, 0, 0, d_mm.data_ptr(), n, first.data_ptr()) == abi.GD_OK
+        eng.sync()
+        torch.cuda.synchronize()
+        free0, _ = torch.cuda.mem_get_info()
+        assert fn(eng.h, 0, 0, 0, d_mm.data_ptr(), n, d_out.data_ptr()) == abi.GD_OK
+        eng.sync()
+        free1, _ = torch.cuda.mem_get_info()
+        assert free1 == free0, (free0, free1)
+        assert torch.equal(first, d_out)
 
 
 def test_noalloc_rejects_too_many_poses():
@@ -61,3 +87,5 @@ def test_noalloc_rejects_too_many_poses():
         rc = fn(eng.h, 0, 0, 0, d.data_ptr(), MAX_POSES + 1, d.data_ptr())
         assert rc == abi.GD_ERR_CAPACITY
         assert b"allocation-free" in engine.lib().gd_last_error_string()
+        assert fn(eng.h, 0, 0, 0, d.data_ptr(), -1, d.data_ptr()) == abi.GD_ERR_INVALID
+        assert fn(eng.h, 0, 0, 0, d.data_ptr(), 0, d.data_ptr()) == abi.GD_OK
