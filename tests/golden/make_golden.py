@@ -19,6 +19,10 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
+if REPO not in sys.path:
+    sys.path.insert(0, REPO)
+
+from oracle import reference_root  # noqa: E402
 
 RUNS = {
     # name: (data dir, pdb, sdf, ff, id, n_tmp, floor, ceil, n_exchanges, n_poses)
@@ -54,7 +58,7 @@ KMEANS = {"edge100": ("edge100.txt", 10), "color100": ("color100.txt", 10),
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=reference_root())
     a = ap.parse_args()
     subprocess.run(["make", "-s", "-C", os.path.join(REPO, "oracle"), "refpin",
                     "REFERENCE=" + a.reference], check=True)

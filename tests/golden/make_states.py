@@ -20,6 +20,7 @@ REPO = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, REPO)
 
 from geaxdock_gpu_b200 import abi  # noqa: E402
+from oracle import reference_root
 
 
 def records(n=300, seed=9):
@@ -46,7 +47,7 @@ def records(n=300, seed=9):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=reference_root())
     a = ap.parse_args()
     subprocess.run(["make", "-s", "-C", os.path.join(REPO, "oracle"), "refpin",
                     "REFERENCE=" + a.reference], check=True)

@@ -14,12 +14,14 @@
 import os
 
 import numpy as np
+
+from oracle import reference_root
 import pytest
 
 from geaxdock_gpu_b200 import abi, loaders
 from tests.golden.fixtures import load_ref
 
-REFERENCE = os.environ.get("GD_REFERENCE", "/root/reference")
+REFERENCE = reference_root() or ""
 DATA = os.path.join(REFERENCE, "data")
 
 RUNS = {
