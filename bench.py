@@ -17,14 +17,18 @@ reference: the reference's own MonteCarlo_d step functions (Move_d, CalcEnergy_d
            Accept_d, RecordLigand_d) compiled for the CPU from its sources (oracle/_ref/refpin),
            one process per host core, a bounded replica sample per step, same metric; the
            oracle's FP32 OpenMP restatement when that build is absent.
-Multi-GPU (torchrun): every rank runs its own config-1 system (own RNG stream), no data-path
-collective (replicas shard without exchange across shards): weak scaling.
+Multi-GPU (torchrun): the job is one batch of N config-1 complexes (complex i drawn with seed
+42 + i, RNG stream i), split across ranks by shard.shard_batch's assignment (one complex per GPU);
+exchange never crosses complexes, so there is no data-path collective: weak scaling.
 delayed_acceptance (N = 1): the config-3 workload on the config-1 system (2,000 burn-in steps of
            training samples, one epoch of Adam, then K intervals of delayed-acceptance and of
            plain steps from the same state, device-timed), at the configured moves and at 20x
            and 60x larger moves; surrogate RMSE, stage acceptances, per-temperature KS p-values.
 batched_screen (N = 1): config 2 (2,048 uneven ligands x 8 uneven pockets, 1,048,576 replicas)
            in one context, one persistent launch per 10-step interval, autotuned tile.
+screen_delayed_acceptance (N = 1): config 4, delayed acceptance on that screen with one network
+           per pocket, against the plain batched run from the same state, at the configured and
+           at 20x larger moves; best-pose energy and RMSD agreement per ligand.
 """
 from __future__ import annotations
 
@@ -63,7 +67,8 @@ def bench_config(world):
                         "GPU, gaussian moves 0.1 A / 0.05 rad, exchange/10",
             "step": "10 MC steps of every replica + 1 exchange",
             "l2": "flushed between steps (256 MB write)",
-            "parallelism": "replica shards, no collective" if world > 1 else "1 GPU"}
+            "parallelism": ("one batch of N config-1 complexes split by shard_batch, one "
+                            "complex per GPU, no collective") if world > 1 else "1 GPU"}
 
 
 def product_library_mapped():
@@ -359,16 +364,13 @@ def delayed_acceptance(w, dev, tile, scale_mult, intervals, burn=2000, iters=166
             "timing": "CUDA events on each engine's stream, L2 flushed between intervals"}
 
 
-def batched_screen(dev, intervals=3):
+def batched_screen(dev, w, intervals=3):
     """Config 2: 2,048 ligands (10-64 atoms, 8 conformers) round-robin over 8 pockets (1,200-6,000
     points, 4 conformers), 16 temperatures = 1,048,576 replicas in one context; every interval is
     one graph-captured persistent launch over all complexes (10 steps) + exchange. Tile autotuned
     on this batch; device time from CUDA events; FLOP at 36 per ligand-protein pair."""
     import torch
-    from geaxdock_gpu_b200 import autotune, engine, system
-    t0 = time.perf_counter()
-    w = system.config(2, load_raw())
-    gen_s = time.perf_counter() - t0
+    from geaxdock_gpu_b200 import autotune, engine
     pairs = sum(c.n_rep * c.lna * c.pnp for c in w.complexes)
     with engine.Engine(w.ff, w.complexes, w.params, device=dev) as eng:
         eng.mc_init()
@@ -398,84 +400,132 @@ def batched_screen(dev, intervals=3):
             "intervals": intervals, "tflops_at_36_flop_per_pair": pairs * 36 * spe / (avg * 1e-3) / 1e12,
             "tile": {"replicas_per_cta": tile[0], "chunk_points": tile[1],
                      "unroll": tile[2], "split": tile[3], "threads": tile[4],
-                     "cached": tuned["cached"]},
-            "generate_s": gen_s}
+                     "cached": tuned["cached"]}}, tile
 
 
-def screen_da(dev, move_mult=1.0, burn=100, steps=100, iters=1665):
-    """Config 4: delayed acceptance on the config-2 screen (2,048 ligands x 8 pockets,
-    1,048,576 replicas). One network for the batch, conditioned on per-pocket features and a
-    learned embedding per (ligand, pocket conformer, ligand conformer); trained on the
-    proposals of `burn` plain burn-in steps; per-ligand fallback to plain steps. Then `steps`
-    delayed-acceptance steps and, from the same state, `steps` plain steps, device-timed; the
-    best (lowest) energy of each ligand's replicas at the end is compared between the runs."""
+def screen_da(dev, w, tile, move_mult=1.0, burn=100, steps=50, iters=1665, n_pockets=8):
+    """Config 4: delayed acceptance on the config-2 screen with one network per pocket. The
+    ligands are grouped by pocket (ligand i docks to pocket i mod 8); each pocket's ligands run
+    in a context of their own (131,072 replicas, every complex keeping its batch index as RNG
+    stream) with its own surrogate, trained on the proposals of that pocket's `burn` plain
+    burn-in steps, and the per-ligand fallback to plain steps. The plain batched run (all
+    ligands in one context) starts from the same state. Both are device-timed (CUDA events on
+    each context's stream) over `steps` steps; per ligand, the best (lowest-energy) pose of its
+    replicas at the end is compared between the two runs, by energy and by RMSD."""
+    import contextlib
     import torch
-    from geaxdock_gpu_b200 import autotune, engine, system
-    w = system.config(2, load_raw())
-    p = w.params
+    from geaxdock_gpu_b200 import engine
+    p = type(w.params).from_buffer_copy(w.params)
     p.record = 0
     for i in range(6):
         p.move_scale[i] *= move_mult
     spe = p.steps_per_exchange
-    with engine.Engine(w.ff, w.complexes, p, device=dev) as b, \
-            engine.Engine(w.ff, w.complexes, p, device=dev) as a:
-        b.mc_init()
-        b.sync()
-        autotune.tune(b, device=dev)
-        a.set_tile(*b.tile())
-        sur = engine.Surrogate(b, fallback_accept=0.5, fallback_window=2000)
+    n_cx = len(w.complexes)
+    groups = [[i for i in range(n_cx) if i % n_pockets == k] for k in range(n_pockets)]
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+    with contextlib.ExitStack() as stack:
+        pk = []
+        for idx in groups:
+            e = stack.enter_context(engine.Engine(w.ff, [w.complexes[i] for i in idx], p,
+                                                  device=dev))
+            for j, i in enumerate(idx):
+                e.set_rng_stream(j, i)
+            e.set_tile(*tile)
+            e.mc_init()
+            sur = engine.Surrogate(e, fallback_accept=0.5, fallback_window=2000,
+                                   sample_cap=burn * e.n_rep)
+            pk.append((e, sur, idx))
         t0 = time.perf_counter()
-        sur.collect(0, burn, exchange=True)
-        b.sync()
+        for e, sur, _ in pk:
+            sur.collect(0, burn, exchange=True)
+        for e, _, _ in pk:
+            e.sync()
         collect_s = time.perf_counter() - t0
         t0 = time.perf_counter()
-        losses = sur.train(iters)
+        losses = [sur.train(iters) for _, sur, _ in pk]
         train_s = time.perf_counter() - t0
+        a = stack.enter_context(engine.Engine(w.ff, w.complexes, p, device=dev))
+        a.set_tile(*tile)
         a.mc_init()
-        start = b.state()
-        a.set_state(start)
+        full = a.state()
+        for e, _, idx in pk:
+            st = e.state()
+            for j, i in enumerate(idx):
+                n = w.complexes[i].n_rep
+                full[a.offsets[i]:a.offsets[i] + n] = st[e.offsets[j]:e.offsets[j] + n]
+        a.set_state(full)
         a.sync()
         sa = torch.cuda.ExternalStream(a.cuda_stream(), device=dev)
-        sb = torch.cuda.ExternalStream(b.cuda_stream(), device=dev)
+        spk = [torch.cuda.ExternalStream(e.cuda_stream(), device=dev) for e, _, _ in pk]
         da_ms = plain_ms = 0.0
         for s in range(burn, burn + steps, spe):
-            e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
-            e[0].record(sb)
-            sur.run(s, spe, exchange=True)
-            e[1].record(sb)
-            b.sync()
-            e[2].record(sa)
+            evs = []
+            for (e, sur, _), stream in zip(pk, spk):
+                e0, e1 = ev(), ev()
+                e0.record(stream)
+                sur.run(s, spe, exchange=True)
+                e1.record(stream)
+                evs.append((e0, e1))
+            for e, _, _ in pk:
+                e.sync()
+            da_ms += sum(x.elapsed_time(y) for x, y in evs)
+            e2, e3 = ev(), ev()
+            e2.record(sa)
             a.run_fused(s, spe, exchange=True)
-            e[3].record(sa)
+            e3.record(sa)
             a.sync()
-            da_ms += e[0].elapsed_time(e[1])
-            plain_ms += e[2].elapsed_time(e[3])
-        stats = sur.stats()
-        fa, fb = a.state(), b.state()
-        offs = list(a.offsets)
-    best_a, best_b = [], []
-    for k, cx in enumerate(w.complexes):
-        sl = slice(offs[k], offs[k] + cx.n_rep)
-        best_a.append(float(fa["energy_old"]["e"][sl, 9].min()))
-        best_b.append(float(fb["energy_old"]["e"][sl, 9].min()))
-    best_a, best_b = np.array(best_a), np.array(best_b)
-    n_off = sum(1 for s_ in stats if not s_["active"])
-    prop = sum(s_["proposed"] for s_ in stats)
-    passed = sum(s_["passed"] for s_ in stats)
-    acc = sum(s_["accepted"] for s_ in stats)
+            plain_ms += e2.elapsed_time(e3)
+        fa = a.state()
+        best = {"da_e": np.zeros(n_cx), "da_r": np.zeros(n_cx), "pl_e": np.zeros(n_cx),
+                "pl_r": np.zeros(n_cx)}
+        per_pocket = []
+        for (e, sur, idx), ls in zip(pk, losses):
+            st, stats = e.state(), sur.stats()
+            for j, i in enumerate(idx):
+                n = w.complexes[i].n_rep
+                mine = st[e.offsets[j]:e.offsets[j] + n]["energy_old"]
+                k = int(np.argmin(mine["e"][:, 9]))
+                best["da_e"][i], best["da_r"][i] = mine["e"][k, 9], mine["rmsd"][k]
+                ref = fa[a.offsets[i]:a.offsets[i] + n]["energy_old"]
+                k = int(np.argmin(ref["e"][:, 9]))
+                best["pl_e"][i], best["pl_r"][i] = ref["e"][k, 9], ref["rmsd"][k]
+            prop = sum(x["proposed"] for x in stats)
+            passed = sum(x["passed"] for x in stats)
+            per_pocket.append({"ligands": len(idx), "replicas": e.n_rep,
+                               "pocket_points": w.complexes[idx[0]].pnp,
+                               "train_loss_first_last": [float(ls[0]), float(ls[-1])],
+                               "proposed": prop, "passed": passed,
+                               "accepted": sum(x["accepted"] for x in stats),
+                               "stage1_pass": passed / max(1, prop),
+                               "stage2_accept": sum(x["accepted"] for x in stats) / max(1, passed),
+                               "rmse": float(np.sqrt(np.mean([x["rmse"] ** 2 for x in stats]))),
+                               "ligands_fallen_back": sum(1 for x in stats if not x["active"])})
+    prop = sum(x["proposed"] for x in per_pocket)
+    passed = sum(x["passed"] for x in per_pocket)
+    acc = sum(x["accepted"] for x in per_pocket)
     rs = w.n_rep * steps
-    return {"workload": "config4: config-2 screen with delayed acceptance",
+    de, dr = best["da_e"] - best["pl_e"], best["da_r"] - best["pl_r"]
+    return {"workload": "config4: config-2 screen (2,048 ligands x 8 pockets, 1,048,576 replicas) "
+                        "with delayed acceptance, one surrogate per pocket",
             "move_scale": [p.move_scale[i] for i in range(6)],
             "value": rs / (da_ms * 1e-3), "unit": UNIT,
             "plain_same_state": rs / (plain_ms * 1e-3), "speedup_vs_plain": plain_ms / da_ms,
             "stage1_pass": passed / max(1, prop), "stage2_accept": acc / max(1, passed),
-            "ligands_fallen_back_to_plain": n_off, "ligands": len(w.complexes),
+            "ligands_fallen_back_to_plain": sum(x["ligands_fallen_back"] for x in per_pocket),
+            "ligands": n_cx, "networks": len(pk), "per_pocket": per_pocket,
             "collect_steps": burn, "collect_s": collect_s, "train_iterations": iters,
-            "train_s": train_s, "train_loss_first_last": [float(losses[0]), float(losses[-1])],
-            "best_energy_mean_da_vs_plain": [float(best_b.mean()), float(best_a.mean())],
-            "best_energy_median_abs_diff": float(np.median(np.abs(best_b - best_a))),
-            "best_energy_corr": float(np.corrcoef(best_a, best_b)[0, 1]),
-            "steps": steps}
+            "train_s": train_s, "steps": steps,
+            "best_pose": {
+                "energy_mean_da_plain": [float(best["da_e"].mean()), float(best["pl_e"].mean())],
+                "energy_median_abs_diff": float(np.median(np.abs(de))),
+                "energy_corr": float(np.corrcoef(best["da_e"], best["pl_e"])[0, 1]),
+                "rmsd_mean_da_plain": [float(best["da_r"].mean()), float(best["pl_r"].mean())],
+                "rmsd_median_abs_diff": float(np.median(np.abs(dr))),
+                "rmsd_corr": float(np.corrcoef(best["da_r"], best["pl_r"])[0, 1]),
+                "note": "per ligand, the lowest-energy replica at the end of each run, both runs "
+                        "from the same burned-in state"},
+            "timing": "CUDA events on each context's stream; delayed acceptance summed over the "
+                      "pockets' contexts, run one after another"}
 
 
 def post_mc_measure(eng, cx, args):
@@ -514,8 +564,13 @@ def run_ours(args, rank, world, local_rank):
 
     dev = local_rank
     torch.cuda.set_device(dev)
-    w = workload(42 + rank)
+    # one batch of `world` config-1 complexes (complex i drawn with seed 42 + i, RNG stream i),
+    # split across the ranks by shard_batch's assignment; at N = 1 it is config 1 itself
+    from geaxdock_gpu_b200 import shard, system
+    mine = shard.assign_complexes([shard.complex_cost(6820, 40, 3000)] * world, world)[rank]
+    w = system.config1_batch(load_raw(), mine)
     cx, ff, params = w.complexes[0], w.ff, w.params
+    n_total = world * cx.n_rep  # replicas of the whole batch (every complex has 6,820)
     spe = params.steps_per_exchange
     intervals_per_dump = params.steps_per_dump // spe
     dist = None
@@ -523,7 +578,9 @@ def run_ours(args, rank, world, local_rank):
         import torch.distributed as dist
 
     # ---------------- device-timed throughput ----------------
-    eng = engine.Engine(ff, [cx], params, device=dev)
+    eng = engine.Engine(ff, w.complexes, params, device=dev)
+    for j, i in enumerate(mine):
+        eng.set_rng_stream(j, i)
     eng.mc_init()
     eng.sync()
     if args.tile:
@@ -578,8 +635,8 @@ def run_ours(args, rank, world, local_rank):
     if dist:
         from geaxdock_gpu_b200.shard import max_over_ranks
         tot_ms = max_over_ranks(tot_ms, dist)
-    rs_per_step = cx.n_rep * spe
-    value = world * rs_per_step * args.steps / (tot_ms * 1e-3)
+    rs_per_step = eng.n_rep * spe
+    value = n_total * spe * args.steps / (tot_ms * 1e-3)
     flops_rs = algorithmic_flops_per_replica_step(eng, w) if rank == 0 else 0.0
     post = None
     if world == 1 and not args.no_postmc:
@@ -592,16 +649,19 @@ def run_ours(args, rank, world, local_rank):
     if not args.no_e2e:
         import ctypes as C
         h2d = 0
-        for name in ("lig_x", "lig_y", "lig_z", "lig_center", "lig_t", "lig_c", "lig_n", "prt_x",
-                     "prt_y", "prt_z", "prt_t", "prt_c", "prt_ele", "prt_seq3r", "prt_hflag",
-                     "prt_hpp", "psp", "kde_x", "kde_y", "kde_z", "kde_t", "mcs_x", "mcs_y",
-                     "mcs_z", "mcs_tcc", "temp"):
-            h2d += getattr(cx, name).nbytes
+        for c in w.complexes:
+            for name in ("lig_x", "lig_y", "lig_z", "lig_center", "lig_t", "lig_c", "lig_n",
+                         "prt_x", "prt_y", "prt_z", "prt_t", "prt_c", "prt_ele", "prt_seq3r",
+                         "prt_hflag", "prt_hpp", "psp", "kde_x", "kde_y", "kde_z", "kde_t",
+                         "mcs_x", "mcs_y", "mcs_z", "mcs_tcc", "temp"):
+                h2d += getattr(c, name).nbytes
         h2d += C.sizeof(abi.EnePara)
         if dist:
             dist.barrier()
         t0 = time.perf_counter()
-        e = engine.Engine(ff, [cx], params, device=dev)
+        e = engine.Engine(ff, w.complexes, params, device=dev)
+        for j, i in enumerate(mine):
+            e.set_rng_stream(j, i)
         e.set_tile(*tile_used)
         e.mc_init()
         it2 = 0
@@ -629,13 +689,13 @@ def run_ours(args, rank, world, local_rank):
         if dist:
             from geaxdock_gpu_b200.shard import max_over_ranks
             dt = max_over_ranks(dt, dist)
-        e2e = {"value": world * rs_per_step * args.steps / dt, "unit": UNIT,
+        e2e = {"value": n_total * spe * args.steps / dt, "unit": UNIT,
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                "scope": "gd_create + gd_mc_init + K x (gd_mc_run + gd_exchange + "
                         "gd_get_etotal) + the filled record rows of every dump window "
                         "(gd_get_record_counts + gd_get_records_raw, as the reference's launcher "
                         "downloads LigRecord per dump) + gd_destroy, host wall clock, every rank "
-                        "its own shard, slowest rank"}
+                        "its shard of the batch, slowest rank"}
 
     if rank != 0:
         return
@@ -669,9 +729,18 @@ def run_ours(args, rank, world, local_rank):
               "moves_x20": delayed_acceptance(w, dev, tile_used, 20.0, args.steps),
               "moves_x60": delayed_acceptance(w, dev, tile_used, 60.0, args.steps)}
 
-    screen = None
+    screen = screen4 = None
     if world == 1 and not args.no_screen:
-        screen = batched_screen(dev)
+        from geaxdock_gpu_b200 import system
+        t0 = time.perf_counter()
+        w2 = system.config(2, load_raw())
+        gen_s = time.perf_counter() - t0
+        screen, tile2 = batched_screen(dev, w2)
+        screen["generate_s"] = gen_s
+        if not args.no_da:
+            screen4 = {"configured_moves": screen_da(dev, w2, tile2, 1.0),
+                       "moves_x20": screen_da(dev, w2, tile2, 20.0)}
+        del w2
 
     cpu = None
     if world == 1 and not args.no_cpu:
@@ -687,7 +756,8 @@ def run_ours(args, rank, world, local_rank):
                     "source": tile_source},
            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
            "gpu_launches": 2 * args.steps + args.steps // max(1, intervals_per_dump),
-           "delayed_acceptance": da, "batched_screen": screen, "post_mc": post}
+           "delayed_acceptance": da, "batched_screen": screen, "screen_delayed_acceptance": screen4,
+           "post_mc": post}
     print(json.dumps(out), flush=True)
 
 
@@ -819,7 +889,10 @@ def main():
                          "prints its own JSON line")
     args = ap.parse_args()
     if args.screen_da:
-        print(json.dumps(screen_da(0, args.move_mult)), flush=True)
+        from geaxdock_gpu_b200 import system
+        w2 = system.config(2, load_raw())
+        _, tile2 = batched_screen(0, w2, intervals=1)
+        print(json.dumps(screen_da(0, w2, tile2, args.move_mult)), flush=True)
         return
     if args.profile_aux:
         profile_aux(args)

@@ -222,3 +222,19 @@ def config(cfg: int, raw: abi.EneParaRaw, seed: int = 42, n_ligands: Optional[in
         params.steps_per_dump = 100
         return Workload("config2", ff, cxs, params, n_steps or 5000)
     raise ValueError("config must be 0, 1 or 2")
+
+
+def config1_batch(raw: abi.EneParaRaw, indices, seed: int = 42, fold=None) -> Workload:
+    """Complexes `indices` of the batch that stands for config 1 on several GPUs: complex i is
+    a config-1 complex (P = 3,000 x 11 conformers, L = 40 x 31 conformers, 20 temperatures)
+    drawn with seed + i, all under the force field of `seed`; complex 0 is config 1's own.
+    A rank generates only its shard's complexes."""
+    ff = forcefield(raw, seed, fold)
+    params = abi.mc_params(steps_per_exchange=10, steps_per_dump=abi.STEPS_PER_DUMP,
+                           move_scale=(0.1, 0.1, 0.1, 0.05, 0.05, 0.05),
+                           move_kind=abi.MOVE_GAUSSIAN, record=1, seed=seed)
+    cxs = []
+    for i in indices:
+        rng = np.random.default_rng(seed + i)
+        cxs.append(make_complex(rng, ff, L=40, n_lig=31, P=3000, n_prt=11, n_tmp=20))
+    return Workload("config1-batch", ff, cxs, params, 20000)

@@ -239,3 +239,133 @@ def test_fallback_to_plain(raw):
         assert st2["proposed"] == st["proposed"]
         assert st2["plain"] == st["plain"] + 20 * cx.n_rep
         assert st["rmse"] > 0 and st["n_err"] == st["passed"]
+
+
+def test_trained_surrogate_gains_over_plain_and_untrained(raw):
+    """What the trained network gains, on the config-0 system at 20x the configured moves
+    (2 A / 1 rad): from one equilibrated state, plain Monte Carlo, delayed acceptance with an
+    untrained network (its random initial weights, normalised like a trained one) and delayed
+    acceptance with the network trained on the burn-in's exact energies each run 300 steps.
+    The cost of an accepted move is the number of exact energy evaluations spent per accepted
+    move: every proposal for plain Monte Carlo, the stage-1 survivors for delayed acceptance.
+    The trained network must spend fewer than both others, by at least a third, and pass its
+    survivors through stage 2 at least 90 % of the time."""
+    w = _small(raw, move_scale=(2.0, 2.0, 2.0, 1.0, 1.0, 1.0))
+    cx, ff, params = w.complexes[0], w.ff, w.params
+    params.record = 0
+    burn, span = 2000, 300
+    R = cx.n_rep
+    with engine.Engine(ff, [cx], params) as plain, \
+            engine.Engine(ff, [cx], params) as good, \
+            engine.Engine(ff, [cx], params) as blind:
+        good.mc_init()
+        sg = engine.Surrogate(good, hidden=256, batch=2048, sample_cap=1 << 20,
+                              fallback_accept=0.0)
+        sg.collect(0, burn, exchange=True)
+        losses = sg.train(1500)
+        assert losses[-50:].mean() < 0.1 * losses[:10].mean()
+        start = good.state()
+        blind.mc_init()
+        sb = engine.Surrogate(blind, hidden=256, batch=2048, sample_cap=1 << 16,
+                              fallback_accept=0.0)
+        sb.collect(0, 20, exchange=True)   # samples only set the output normalisation
+        sb.train(0)                        # stage on with the untrained network
+        blind.set_state(start)
+        plain.mc_init()
+        plain.set_state(start)
+        for e in (plain, good, blind):
+            e.sync()
+        st0 = {k: s.stats()[0] for k, s in (("good", sg), ("blind", sb))}
+        plain.run_fused(burn, span, exchange=True)
+        sg.run(burn, span, exchange=True)
+        sb.run(burn, span, exchange=True)
+        plain_acc = int((plain.state()["n_accept"] - start["n_accept"]).sum())
+        st1 = {k: s.stats()[0] for k, s in (("good", sg), ("blind", sb))}
+    d = {k: {f: st1[k][f] - st0[k][f] for f in ("proposed", "passed", "accepted")}
+         for k in st1}
+    assert d["good"]["proposed"] == d["blind"]["proposed"] == span * R
+    cost_plain = span * R / max(1, plain_acc)
+    cost_good = d["good"]["passed"] / max(1, d["good"]["accepted"])
+    cost_blind = d["blind"]["passed"] / max(1, d["blind"]["accepted"])
+    stage2_good = d["good"]["accepted"] / max(1, d["good"]["passed"])
+    print("exact evaluations per accepted move: plain %.3f, untrained %.3f, trained %.3f; "
+          "trained stage-2 acceptance %.3f, acceptance plain %.3f / trained %.3f"
+          % (cost_plain, cost_blind, cost_good, stage2_good, plain_acc / (span * R),
+             d["good"]["accepted"] / (span * R)))
+    assert stage2_good >= 0.9
+    assert cost_good < (2.0 / 3.0) * cost_plain
+    assert cost_good < (2.0 / 3.0) * cost_blind
+
+
+def test_decisions_replay_ragged_batch(raw):
+    """Delayed acceptance with the stage on over a ragged config-2 batch (6 ligands of uneven
+    size on uneven pockets, one network for the batch): every stage-1 and stage-2 decision of
+    every replica is replayed on the CPU from the Philox draws of its complex's stream, the
+    traced surrogate energies and the exact energies; a sample of the exact energies is
+    checked against the FP64 oracle."""
+    w = system.config(2, raw, n_ligands=6)
+    params = w.params
+    params.steps_per_dump = 400
+    for i in range(6):
+        params.move_scale[i] *= 8.0
+    s0, n = 60, 12
+    with engine.Engine(w.ff, w.complexes, params) as eng:
+        eng.set_tile(4, 256)
+        eng.mc_init()
+        sur = engine.Surrogate(eng, hidden=128, batch=1024, sample_cap=1 << 20,
+                               fallback_accept=0.0)
+        sur.collect(0, s0, exchange=True)
+        losses = sur.train(200)
+        assert losses[-1] < losses[0]
+        st0 = eng.state()
+        sur.trace_enable(s0, n)
+        sur.run(s0, n, exchange=False)
+        eng.sync()
+        s_tr, e_tr, f_tr = sur.trace()
+        st1 = eng.state()
+        offs = list(eng.offsets)
+    assert (f_tr == 0).any() and (f_tr == 1).any() and (f_tr == 2).any()
+    mm_all = st0["movematrix_old"].copy()
+    eo_all = st0["energy_old"]["e"][:, 9].copy()
+    checked, worst = 0, 0.0
+    for ci, cx in enumerate(w.complexes):
+        sl = slice(offs[ci], offs[ci] + cx.n_rep)
+        mm, e_old = mm_all[sl], eo_all[sl]
+        ft, st_, et = f_tr[sl], s_tr[sl], e_tr[sl]
+        s_cur = np.full(cx.n_rep, np.nan, np.float32)
+        idx_tmp = st0["replica"]["idx_tmp"][sl]
+        mbs = np.asarray(cx.temp["minus_beta"], np.float32)
+        refmap = po.ref_map(w.ff, cx)
+        reps = np.arange(cx.n_rep, dtype=np.uint32)
+        for k in range(n):
+            step = s0 + k
+            delta, u2 = po.draw_steps(params.seed, params.move_kind, list(params.move_scale),
+                                      reps, np.full(cx.n_rep, step, np.uint32), stream=ci)
+            for r in range(cx.n_rep):
+                mb = mbs[idx_tmp[r]]
+                mmn = (mm[r] + delta[r]).astype(np.float32)
+                f, sn = ft[r, k], st_[r, k]
+                if not np.isnan(s_cur[r]):
+                    u1 = _stage1_uniform(params.seed, ci, r, step)
+                    d1 = np.float32(np.float32(sn - s_cur[r]) * mb)
+                    assert (f > 0) == bool(u1 < po.expf(d1)), (ci, r, k)
+                if f == 0:
+                    continue
+                en = np.float32(et[r, k])
+                if r % 101 == 0:
+                    p, l = r // (cx.n_tmp * cx.n_lig), r % cx.n_lig
+                    o = po.pose_energy(w.ff, cx, int(p), int(l), mmn, refmap, 64)
+                    worst = max(worst, abs(float(en) - o["e"][9]) / scales(o, w.ff)[9])
+                    checked += 1
+                sc = s_cur[r] if not np.isnan(s_cur[r]) else sn
+                d2 = np.float32(np.float32(np.float32(en - e_old[r]) - np.float32(sn - sc)) * mb)
+                if not np.isnan(s_cur[r]):
+                    assert bool(u2[r] < po.expf(d2)) == (f == 2), (ci, r, k)
+                if f == 2:
+                    mm[r] = mmn
+                    e_old[r] = en
+                    s_cur[r] = sn
+        mm_all[sl], eo_all[sl] = mm, e_old
+    assert checked > 20 and worst < 1e-5, (checked, worst)
+    assert np.array_equal(st1["movematrix_old"].view(np.uint32), mm_all.view(np.uint32))
+    assert np.array_equal(st1["energy_old"]["e"][:, 9], eo_all)

@@ -89,3 +89,84 @@ def test_shard_batch_keeps_batch_index_as_stream():
         assert [batch[s] for s in streams] == cxs
         seen += streams
     assert sorted(seen) == list(range(6))
+
+
+def _mc_shard_worker(rank, world, port, q):
+    """One rank: its shard of a small ragged batch through the oracle's FP32 Monte Carlo
+    restatement (each complex with its batch index as RNG stream), states gathered on rank 0."""
+    import datetime
+
+    import numpy as np
+    import torch.distributed as dist
+
+    from geaxdock_gpu_b200 import abi, system
+    from oracle import pyoracle as po
+    from tests.golden.fixtures import load_ref
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=120))
+    try:
+        z, _, _ = load_ref("1a07C1")
+        w = system.config(2, abi.enepara_raw_from_array(z["enepara_raw"]), n_ligands=5,
+                          fold=po.fold_enepara)
+        batch = [c.subset(n_lig=2, n_prt=1, n_tmp=4) for c in w.complexes]
+        params = w.params
+        params.record = 0
+        mine, streams = shard.shard_batch(batch, world, rank)
+        out = {}
+        for cx, sid in zip(mine, streams):
+            mc = po.MC(w.ff, cx, params, stream=sid, precision=32)
+            mc.init()
+            for e in range(2):
+                mc.run(0, 10 * e, 10, 1)
+                mc.exchange(int(not (e % 2)))
+            g = mc.get()
+            out[sid] = (g["mm_old"].tobytes(), g["e_old"].tobytes(), g["replica"].tobytes())
+        gathered = [None] * world
+        dist.all_gather_object(gathered, out)
+        q.put((rank, gathered))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_shard_a_batch_and_reproduce_the_single_run():
+    """A ragged batch split by shard_batch over two ranks: every complex runs on exactly one
+    rank with its batch index as RNG stream, and the union of the ranks' final states equals
+    the single-rank run of the whole batch bit for bit."""
+    from geaxdock_gpu_b200 import abi, system
+    from oracle import pyoracle as po
+    from tests.golden.fixtures import load_ref
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_mc_shard_worker, args=(r, world, port, q))
+             for r in range(world)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=300) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    union = {}
+    for part in res[0][1]:
+        assert not set(part) & set(union)
+        union.update(part)
+    assert res[0][1] == res[1][1]
+    z, _, _ = load_ref("1a07C1")
+    w = system.config(2, abi.enepara_raw_from_array(z["enepara_raw"]), n_ligands=5,
+                      fold=po.fold_enepara)
+    batch = [c.subset(n_lig=2, n_prt=1, n_tmp=4) for c in w.complexes]
+    params = w.params
+    params.record = 0
+    assert sorted(union) == list(range(len(batch)))
+    for sid, cx in enumerate(batch):
+        mc = po.MC(w.ff, cx, params, stream=sid, precision=32)
+        mc.init()
+        for e in range(2):
+            mc.run(0, 10 * e, 10, 1)
+            mc.exchange(int(not (e % 2)))
+        g = mc.get()
+        assert union[sid] == (g["mm_old"].tobytes(), g["e_old"].tobytes(),
+                              g["replica"].tobytes()), sid
