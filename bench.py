@@ -400,7 +400,7 @@ def batched_screen(dev, w, intervals=3):
             "intervals": intervals, "tflops_at_36_flop_per_pair": pairs * 36 * spe / (avg * 1e-3) / 1e12,
             "tile": {"replicas_per_cta": tile[0], "chunk_points": tile[1],
                      "unroll": tile[2], "split": tile[3], "threads": tile[4],
-                     "cached": tuned["cached"]}}, tile
+                     "replicas_per_lane": tile[5], "cached": tuned["cached"]}}, tile
 
 
 def screen_da(dev, w, tile, move_mult=1.0, burn=100, steps=50, iters=1665, n_pockets=8):
@@ -753,7 +753,7 @@ def run_ours(args, rank, world, local_rank):
            "config": bench_config(world),
            "tile": {"replicas_per_cta": tile_used[0], "chunk_points": tile_used[1],
                     "unroll": tile_used[2], "split": tile_used[3], "threads": tile_used[4],
-                    "source": tile_source},
+                    "replicas_per_lane": tile_used[5], "source": tile_source},
            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
            "gpu_launches": 2 * args.steps + args.steps // max(1, intervals_per_dump),
            "delayed_acceptance": da, "batched_screen": screen, "screen_delayed_acceptance": screen4,

@@ -113,7 +113,7 @@ class McParams(C.Structure):
 
 class Tile(C.Structure):
     _fields_ = [("replicas_per_cta", I), ("chunk_points", I), ("unroll", I), ("split", I),
-                ("threads", I)]
+                ("threads", I), ("replicas_per_lane", I)]
 
 
 class ReplicaState(C.Structure):

@@ -1,7 +1,8 @@
 """Tile autotuner with a JSON cache.
 
 The fused kernel's tile is (replicas per CTA, protein points per shared-memory chunk, point
-pairs in flight per lane). `tune(engine)` times a candidate grid with gd_autotune (pose
+pairs in flight per lane, protein split, CTA lanes in fill mode, replicas per thread).
+`tune(engine)` times a candidate grid with gd_autotune (pose
 evaluation of the chains' current poses, chains untouched), applies the fastest and stores it
 in a JSON cache keyed by (ligand atoms, protein points, replicas, device name); later engines
 with the same key reuse the entry without timing.
@@ -19,21 +20,27 @@ from .engine import Engine, check, lib
 DEFAULT_CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tile_cache.json")
 
 
-def candidates(lna: int, ragged: bool = False) -> List[Tuple[int, int, int, int, int]]:
-    """(replicas_per_cta, chunk_points, unroll, split, threads) candidates: one replica count for
-    every complex that fills 128..256 lanes for the largest ligand, and for a ragged batch also
-    CTAs of 128..256 threads that every complex fills with as many replicas as fit."""
+def candidates(lna: int, ragged: bool = False,
+               pack: bool = None) -> List[Tuple[int, int, int, int, int, int]]:
+    """(replicas_per_cta, chunk_points, unroll, split, threads, replicas_per_lane) candidates:
+    one replica count for every complex that fills 128..256 lanes for the largest ligand, and
+    for a ragged batch also CTAs of 128..256 lanes that every complex fills with as many
+    replicas as fit; with `pack` (default: uniform batches, whose timing is cheap) each also
+    with two replicas per thread. Candidates that a batch cannot take are skipped by the
+    timing."""
     ks = sorted({max(1, t // lna) for t in (128, 160, 192, 224, 256)} | {1})
     ks = [k for k in ks if k * lna <= 256]
+    packs = (1, 2) if (not ragged if pack is None else pack) else (1,)
     out = []
-    for chunk in (256, 512, 1024):
-        for unroll in (1, 2):
-            for k in ks:
-                out.append((k, chunk, unroll, 1, 0))
-            if ragged:
-                for threads in (128, 192, 256):
-                    if threads >= lna:
-                        out.append((0, chunk, unroll, 1, threads))
+    for p in packs:
+        for chunk in (256, 512, 1024):
+            for unroll in (1, 2):
+                for k in ks:
+                    out.append((k, chunk, unroll, 1, 0, p))
+                if ragged:
+                    for threads in (128, 192, 256):
+                        if threads >= lna:
+                            out.append((0, chunk, unroll, 1, threads, p))
     return out
 
 
@@ -59,6 +66,7 @@ def time_candidates(eng: Engine, cands: Sequence[Tuple[int, ...]], repeats: int 
         arr[i].replicas_per_cta, arr[i].chunk_points, arr[i].unroll = k, ch, u
         arr[i].split = c[3] if len(c) > 3 else 1
         arr[i].threads = c[4] if len(c) > 4 else 0
+        arr[i].replicas_per_lane = c[5] if len(c) > 5 else 1
     best = abi.Tile()
     ms = (C.c_float * len(cands))()
     fn = lib().gd_autotune
@@ -66,8 +74,8 @@ def time_candidates(eng: Engine, cands: Sequence[Tuple[int, ...]], repeats: int 
                    C.POINTER(C.c_float)]
     fn.restype = C.c_int
     check(fn(eng.h, arr, len(cands), repeats, C.byref(best), ms))
-    return (best.replicas_per_cta, best.chunk_points, best.unroll, best.split, best.threads), \
-        list(ms)
+    return (best.replicas_per_cta, best.chunk_points, best.unroll, best.split, best.threads,
+            best.replicas_per_lane), list(ms)
 
 
 def tune(eng: Engine, cache_path: Optional[str] = DEFAULT_CACHE, device: int = 0,
@@ -80,7 +88,7 @@ def tune(eng: Engine, cache_path: Optional[str] = DEFAULT_CACHE, device: int = 0
             cache = json.load(open(cache_path))
         except (OSError, ValueError):
             cache = {}
-    if key in cache and not force and len(cache[key]["tile"]) == 5:
+    if key in cache and not force and len(cache[key]["tile"]) == 6:
         eng.set_tile(*cache[key]["tile"])
         return dict(cache[key], cached=True)
     lna = max(c.lna for c in eng.complexes)

@@ -30,13 +30,15 @@
 #include "gd_numerics.h"
 
 namespace gd {
-template <int UNROLL, bool SPLIT, bool DA>
+template <int UNROLL, bool SPLIT, bool DA, int PACK>
 __global__ void gd_mc_kernel(GdMcArgs a, GdForceConst f);
-#define GD_EXT(U, S, D) extern template __global__ void gd_mc_kernel<U, S, D>(GdMcArgs, GdForceConst);
-GD_EXT(1, false, false) GD_EXT(2, false, false) GD_EXT(4, false, false)
-GD_EXT(1, true, false) GD_EXT(2, true, false) GD_EXT(4, true, false)
-GD_EXT(1, false, true) GD_EXT(2, false, true) GD_EXT(4, false, true)
-GD_EXT(1, true, true) GD_EXT(2, true, true) GD_EXT(4, true, true)
+#define GD_EXT(U, S, D, P) \
+  extern template __global__ void gd_mc_kernel<U, S, D, P>(GdMcArgs, GdForceConst);
+GD_EXT(1, false, false, 1) GD_EXT(2, false, false, 1) GD_EXT(4, false, false, 1)
+GD_EXT(1, true, false, 1) GD_EXT(2, true, false, 1) GD_EXT(4, true, false, 1)
+GD_EXT(1, false, true, 1) GD_EXT(2, false, true, 1) GD_EXT(4, false, true, 1)
+GD_EXT(1, true, true, 1) GD_EXT(2, true, true, 1) GD_EXT(4, true, true, 1)
+GD_EXT(1, false, false, 2) GD_EXT(2, false, false, 2)
 #undef GD_EXT
 __global__ void gd_exchange_kernel(const GdDevComplex *cxs, const int *group_base, int n_complex,
                                    int g_begin, int g_end, gd_replica *replica,
@@ -93,6 +95,8 @@ struct ComplexInfo {
   int n_lig, n_prt, n_tmp, lna, pnp, pnp_pad, pnk, pos;
   int rep_offset, n_rep, k;
   int stream;
+  int types_uniform; /* every ligand conformer has the same atom types (two replicas per
+                        thread share their atom's pair parameters) */
 };
 
 /* One chain of the fused loops: a contiguous range of (complex, protein conformer) blocks,
@@ -113,6 +117,8 @@ struct gd_ctx {
   gd_mc_params mc{};
   int n_complex = 0, n_rep = 0, n_groups = 0;
   int threads = 256, chunk = 512, unroll = 2, split = 1, num_sms = 148;
+  int pack = 1; /* replicas per thread of the plain launches: the tile's lanes (threads) run on
+                   threads / pack threads */
   int fill_threads = 0, fill_cap = 0; /* the last gd_set_tile in fill mode (threads > 0) */
   std::vector<ComplexInfo> info;
   std::vector<void *> allocs;
@@ -583,19 +589,37 @@ typedef void (*McKernel)(GdMcArgs, GdForceConst);
 /* the kernel variant for an unroll depth, a protein split and the mode-3 epilogue */
 template <bool S, bool D>
 McKernel mc_variant(int unroll) {
-  if (unroll >= 4) return gd::gd_mc_kernel<4, S, D>;
-  if (unroll >= 2) return gd::gd_mc_kernel<2, S, D>;
-  return gd::gd_mc_kernel<1, S, D>;
+  if (unroll >= 4) return gd::gd_mc_kernel<4, S, D, 1>;
+  if (unroll >= 2) return gd::gd_mc_kernel<2, S, D, 1>;
+  return gd::gd_mc_kernel<1, S, D, 1>;
 }
 
-McKernel mc_kernel(int unroll, int split, bool da = false) {
+McKernel mc_kernel(int unroll, int split, bool da = false, int pack = 1) {
   if (da) return split > 1 ? mc_variant<true, true>(unroll) : mc_variant<false, true>(unroll);
+  if (pack == 2 && split <= 1)
+    return unroll >= 2 ? gd::gd_mc_kernel<2, false, false, 2> : gd::gd_mc_kernel<1, false, false, 2>;
   return split > 1 ? mc_variant<true, false>(unroll) : mc_variant<false, false>(unroll);
+}
+
+/* replicas per thread of a launch: the context's packing for the plain modes without split */
+int launch_pack(const gd_ctx *c, int split, bool da) {
+  return (!da && (split ? split : c->split) <= 1) ? c->pack : 1;
+}
+
+/* threads per CTA of a launch: the tile's lanes over the replicas per thread */
+int launch_threads(const gd_ctx *c, int split = 0, bool da = false) {
+  return c->threads / launch_pack(c, split, da);
+}
+
+McKernel launch_kernel(const gd_ctx *c, int split = 0, bool da = false) {
+  const int S = split ? split : c->split;
+  return mc_kernel(c->unroll, S, da, launch_pack(c, split, da));
 }
 
 int grid_for(gd_ctx *c, int n_tiles, size_t smem, int split = 0, bool da = false) {
   int nb = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, mc_kernel(c->unroll, split ? split : c->split, da), c->threads,
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, launch_kernel(c, split, da),
+                                                    launch_threads(c, split, da),
                                                     smem) != cudaSuccess ||
       nb < 1)
     nb = 1;
@@ -630,7 +654,7 @@ GdMcArgs base_args(gd_ctx *c) {
 }
 
 int set_kernel_attrs(const gd_ctx *c, size_t smem, int split = 0, bool da = false) {
-  const McKernel k = mc_kernel(c->unroll, split ? split : c->split, da);
+  const McKernel k = launch_kernel(c, split, da);
   CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   CK(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
                           cudaSharedmemCarveoutMaxShared));
@@ -647,7 +671,7 @@ int launch_mc(gd_ctx *c, GdMcArgs a, const GdTileDesc *d_tiles, int n_tiles, int
   a.tile_counter = counter;
   CK(cudaMemsetAsync(counter, 0, sizeof(int), c->stream));
   const int grid = grid_for(c, n_tiles, smem);
-  mc_kernel(c->unroll, a.split)<<<grid, c->threads, smem, c->stream>>>(a, c->fc);
+  launch_kernel(c)<<<grid, launch_threads(c), smem, c->stream>>>(a, c->fc);
   CK(cudaGetLastError());
   return GD_OK;
 }
@@ -1033,6 +1057,13 @@ int gd_create(const gd_enepara *ff, const gd_complex_desc *cxs, int n_complexes,
     x.n_rep = d.n_prt * d.n_tmp * d.n_lig;
     x.stream = ci;
     x.k = 1;
+    x.types_uniform = 1;
+    for (int lc = 1; lc < d.n_lig && x.types_uniform; ++lc)
+      for (int i = 0; i < d.lna; ++i)
+        if (d.lig_t[lc * d.lna + i] != d.lig_t[i]) {
+          x.types_uniform = 0;
+          break;
+        }
     c->info.push_back(x);
     group_base[ci] = goff;
     goff += d.n_prt * d.n_lig;
@@ -1268,9 +1299,21 @@ int gd_set_tile(gd_ctx *c, int k, const gd_tile *t) {
   if (t->threads < 0 || t->threads > GD_MAX_TPB || (t->threads & 31))
     return fail(GD_ERR_INVALID, "threads must be a multiple of 32 in 0..%d", GD_MAX_TPB);
   if (k < -1 || k >= c->n_complex) return fail(GD_ERR_INVALID, "bad complex index");
+  if (t->replicas_per_lane < 0 || t->replicas_per_lane > 2)
+    return fail(GD_ERR_INVALID, "replicas_per_lane must be 0, 1 or 2");
   const int S = t->split ? t->split : 1;
+  const int P = t->replicas_per_lane == 2 ? 2 : 1;
   if ((t->chunk_points / 2) < S)
     return fail(GD_ERR_INVALID, "chunk_points must hold at least two points per split");
+  if (P == 2) {
+    if (S != 1) return fail(GD_ERR_INVALID, "two replicas per lane need split 1");
+    for (int i = 0; i < c->n_complex; ++i)
+      if (!c->info[i].types_uniform || c->info[i].lna < 2)
+        return fail(GD_ERR_INVALID,
+                    "complex %d: two replicas per lane need at least two ligand atoms and the "
+                    "same atom types in every ligand conformer",
+                    i);
+  }
   /* one block size per context: every complex's k must fit the block */
   std::vector<ComplexInfo> info = c->info;
   for (int i = 0; i < c->n_complex; ++i) {
@@ -1280,21 +1323,34 @@ int gd_set_tile(gd_ctx *c, int k, const gd_tile *t) {
     if (t->threads > 0) {
       if (S * info[i].lna > t->threads)
         return fail(GD_ERR_INVALID, "complex %d: split * lna exceeds threads", i);
-      kk = std::min(kk, t->threads / (S * info[i].lna));
+      /* two per lane: an even count whose lane pairs fill half the CTA's lanes */
+      kk = std::min(kk, P == 2 ? 2 * ((t->threads / 2) / info[i].lna)
+                               : t->threads / (S * info[i].lna));
+      if (kk < 1)
+        return fail(GD_ERR_INVALID, "complex %d: no replica pair fits %d lanes", i, t->threads);
     }
     info[i].k = std::min(kk, GD_MAX_SLOTS);
   }
+  /* T: the tile's lanes (a multiple of 32 per pack, so that T / pack threads are whole warps) */
   int T = 32;
-  for (auto &x : info) T = std::max(T, ((x.k * S * x.lna + 31) / 32) * 32);
-  if (t->threads > 0) T = std::max(T, t->threads);
+  if (P == 2) {
+    int Tp = 32;
+    for (auto &x : info) Tp = std::max(Tp, (((x.k + 1) / 2 * x.lna + 31) / 32) * 32);
+    if (t->threads > 0) Tp = std::max(Tp, ((t->threads / 2 + 31) / 32) * 32);
+    T = 2 * Tp; /* Tp, the threads of a launch, is whole warps */
+  } else {
+    for (auto &x : info) T = std::max(T, ((x.k * S * x.lna + 31) / 32) * 32);
+    if (t->threads > 0) T = std::max(T, t->threads);
+  }
   if (T > GD_MAX_TPB)
-    return fail(GD_ERR_INVALID, "replicas_per_cta * split * lna exceeds %d", GD_MAX_TPB);
+    return fail(GD_ERR_INVALID, "replicas_per_cta * split * lna exceeds %d lanes", GD_MAX_TPB);
   c->info = info;
   c->threads = T;
   c->chunk = t->chunk_points;
   c->split = S;
   c->fill_threads = t->threads;
   c->fill_cap = t->threads > 0 ? t->replicas_per_cta : 0;
+  c->pack = P;
   if (t->unroll) c->unroll = t->unroll;
   c->tile_gen += 1;
   build_tiles(c, 0, c->n_rep - 1, c->full_tiles);
@@ -1335,7 +1391,7 @@ int gd_autotune(gd_ctx *c, const gd_tile *cand, int n_cand, int repeats, gd_tile
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  const gd_tile keep_tile = {c->info[0].k, c->chunk, c->unroll, c->split, c->threads};
+  const gd_tile keep_tile = {c->info[0].k, c->chunk, c->unroll, c->split, c->threads, c->pack};
   const int keep_fill_threads = c->fill_threads, keep_fill_cap = c->fill_cap;
   std::vector<int> keep_k;
   for (auto &x : c->info) keep_k.push_back(x.k);
@@ -1387,6 +1443,7 @@ int gd_autotune(gd_ctx *c, const gd_tile *cand, int n_cand, int repeats, gd_tile
     best->unroll = c->unroll;
     best->split = c->split;
     best->threads = cand[best_i].threads;
+    best->replicas_per_lane = c->pack;
   } else {
     /* restore the tile in use before the probe */
     for (int i = 0; i < c->n_complex; ++i) c->info[i].k = keep_k[i];
@@ -1394,6 +1451,7 @@ int gd_autotune(gd_ctx *c, const gd_tile *cand, int n_cand, int repeats, gd_tile
     c->chunk = keep_tile.chunk_points;
     c->unroll = keep_tile.unroll;
     c->split = keep_tile.split;
+    c->pack = keep_tile.replicas_per_lane;
     c->fill_threads = keep_fill_threads;
     c->fill_cap = keep_fill_cap;
     c->tile_gen += 1;
@@ -1451,6 +1509,7 @@ int gd_get_tile(const gd_ctx *c, int k, gd_tile *t) {
   t->unroll = c->unroll;
   t->split = c->split;
   t->threads = c->fill_threads;
+  t->replicas_per_lane = c->pack;
   return GD_OK;
 }
 
@@ -1550,7 +1609,7 @@ int gd_mc_run_fused(gd_ctx *c, int s1, int n_steps, int exchange) {
         a.tiles = c->d_chain_tiles + ch.t_off;
         a.n_tiles = ch.t_cnt;
         a.tile_counter = c->d_counters + k * chunks + i;
-        mc_kernel(c->unroll, a.split)<<<grid, c->threads, smem, st>>>(a, c->fc);
+        launch_kernel(c)<<<grid, launch_threads(c), smem, st>>>(a, c->fc);
         if (exchange)
           gd::gd_exchange_kernel<<<(ch.xg1 - ch.xg0 + 127) / 128, 128, 0, st>>>(
               c->d_cx, c->d_group_base, c->n_complex, ch.xg0, ch.xg1, c->d_replica, c->d_etotal,
@@ -2040,7 +2099,7 @@ extern "C" int gd_eval_energy_noalloc(gd_ctx *c, int ci, int prt_conf, int lig_c
   const size_t smem = smem_bytes(c);
   if ((rc = set_kernel_attrs(c, smem))) return rc;
   const int grid = grid_for(c, n_tiles, smem);
-  mc_kernel(c->unroll, a.split)<<<grid, c->threads, smem, c->stream>>>(a, c->fc);
+  launch_kernel(c)<<<grid, launch_threads(c), smem, c->stream>>>(a, c->fc);
   CK(cudaGetLastError());
   return GD_OK;
 }

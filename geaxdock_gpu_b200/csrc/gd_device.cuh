@@ -31,6 +31,9 @@
 #define GD_SLOT_BYTES 192      /* shared-memory bytes per replica slot (sizeof gd::Slot) */
 /* resident 256-thread CTAs per SM the register budget is set for, per unroll depth */
 #define GD_MIN_BLOCKS(u) ((u) >= 4 ? 2 : ((u) >= 2 ? 3 : 4))
+/* two replicas per thread: CTAs of at most GD_MAX_TPB / 2 threads (the tile's lanes over two),
+ * 4 resident per SM with one point pair in flight per replica, 3 with two */
+#define GD_MIN_BLOCKS_PACK(u, p) ((p) == 2 ? ((u) >= 2 ? 3 : 4) : GD_MIN_BLOCKS(u))
 #define GD_MAX_SLOTS 128       /* replicas per CTA */
 #define GD_NQ 12               /* per-lane partial sums handed to the reducer */
 

@@ -4,7 +4,8 @@
  * gd_mc_kernel: one persistent kernel for MonteCarlo_Init_d, MonteCarlo_d and pose
  * evaluation (reference src/kernel_cuda_l1_montecarlo.cu:12-127). Each CTA pulls tiles from
  * a work queue; a tile is `count` replicas of one protein conformer. Lane (slot j, atom l)
- * owns one ligand atom of one replica for all steps of the launch:
+ * owns one ligand atom of one replica for all steps of the launch (a thread holds one lane,
+ * or with PACK = 2 the lanes of the same atom in two slots, which share every load):
  *   Move_d        (src/kernel_cuda_l2_move.cu:21-80)       placed in registers from a
  *                                                         Philox draw, no HBM traffic;
  *   CalcEnergy_d  (src/kernel_cuda_l2_calcenergy.cu:19-360) pair loop over protein points
@@ -225,6 +226,32 @@ __device__ __forceinline__ void pair_range(const float4 *__restrict__ PA,
   if (i1 & 1) pair_body<KIND, HDB, false>(PA[m1], PB[m1], PX, m1, ax2, ay2, az2, q, psprow, f, a);
 }
 
+/* The same range for the same atom of two replicas (the lane's two slots): one load of each
+ * point pair, one loop, the segment's parameters and table rows shared; each atom's sums are
+ * the operations of pair_range in the same order, so its energies are bit-identical. */
+template <int KIND, bool HDB, int UNROLL>
+__device__ __forceinline__ void pair_range2(const float4 *__restrict__ PA,
+                                            const float4 *__restrict__ PB,
+                                            const float4 *__restrict__ PX, int i0, int i1,
+                                            const float *ax, const float *ay, const float *az,
+                                            const Pair2 &q, const float *__restrict__ psprow,
+                                            const GdForceConst &f, Acc *a) {
+  const float2 ax0 = f2(ax[0]), ay0 = f2(ay[0]), az0 = f2(az[0]);
+  const float2 ax1 = f2(ax[1]), ay1 = f2(ay[1]), az1 = f2(az[1]);
+  const int m0 = i0 >> 1, m1 = i1 >> 1;
+#pragma unroll UNROLL
+  for (int m = m0; m < m1; ++m) {
+    const float4 A = PA[m], B = PB[m];
+    pair_body<KIND, HDB, true>(A, B, PX, m, ax0, ay0, az0, q, psprow, f, a[0]);
+    pair_body<KIND, HDB, true>(A, B, PX, m, ax1, ay1, az1, q, psprow, f, a[1]);
+  }
+  if (i1 & 1) {
+    const float4 A = PA[m1], B = PB[m1];
+    pair_body<KIND, HDB, false>(A, B, PX, m1, ax0, ay0, az0, q, psprow, f, a[0]);
+    pair_body<KIND, HDB, false>(A, B, PX, m1, ax1, ay1, az1, q, psprow, f, a[1]);
+  }
+}
+
 /* Per-replica state of the CTA's slots, in shared memory. */
 struct Slot {
   int rep, lig_conf, accept, n_acc;
@@ -250,13 +277,17 @@ __device__ __forceinline__ double warp_sum(double v) {
 
 /* One segment range of the pair loop, dispatched on the segment kind: bits 0-1 point kind,
  * bit 2 live hydrogen-bond term. */
-template <int UNROLL>
+template <int UNROLL, int PACK>
 __device__ __forceinline__ void pair_dispatch(int kind, const float4 *PA, const float4 *PB,
-                                              const float4 *PX, int i0, int i1, float ax,
-                                              float ay, float az, const Pair2 &pq,
+                                              const float4 *PX, int i0, int i1, const float *ax,
+                                              const float *ay, const float *az, const Pair2 &pq,
                                               const float *psprow, const GdForceConst &f,
-                                              Acc &acc) {
-#define GD_PR(K, H) pair_range<K, H, UNROLL>(PA, PB, PX, i0, i1, ax, ay, az, pq, psprow, f, acc)
+                                              Acc *acc) {
+#define GD_PR(K, H)                                                                          \
+  if constexpr (PACK == 2)                                                                   \
+    pair_range2<K, H, UNROLL>(PA, PB, PX, i0, i1, ax, ay, az, pq, psprow, f, acc);          \
+  else                                                                                       \
+    pair_range<K, H, UNROLL>(PA, PB, PX, i0, i1, ax[0], ay[0], az[0], pq, psprow, f, acc[0])
   switch (kind) {
     case 0: GD_PR(0, false); break;
     case 1: GD_PR(1, false); break;
@@ -332,11 +363,14 @@ __device__ __forceinline__ void da_decide(const GdMcArgs &a, const GdDevComplex 
  * chunk two ahead. Every wait is bounded (globaltimer); a wait that runs out sets the error
  * word, the CTA leaves at the next step barrier after letting its copies in flight land.
  */
-template <int UNROLL, bool SPLIT, bool DA>
-__global__ void __launch_bounds__(GD_MAX_TPB, GD_MIN_BLOCKS(UNROLL))
+template <int UNROLL, bool SPLIT, bool DA, int PACK>
+__global__ void __launch_bounds__(GD_MAX_TPB / PACK, GD_MIN_BLOCKS_PACK(UNROLL, PACK))
     gd_mc_kernel(GdMcArgs a, GdForceConst f) {
+  static_assert(PACK == 1 || (PACK == 2 && !SPLIT && !DA),
+                "two replicas per lane: plain modes with one lane per atom");
   extern __shared__ __align__(16) unsigned char smem[];
-  const int T = blockDim.x, tid = threadIdx.x, D = a.chunk;
+  /* T: lanes of the tile (PACK per thread), the stride of the placed atoms and partials */
+  const int NT = blockDim.x, T = NT * PACK, tid = threadIdx.x, D = a.chunk;
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem);
   /* ring buffers: buffer b holds D slots as D/2 pairs in three float4 streams */
   float4 *bpa = reinterpret_cast<float4 *>(smem + 16);
@@ -360,9 +394,9 @@ __global__ void __launch_bounds__(GD_MAX_TPB, GD_MIN_BLOCKS(UNROLL))
   __syncthreads();
   uint32_t consumed0 = 0, consumed1 = 0; /* completed phases waited for, per buffer */
   const int step_first = a.step0 + (a.step_base ? *a.step_base : 0);
-  const int warp = tid >> 5, lane = tid & 31, nwarps = T >> 5;
+  const int warp = tid >> 5, lane = tid & 31, nwarps = NT >> 5;
   if (DA && a.mode == 3 && blockIdx.x == 0)
-    for (int g = a.da_g0 + tid; g < a.da_g1; g += T) a.da_cnt_next[g] = 0;
+    for (int g = a.da_g0 + tid; g < a.da_g1; g += NT) a.da_cnt_next[g] = 0;
 
   for (;;) {
     if (tid == 0) s_tile = atomicAdd(a.tile_counter, 1);
@@ -386,10 +420,23 @@ __global__ void __launch_bounds__(GD_MAX_TPB, GD_MIN_BLOCKS(UNROLL))
     /* lane = (slot j, protein split sp, ligand atom l): the S copies of an atom each walk
      * 1/S of every protein segment; S = 1 is one lane per atom */
     const int L = cx.lna, S = SPLIT ? a.split : 1, SL = S * L;
-    const bool active = tid < k * SL;
-    const int j = active ? tid / SL : 0;
-    const int sp = active ? (tid - j * SL) / L : 0;
-    const int l = active ? tid - j * SL - sp * L : 0;
+    const int kp = (k + PACK - 1) / PACK; /* lane groups */
+    const bool active = tid < kp * SL;
+    const int jj = active ? tid / SL : 0;
+    const int sp = active ? (tid - jj * SL) / L : 0;
+    const int l = active ? tid - jj * SL - sp * L : 0;
+    /* the thread's lanes: slot jj (PACK 1), or slots 2 jj and 2 jj + 1, the same atom of two
+     * replicas (PACK 2); a missing second slot (odd k) repeats the first one's atom and stores
+     * nothing. sl_of: each lane's slot; vl: its index in the placed-atom and partial arrays */
+    int sl_of[PACK], vl[PACK];
+    bool ok[PACK];
+#pragma unroll
+    for (int h = 0; h < PACK; ++h) {
+      const int jh = jj * PACK + h;
+      ok[h] = active && jh < k;
+      sl_of[h] = ok[h] ? jh : jj * PACK;
+      vl[h] = sl_of[h] * SL + sp * L + l;
+    }
 
     /* ---- slot set-up (one thread per replica) ---- */
     if (tid < k) {
@@ -441,9 +488,11 @@ __global__ void __launch_bounds__(GD_MAX_TPB, GD_MIN_BLOCKS(UNROLL))
     __syncthreads();
 
     /* ---- per-lane constants ---- */
-    const int lig_conf = slots[j].lig_conf;
-    const float4 orig = cx.lig_pos[lig_conf * L + l];
-    const int tl = cx.lig_meta[lig_conf * L + l].x;
+    float4 orig[PACK];
+#pragma unroll
+    for (int h = 0; h < PACK; ++h) orig[h] = cx.lig_pos[slots[sl_of[h]].lig_conf * L + l];
+    /* atom types are the same in every conformer of a ligand when PACK is 2 (host-checked) */
+    const int tl = cx.lig_meta[slots[sl_of[0]].lig_conf * L + l].x;
     const float *psprow = cx.psp + (size_t)tl * cx.psp_ld;
     const GdPairParam *pprow = a.pp + tl * GD_MAXTP1;
     const int4 *segs = cx.seg + pc * GD_MAX_SEG;
@@ -481,15 +530,23 @@ __global__ void __launch_bounds__(GD_MAX_TPB, GD_MIN_BLOCKS(UNROLL))
         sl.u = u;
       }
       __syncthreads();
-      float ax = 0.0f, ay = 0.0f, az = 0.0f;
-      if (active) {
-        const Slot &sl = slots[j];
-        gd_place_atom(sl.rot, sl.tx, sl.ty, sl.tz, orig.x, orig.y, orig.z, &ax, &ay, &az);
-        atoms[tid] = make_float4(ax, ay, az, 0.0f);
+      float ax[PACK], ay[PACK], az[PACK];
+#pragma unroll
+      for (int h = 0; h < PACK; ++h) {
+        ax[h] = ay[h] = az[h] = 0.0f;
+        if (active) {
+          const Slot &sl = slots[sl_of[h]];
+          gd_place_atom(sl.rot, sl.tx, sl.ty, sl.tz, orig[h].x, orig[h].y, orig[h].z, &ax[h],
+                        &ay[h], &az[h]);
+          if (ok[h]) atoms[vl[h]] = make_float4(ax[h], ay[h], az[h], 0.0f);
+        }
       }
 #pragma unroll
-      for (int qi = 0; qi < NQ; ++qi) part[qi * T + tid] = 0.0;
-      int ncon = 0;
+      for (int qi = 0; qi < NQ; ++qi)
+        for (int i = tid; i < T; i += NT) part[qi * T + i] = 0.0;
+      int ncon[PACK];
+#pragma unroll
+      for (int h = 0; h < PACK; ++h) ncon[h] = 0;
 
       /* ---- CalcEnergy_d pair loop over the protein ring ---- */
       for (int ci = 0; ci < nch; ++ci) {
@@ -530,15 +587,22 @@ __global__ void __launch_bounds__(GD_MAX_TPB, GD_MIN_BLOCKS(UNROLL))
             pq.pmf1 = f2(q1.y); pq.hc1 = f2(q1.z); pq.hc0 = f2(q1.w);
             pq.hs = f2(q2.x); pq.b2 = f2(q2.z); pq.c2 = f2(q2.w);
             const float2 z2 = f2(0.0f);
-            Acc acc = {z2, z2, z2, z2, z2, z2, 0.0f};
-            pair_dispatch<UNROLL>(g.w, PA, PB, PX, i0, i1, ax, ay, az, pq, psprow, f, acc);
-            part[0 * T + tid] += (double)acc.vdw.x + (double)acc.vdw.y;
-            part[1 * T + tid] += (double)acc.ele.x + (double)acc.ele.y;
-            part[2 * T + tid] += (double)acc.pmf.x + (double)acc.pmf.y;
-            part[3 * T + tid] += (double)acc.psp;
-            part[4 * T + tid] += (double)acc.hdb.x + (double)acc.hdb.y;
-            part[5 * T + tid] += (double)acc.hsum.x + (double)acc.hsum.y;
-            ncon += (int)(acc.ncon.x + acc.ncon.y);
+            Acc acc[PACK];
+#pragma unroll
+            for (int h = 0; h < PACK; ++h) acc[h] = {z2, z2, z2, z2, z2, z2, 0.0f};
+            pair_dispatch<UNROLL, PACK>(g.w, PA, PB, PX, i0, i1, ax, ay, az, pq, psprow, f, acc);
+#pragma unroll
+            for (int h = 0; h < PACK; ++h) {
+              if (!ok[h]) continue;
+              const int v = vl[h];
+              part[0 * T + v] += (double)acc[h].vdw.x + (double)acc[h].vdw.y;
+              part[1 * T + v] += (double)acc[h].ele.x + (double)acc[h].ele.y;
+              part[2 * T + v] += (double)acc[h].pmf.x + (double)acc[h].pmf.y;
+              part[3 * T + v] += (double)acc[h].psp;
+              part[4 * T + v] += (double)acc[h].hdb.x + (double)acc[h].hdb.y;
+              part[5 * T + v] += (double)acc[h].hsum.x + (double)acc[h].hsum.y;
+              ncon[h] += (int)(acc[h].ncon.x + acc[h].ncon.y);
+            }
           }
         }
         if (!resident) {
@@ -573,36 +637,38 @@ __global__ void __launch_bounds__(GD_MAX_TPB, GD_MIN_BLOCKS(UNROLL))
             part[5 * T + tid + q * L] = 0.0;
           }
       }
-      if (active && !aborted) {
-        part[1 * T + tid] *= (double)orig.w;
-        part[8 * T + tid] = (double)ncon;
-      }
-      if (active && !aborted && sp == 0) {
-        const double hpc2 = (part[5 * T + tid] - (double)f.hpl0[tl]) / (double)f.hpl1[tl];
-        part[5 * T + tid] = 0.5 * hpc2 * hpc2 - (double)f.hpl2[tl];
+#pragma unroll
+      for (int h = 0; h < PACK; ++h) {
+        if (!ok[h] || aborted) continue;
+        const int v = vl[h];
+        part[1 * T + v] *= (double)orig[h].w;
+        part[8 * T + v] = (double)ncon[h];
+        if (sp != 0) continue;
+        const double hpc2 = (part[5 * T + v] - (double)f.hpl0[tl]) / (double)f.hpl1[tl];
+        part[5 * T + v] = 0.5 * hpc2 * hpc2 - (double)f.hpl2[tl];
         float ks = 0.0f;
         int kn = 0;
         for (int kk = 0; kk < cx.pnk; ++kk) {
           const float4 kd = __ldg(cx.kde + kk);
           if ((int)kd.w == tl) {
-            const float dx = ax - kd.x, dy = ay - kd.y, dz = az - kd.z;
+            const float dx = ax[h] - kd.x, dy = ay[h] - kd.y, dz = az[h] - kd.z;
             ks += expf(f.kde2 * (dx * dx + dy * dy + dz * dz));
             ++kn;
           }
         }
-        part[6 * T + tid] = kn ? (double)ks / (double)kn : 0.0;
-        const Slot &sl = slots[j];
+        part[6 * T + v] = kn ? (double)ks / (double)kn : 0.0;
+        const Slot &sl = slots[sl_of[h]];
         const float *lc = cx.lig_center + sl.lig_conf * 3;
-        const float rx = ax - (orig.x + lc[0]), ry = ay - (orig.y + lc[1]),
-                    rz = az - (orig.z + lc[2]);
-        part[7 * T + tid] = (double)(rx * rx + ry * ry + rz * rz);
+        const float rx = ax[h] - (orig[h].x + lc[0]), ry = ay[h] - (orig[h].y + lc[1]),
+                    rz = az[h] - (orig[h].z + lc[2]);
+        part[7 * T + v] = (double)(rx * rx + ry * ry + rz * rz);
         int tp = 0;
         const int *rs = cx.ref_start + pc * (L + 1);
         for (int i = rs[l]; i < rs[l + 1]; ++i) {
           const float4 rp = __ldg(cx.ref_pts + i);
-          tp += dist2(ax, ay, az, rp.x, rp.y, rp.z) <= rp.w ? 1 : 0;
+          tp += dist2(ax[h], ay[h], az[h], rp.x, rp.y, rp.z) <= rp.w ? 1 : 0;
         }
-        part[9 * T + tid] = (double)tp;
+        part[9 * T + v] = (double)tp;
       }
       if (__syncthreads_or(aborted)) {
         aborted = true;
@@ -747,12 +813,15 @@ __global__ void __launch_bounds__(GD_MAX_TPB, GD_MIN_BLOCKS(UNROLL))
 }
 
 /* the kernel variants the host can launch: point pairs in flight per lane; protein split
- * and the delayed-acceptance exact stage (mode 3) compiled out when false */
-#define GD_INST(U, S, D) template __global__ void gd_mc_kernel<U, S, D>(GdMcArgs, GdForceConst);
-GD_INST(1, false, false) GD_INST(2, false, false) GD_INST(4, false, false)
-GD_INST(1, true, false) GD_INST(2, true, false) GD_INST(4, true, false)
-GD_INST(1, false, true) GD_INST(2, false, true) GD_INST(4, false, true)
-GD_INST(1, true, true) GD_INST(2, true, true) GD_INST(4, true, true)
+ * and the delayed-acceptance exact stage (mode 3) compiled out when false; replicas per
+ * thread (two only for the plain modes without split) */
+#define GD_INST(U, S, D, P) \
+  template __global__ void gd_mc_kernel<U, S, D, P>(GdMcArgs, GdForceConst);
+GD_INST(1, false, false, 1) GD_INST(2, false, false, 1) GD_INST(4, false, false, 1)
+GD_INST(1, true, false, 1) GD_INST(2, true, false, 1) GD_INST(4, true, false, 1)
+GD_INST(1, false, true, 1) GD_INST(2, false, true, 1) GD_INST(4, false, true, 1)
+GD_INST(1, true, true, 1) GD_INST(2, true, true, 1) GD_INST(4, true, true, 1)
+GD_INST(1, false, false, 2) GD_INST(2, false, false, 2)
 #undef GD_INST
 
 /* ExchangeReplicas_d, one thread per (complex, protein conformer, ligand conformer) group of

@@ -197,12 +197,14 @@ class Engine:
         check(lib().gd_sync(self.h))
 
     def set_tile(self, replicas_per_cta: int, chunk_points: int, unroll: int = 0,
-                 split: int = 0, threads: int = 0, complex_index: int = -1):
+                 split: int = 0, threads: int = 0, replicas_per_lane: int = 1,
+                 complex_index: int = -1):
         """threads > 0: every complex gets as many replicas as fill a CTA of that size
-        (replicas_per_cta > 0 caps them)."""
+        (replicas_per_cta > 0 caps them); replicas_per_lane 2: each thread of the plain launches
+        holds the same atom of two replicas."""
         t = abi.Tile()
         t.replicas_per_cta, t.chunk_points, t.unroll = replicas_per_cta, chunk_points, unroll
-        t.split, t.threads = split, threads
+        t.split, t.threads, t.replicas_per_lane = split, threads, replicas_per_lane
         check(lib().gd_set_tile(self.h, complex_index, C.byref(t)))
 
     def cuda_stream(self) -> int:
@@ -226,11 +228,12 @@ class Engine:
         return n.value
 
     def tile(self, complex_index=0):
-        """The tile as set: (replicas_per_cta, chunk_points, unroll, split, threads); in fill
-        mode (threads > 0) replicas_per_cta is the cap (0: none)."""
+        """The tile as set: (replicas_per_cta, chunk_points, unroll, split, threads,
+        replicas_per_lane); in fill mode (threads > 0) replicas_per_cta is the cap (0: none)."""
         t = abi.Tile()
         check(lib().gd_get_tile(self.h, complex_index, C.byref(t)))
-        return t.replicas_per_cta, t.chunk_points, t.unroll, t.split, t.threads
+        return (t.replicas_per_cta, t.chunk_points, t.unroll, t.split, t.threads,
+                t.replicas_per_lane)
 
     # ---- results ----
     def records(self, r0=0, r1=None):

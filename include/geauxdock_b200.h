@@ -174,6 +174,12 @@ typedef struct {
                                complex gets as many replicas as fill the CTA (at most
                                replicas_per_cta when that is > 0): a ragged batch keeps its
                                lanes busy whatever its ligands' sizes. */
+  int replicas_per_lane;    /* 0 or 1: a thread holds one lane; 2: a thread holds the same
+                               atom of two replicas (the plain Monte Carlo, init and pose
+                               evaluation launches; split 1, every ligand conformer with the same
+                               atom types), sharing each protein point's loads and pair
+                               parameters, on half as many threads. Energies are bit-identical
+                               to one replica per lane. */
 } gd_tile;
 
 /* Per-replica Monte Carlo state (checkpoint unit). */

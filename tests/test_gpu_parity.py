@@ -251,7 +251,7 @@ def test_fill_tile_gives_each_complex_its_own_replica_count(raw):
         ks = [b.replicas_per_cta(i) for i in range(len(w.complexes))]
         for i, cx in enumerate(w.complexes):
             assert ks[i] == min(cx.n_tmp * cx.n_lig, 256 // cx.lna), (i, ks[i], cx.lna)
-        assert b.tile() == (0, 256, 2, 1, 256)
+        assert b.tile() == (0, 256, 2, 1, 256, 1)
         for e in (a, b):
             e.mc_init()
             e.run_fused(0, 20, exchange=True)
@@ -371,8 +371,8 @@ def test_autotune_picks_a_tile_and_keeps_the_chains(raw, tmp_path):
         before = eng.state()
         res = autotune.tune(eng, cache_path=str(tmp_path / "cache.json"), repeats=1)
         assert not res["cached"]
-        k, ch, u, sp, thr = eng.tile()
-        assert [k, ch, u, sp] == res["tile"][:4] and sp == 1
+        k, ch, u, sp, thr, pk = eng.tile()
+        assert [k, ch, u, sp, pk] == res["tile"][:4] + res["tile"][5:] and sp == 1
         assert all(m > 0 or m == -1 for m in res["ms"].values())
         after = eng.state()
         assert np.array_equal(before.view(np.uint8), after.view(np.uint8))
@@ -485,3 +485,49 @@ def test_config2_extreme_shapes_against_oracle(raw, chunk):
                 assert abs(got["rmsd"] - o["rmsd"]) <= 1e-5 * max(1.0, o["rmsd"])
     report("config-2 extremes, chunk %d" % chunk, sumabs, plain)
     assert sumabs.max() <= TOL, sumabs
+
+
+@pytest.mark.parametrize("cfg", [0, 2])
+def test_two_replicas_per_lane_is_bit_identical(raw, cfg):
+    """Two replicas per thread (the same atom of two slots sharing each point's loads) gives
+    the chains, records and pose energies of one replica per lane bit for bit: config 0 with an
+    odd replica count per CTA (the last thread's second slot empty), and a ragged config-2
+    batch in fill mode."""
+    if cfg == 0:
+        w = system.config(0, raw)
+        tiles = ((5, 512, 1, 1, 0, 1), (5, 512, 1, 1, 0, 2), (5, 512, 2, 1, 0, 2))
+    else:
+        w = system.config(2, raw, n_ligands=6)
+        tiles = ((0, 256, 1, 1, 256, 1), (0, 256, 1, 1, 256, 2), (0, 256, 2, 1, 256, 2))
+    params = w.params
+    params.steps_per_dump = 40
+    states, recs, energies = [], [], []
+    mm = np.random.default_rng(3).normal(0, 1.0, (9, 6)).astype(np.float32)
+    for t in tiles:
+        with engine.Engine(w.ff, w.complexes, params) as e:
+            e.set_tile(*t)
+            assert e.tile()[5] == t[5]
+            e.mc_init()
+            e.run_fused(0, 20, exchange=True)
+            e.mc_run(20, 0)
+            e.exchange(1)
+            e.sync()
+            states.append(e.state().tobytes())
+            r, n = e.records()
+            recs.append((r.tobytes(), n.tobytes()))
+            ci = len(w.complexes) - 1
+            ip = min(1, w.complexes[ci].n_prt - 1)
+            energies.append(e.eval_energy(ci, ip, 2, mm).tobytes())
+    for i in (1, 2):
+        assert states[i] == states[0], tiles[i]
+        assert recs[i] == recs[0], tiles[i]
+        assert energies[i] == energies[0], tiles[i]
+
+
+def test_two_replicas_per_lane_rejects_what_it_cannot_take(raw):
+    z, cx, ff = load_ref("1a07C1")
+    with engine.Engine(ff, [cx], abi.mc_params()) as e:
+        with pytest.raises(engine.GDError):
+            e.set_tile(2, 256, 1, 2, 0, 2)  # split 2
+        e.set_tile(6, 256, 1, 1, 0, 2)
+        assert e.tile()[5] == 2 and e.replicas_per_cta(0) == 6
