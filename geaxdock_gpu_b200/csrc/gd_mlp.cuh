@@ -2,7 +2,7 @@
  * gd_mlp.cuh -- the energy surrogate: a 64 -> H -> H -> H -> 1 SiLU MLP with a learned
  * conformer embedding, BF16 weights and activations on the tensor cores, FP32 accumulation,
  * FP32 master parameters and Adam moments. Internal C++ interface shared by gd_mlp.cu (the
- * kernels) and gd_capi.cu (delayed acceptance).
+ * kernels) and gd_capi_da.cu (delayed acceptance).
  *
  * Input row (64 features): [0,3) ligand centre minus pocket centre / 4 A, [3,7) unit
  * quaternion of the pose rotation (w >= 0), [7,39) conformer embedding (32, learned, one row
