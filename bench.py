@@ -26,6 +26,9 @@ delayed_acceptance (N = 1): the config-3 workload on the config-1 system (2,000 
            and 60x larger moves; surrogate RMSE, stage acceptances, per-temperature KS p-values.
 batched_screen (N = 1): config 2 (2,048 uneven ligands x 8 uneven pockets, 1,048,576 replicas)
            in one context, one persistent launch per 10-step interval, autotuned tile.
+delayed_acceptance.sampling_efficiency (N = 1): effective samples per second (integrated
+           autocorrelation time of every chain's energy) of plain Monte Carlo and of delayed
+           acceptance, each at its best move scale of x1 / x5 / x20 / x60.
 screen_delayed_acceptance (N = 1): config 4, delayed acceptance on that screen with one network
            per pocket, against the plain batched run from the same state, at the configured and
            at 20x larger moves; best-pose energy and RMSD agreement per ligand.
@@ -362,6 +365,127 @@ def delayed_acceptance(w, dev, tile, scale_mult, intervals, burn=2000, iters=166
             "intervals": intervals, "ms_per_interval": da_ms / intervals,
             "gpu_launches_per_interval": 3 + 5 * spe + 1,
             "timing": "CUDA events on each engine's stream, L2 flushed between intervals"}
+
+
+def integrated_autocorr_time(x, c=5.0):
+    """Integrated autocorrelation time of each row of x [chains, steps] (Sokal's automatic
+    window: the smallest M with M >= c tau(M), tau(M) = 1 + 2 sum_{k=1..M} rho(k)); a chain
+    that never moves has tau = steps. FFT autocovariance, float64."""
+    x = np.asarray(x, np.float64)
+    n = x.shape[1]
+    y = x - x.mean(axis=1, keepdims=True)
+    nf = 1 << int(np.ceil(np.log2(2 * n)))
+    f = np.fft.rfft(y, nf, axis=1)
+    acov = np.fft.irfft(f * np.conj(f), nf, axis=1)[:, :n]
+    var = acov[:, 0]
+    tau = np.full(x.shape[0], float(n))
+    ok = var > 0
+    rho = acov[ok] / var[ok, None]
+    t = 2.0 * np.cumsum(rho, axis=1) - 1.0  # tau(M) for M = 0..n-1
+    m = np.arange(n)[None, :]
+    win = np.argmax(m >= c * t, axis=1)
+    found = (m >= c * t).any(axis=1)
+    tau_ok = np.where(found, t[np.arange(t.shape[0]), win], float(n))
+    tau[ok] = np.clip(tau_ok, 1.0, float(n))
+    return tau
+
+
+def _energy_series(e0, e_prop, took):
+    """Each chain's current energy after every step: the proposal's where it was taken."""
+    cur = np.array(e0, np.float32)
+    out = np.empty(e_prop.shape, np.float32)
+    for t in range(e_prop.shape[1]):
+        cur = np.where(took[:, t], e_prop[:, t], cur)
+        out[:, t] = cur
+    return out
+
+
+def sampling_efficiency(w, dev, tile, scales=(1.0, 5.0, 20.0, 60.0), burn=1000, n=2000,
+                        iters=1665):
+    """Effective samples per second of plain Monte Carlo and of delayed acceptance on the
+    config-1 system, each at its best move scale. Per scale: `burn` steps with exchange from
+    the initial poses (for delayed acceptance these are the surrogate's collect steps, the same
+    trajectory), one epoch of training, then `n` steps without exchange (every replica a
+    chain at a fixed temperature) with each chain's energy traced; the integrated
+    autocorrelation time tau of each chain's energy gives n / tau effective samples, summed
+    over the chains and divided by the device time of the n steps (CUDA events)."""
+    import torch
+    from geaxdock_gpu_b200 import engine
+    cx, ff = w.complexes[0], w.ff
+    rows = []
+    for m in scales:
+        p = type(w.params).from_buffer_copy(w.params)
+        p.record = 0
+        for i in range(6):
+            p.move_scale[i] = w.params.move_scale[i] * m
+        row = {"move_mult": m}
+        with engine.Engine(ff, [cx], p, device=dev) as a:
+            a.set_tile(*tile)
+            a.mc_init()
+            a.run_fused(0, burn, exchange=True)
+            s0 = burn + 10
+            a.trace_enable(s0 + n)  # absolute steps 0 .. s0 + n - 1
+            a.run_fused(burn, 10, exchange=False)  # builds the 10-step graph
+            a.sync()
+            e0 = a.state()["energy_old"]["e"][:, 9].copy()
+            st = torch.cuda.ExternalStream(a.cuda_stream(), device=dev)
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+            ev[0].record(st)
+            for s in range(s0, s0 + n, 10):
+                a.run_fused(s, 10, exchange=False)
+            ev[1].record(st)
+            a.sync()
+            ms = ev[0].elapsed_time(ev[1])
+            te, ta = a.trace()
+            te, ta = te[:, s0:], ta[:, s0:]
+            ser = _energy_series(e0, te, ta == 1)
+            tau = integrated_autocorr_time(ser)
+            row["plain"] = {"accept": float((ta == 1).mean()), "ms": ms,
+                            "tau_median": float(np.median(tau)),
+                            "ess_per_s": float((n / tau).sum() / (ms * 1e-3))}
+        with engine.Engine(ff, [cx], p, device=dev) as b:
+            b.set_tile(*tile)
+            b.mc_init()
+            sur = engine.Surrogate(b, sample_cap=burn * cx.n_rep, fallback_accept=0.0)
+            sur.collect(0, burn, exchange=True)
+            sur.train(iters)
+            s0 = burn + 20
+            sur.trace_enable(s0, n)
+            # two untraced calls build the step graph and settle the exact stage's split
+            sur.run(burn, 10, exchange=False)
+            sur.run(burn + 10, 10, exchange=False)
+            b.sync()
+            e0 = b.state()["energy_old"]["e"][:, 9].copy()
+            st0 = sur.stats()[0]
+            st = torch.cuda.ExternalStream(b.cuda_stream(), device=dev)
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+            ev[0].record(st)
+            for s in range(s0, s0 + n, 10):
+                sur.run(s, 10, exchange=False)
+            ev[1].record(st)
+            b.sync()
+            ms = ev[0].elapsed_time(ev[1])
+            st1 = sur.stats()[0]
+            _, e_tr, f_tr = sur.trace()
+            ser = _energy_series(e0, e_tr, f_tr == 2)
+            tau = integrated_autocorr_time(ser)
+            passed = st1["passed"] - st0["passed"]
+            row["delayed_acceptance"] = {
+                "accept": float((f_tr == 2).mean()), "ms": ms,
+                "stage1_pass": passed / max(1, st1["proposed"] - st0["proposed"]),
+                "stage2_accept": (st1["accepted"] - st0["accepted"]) / max(1, passed),
+                "tau_median": float(np.median(tau)),
+                "ess_per_s": float((n / tau).sum() / (ms * 1e-3))}
+        rows.append(row)
+    bp = max(rows, key=lambda r: r["plain"]["ess_per_s"])
+    bd = max(rows, key=lambda r: r["delayed_acceptance"]["ess_per_s"])
+    return {"unit": "effective samples/s (sum over chains of n / tau_int of the energy)",
+            "steps_traced": n, "burn": burn, "scales": rows,
+            "plain_best": {"move_mult": bp["move_mult"], "ess_per_s": bp["plain"]["ess_per_s"]},
+            "da_best": {"move_mult": bd["move_mult"],
+                        "ess_per_s": bd["delayed_acceptance"]["ess_per_s"]},
+            "da_over_plain": bd["delayed_acceptance"]["ess_per_s"] / bp["plain"]["ess_per_s"],
+            "timing": "CUDA events on each engine's stream around the n traced steps"}
 
 
 def batched_screen(dev, w, intervals=3):
@@ -727,7 +851,8 @@ def run_ours(args, rank, world, local_rank):
     if world == 1 and not args.no_da:
         da = {"configured_moves": delayed_acceptance(w, dev, tile_used, 1.0, args.steps),
               "moves_x20": delayed_acceptance(w, dev, tile_used, 20.0, args.steps),
-              "moves_x60": delayed_acceptance(w, dev, tile_used, 60.0, args.steps)}
+              "moves_x60": delayed_acceptance(w, dev, tile_used, 60.0, args.steps),
+              "sampling_efficiency": sampling_efficiency(w, dev, tile_used)}
 
     screen = screen4 = None
     if world == 1 and not args.no_screen:
