@@ -28,7 +28,7 @@ batched_screen (N = 1): config 2 (2,048 uneven ligands x 8 uneven pockets, 1,048
            in one context, one persistent launch per 10-step interval, autotuned tile.
 delayed_acceptance.sampling_efficiency (N = 1): effective samples per second (integrated
            autocorrelation time of every chain's energy) of plain Monte Carlo and of delayed
-           acceptance, each at its best move scale of x1 / x5 / x20 / x60.
+           acceptance, each at its best move scale of x1 / x5 / x20 / x40 / x60 / x100.
 screen_delayed_acceptance (N = 1): config 4, delayed acceptance on that screen with one network
            per pocket, against the plain batched run from the same state, at the configured and
            at 20x larger moves; best-pose energy and RMSD agreement per ligand.
@@ -400,7 +400,7 @@ def _energy_series(e0, e_prop, took):
     return out
 
 
-def sampling_efficiency(w, dev, tile, scales=(1.0, 5.0, 20.0, 60.0), burn=1000, n=2000,
+def sampling_efficiency(w, dev, tile, scales=(1.0, 5.0, 20.0, 40.0, 60.0, 100.0), burn=1000, n=2000,
                         iters=1665):
     """Effective samples per second of plain Monte Carlo and of delayed acceptance on the
     config-1 system, each at its best move scale. Per scale: `burn` steps with exchange from

@@ -99,7 +99,8 @@ def _chain(rng, n, n_conf):
     out = np.zeros((n_conf, n, 3))
     for c in range(n_conf):
         x = np.zeros((n, 3))
-        x[1] = [bond, 0, 0]
+        if n > 1:
+            x[1] = [bond, 0, 0]
         if n > 2:
             x[2] = x[1] + bond * np.array([-math.cos(ang), math.sin(ang), 0.0])
         for i in range(3, n):

@@ -531,3 +531,49 @@ def test_two_replicas_per_lane_rejects_what_it_cannot_take(raw):
             e.set_tile(2, 256, 1, 2, 0, 2)  # split 2
         e.set_tile(6, 256, 1, 1, 0, 2)
         assert e.tile()[5] == 2 and e.replicas_per_cta(0) == 6
+
+
+def test_largest_and_smallest_complexes_against_oracle(raw):
+    """The capacities the C ABI accepts, batched in one context: a ligand of GD_MAXLIG = 100
+    atoms against GD_MAXPRO = 10,000 protein points at GD_MAXTMP = 40 temperatures with 3,000
+    KDE points and 20 MCS positions, next to a one-atom ligand against a one-point protein.
+    Every term, cms and rmsd of given poses and of the initial poses against the FP64 oracle,
+    with the default tile and with the 256-lane fill tile; ten Monte Carlo steps stay finite."""
+    rng = np.random.default_rng(77)
+    ff = system.forcefield(raw, 42)
+    big = system.make_complex(rng, ff, L=abi.MAXLIG, n_lig=2, P=abi.MAXPRO, n_prt=1,
+                              n_tmp=abi.MAXTMP, K=3000, M=20)
+    small = system.make_complex(rng, ff, L=1, n_lig=2, P=1, n_prt=1, n_tmp=3, K=5, M=2,
+                                pocket=np.array([200.0, 0.0, 0.0]))
+    for m in range(small.pos):  # every MCS position restrains the single atom
+        small.mcs_x[m, 1], small.mcs_y[m, 1], small.mcs_z[m, 1] = 200.5, 0.3, -0.2
+    cxs = [big, small]
+    params = abi.mc_params(steps_per_exchange=10, steps_per_dump=20, seed=3)
+    sumabs = np.zeros(10)
+    for tile in ((0, 512, 2, 1, 0, 1), (0, 512, 1, 1, 256, 1)):
+        with engine.Engine(ff, cxs, params) as eng:
+            if tile[4] == 0:
+                eng.set_tile(2, 512, 2)
+            else:
+                eng.set_tile(*tile)
+            for ci, cx in enumerate(cxs):
+                rm = po.ref_map(ff, cx)
+                mm = np.zeros((6, 6), np.float32)
+                mm[:, :3] = rng.normal(0, 1.0, (6, 3))
+                mm[:, 3:] = rng.uniform(-3.1, 3.1, (6, 3))
+                for il in range(cx.n_lig):
+                    sumabs = np.maximum(sumabs, _energy_check(eng, ff, cx, ci, 0, il, mm, rm))
+            eng.mc_init()
+            eng.sync()
+            st = eng.state()
+            for ci, cx in enumerate(cxs):
+                rm = po.ref_map(ff, cx)
+                for r in range(0, cx.n_rep, 7):
+                    o = po.pose_energy(ff, cx, 0, r % cx.n_lig, np.zeros(6, np.float32), rm, 64)
+                    got = st["energy_old"][eng.offsets[ci] + r]
+                    sumabs = np.maximum(sumabs, rel_errors(got["e"], o, ff))
+                    assert abs(got["cms"] - o["cms"]) <= 2e-6
+            eng.run_fused(0, 10, exchange=True)
+            eng.sync()
+            assert np.all(np.isfinite(eng.etotal()))
+    assert sumabs.max() <= TOL, sumabs
