@@ -6,16 +6,20 @@
  * 256 reduction elements, so both operand tiles fit in shared memory at once (<= 128 KB) and
  * no stage is ever refilled:
  *
- *   thread 0   arms one mbarrier with the tiles' byte count, issues every TMA box load (2-D
- *              tiled cp.async.bulk.tensor, 128-byte swizzle, boxes 64 elements wide), waits for
- *              them (bounded), then issues K/16 tcgen05.mma (kind::f16, BF16 x BF16 -> FP32,
- *              M = 128, N = BN, K = 16) into a BN-column tensor-memory accumulator and commits
- *              them to a second mbarrier;
+ *   thread 0   issues every TMA box load (2-D tiled cp.async.bulk.tensor, 128-byte swizzle,
+ *              boxes 64 elements wide), each 64-wide slice of K completing on its own mbarrier,
+ *              and as each slice lands (bounded wait) issues its tcgen05.mma (kind::f16, BF16 x
+ *              BF16 -> FP32, M = 128, N = BN, K = 16) into a BN-column tensor-memory
+ *              accumulator, so the products of the first slices run while the later ones are
+ *              still in flight; the MMAs are committed to one more mbarrier;
  *   warp w     reads accumulator lanes 32 (w % 4)..+31 (rows) of column half w / 4 with
  *              tcgen05.ld.32x32b.x32, 32 columns at a time, turns the 32 x 32 block around in
  *              shared memory so that lanes run along a row (coalesced stores), and applies the
  *              epilogue (bias + SiLU into BF16 activations and FP32 pre-activations, the SiLU
  *              derivative for input gradients, or FP32 partial sums, optionally transposed).
+ *              The turn-around buffer reuses the operand tiles' shared memory once the MMAs
+ *              have completed, so a CTA needs only its two tiles: two BN = 64 CTAs share an SM
+ *              and one's epilogue overlaps the other's loads and products.
  *
  * Shared-memory operand layouts are the canonical swizzled forms the descriptors name:
  *   K-major  per 64-wide slice of K, rows x 128 bytes, 8-row groups 1024 bytes apart
@@ -28,6 +32,7 @@
  */
 #include <cuda.h> /* CUtensorMap and its enums; the encoder is fetched from the driver at run time */
 
+#include <algorithm>
 #include <atomic>
 #include <cstdint>
 
@@ -42,6 +47,7 @@ using bf16 = __nv_bfloat16;
 constexpr int BM = 128;
 constexpr long long WAIT_NS = 2000000000LL;
 constexpr int STAGE_BYTES = 8 * 32 * 33 * 4;
+constexpr int MAX_SLICES = 4; /* K <= 256 in slices of 64 */
 
 struct UmmaArgs {
   int M, N, K, a_mn, b_mn;
@@ -123,11 +129,26 @@ __device__ __forceinline__ uint64_t op_desc(uint32_t s, int mn, int rows_tile, i
                1u, 64u);
 }
 
-/* every box of one operand tile: K-major boxes are 64 (k) x rows_tile, MN-major 64 (mn) x K */
-__device__ __forceinline__ void load_tile(unsigned char *dst, const CUtensorMap *map, int mn,
-                                          int rows_tile, int K, int r0, int k0, uint64_t *bar) {
+/* K slices the loads complete on: 64 wide when K is a multiple of 64 (MN-major boxes are then
+ * 64 x 64 and land inside their block), else one slice with MN-major boxes K rows high */
+__host__ __device__ inline int k_slices(int K) { return (K % 64 == 0) ? K / 64 : 1; }
+
+/* bytes of slice s of an operand tile (a whole tile when there is one slice) */
+__device__ __forceinline__ uint32_t slice_bytes(int mn, int rows_tile, int K, int ns) {
+  if (ns == 1) return tile_bytes(mn, rows_tile, K);
+  return mn ? (uint32_t)(rows_tile / 64) * 8192u : (uint32_t)rows_tile * 128u;
+}
+
+/* the boxes of slice s of one operand tile: K-major boxes are 64 (k) x rows_tile; MN-major
+ * boxes 64 (mn) x 64 (k) at 64 s rows into each 64-wide block, or 64 (mn) x K for one slice */
+__device__ __forceinline__ void load_slice(unsigned char *dst, const CUtensorMap *map, int mn,
+                                           int rows_tile, int K, int r0, int k0, int s, int ns,
+                                           uint64_t *bar) {
   if (mn) {
-    for (int b = 0; b < rows_tile / 64; ++b) tma_2d(dst + (size_t)b * K * 128, map, r0 + 64 * b, k0, bar);
+    for (int b = 0; b < rows_tile / 64; ++b)
+      tma_2d(dst + (size_t)b * K * 128 + (size_t)s * 8192, map, r0 + 64 * b, k0 + 64 * s, bar);
+  } else if (ns > 1) {
+    tma_2d(dst + (size_t)s * rows_tile * 128, map, k0 + 64 * s, r0, bar);
   } else {
     for (int b = 0; b < (K + 63) / 64; ++b)
       tma_2d(dst + (size_t)b * rows_tile * 128, map, k0 + 64 * b, r0, bar);
@@ -135,11 +156,12 @@ __device__ __forceinline__ void load_tile(unsigned char *dst, const CUtensorMap 
 }
 
 template <int BN>
-__global__ void __launch_bounds__(256, 1)
+__global__ void __launch_bounds__(256, 2)
     umma_kernel(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb,
                 UmmaArgs g) {
   extern __shared__ unsigned char dsm[];
-  __shared__ __align__(8) uint64_t bar[2];
+  /* bar[0 .. MAX_SLICES - 1]: the K slices' loads; bar[MAX_SLICES]: the MMAs' commit */
+  __shared__ __align__(8) uint64_t bar[MAX_SLICES + 1];
   __shared__ uint32_t tmem_sh;
   __shared__ int ok_sh;
   __shared__ float cs[4][BN]; /* per-quadrant column sums (UMMA_DGRAD with colsum) */
@@ -147,8 +169,10 @@ __global__ void __launch_bounds__(256, 1)
   /* 1024-byte aligned operand tiles (the swizzle pattern is a function of the address) */
   unsigned char *base = dsm + ((1024u - (su32(dsm) & 1023u)) & 1023u);
   unsigned char *sa = base, *sb = base + tile_bytes(g.a_mn, BM, g.K);
-  unsigned char *sst = sb + tile_bytes(g.b_mn, BN, g.K); /* epilogue staging, 8 x 32 x 33 floats */
+  /* epilogue staging, 8 x 32 x 33 floats, over the operand tiles once the MMAs are done */
+  unsigned char *sst = base;
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN, k0 = blockIdx.z * g.K;
+  const int ns = k_slices(g.K);
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
@@ -158,8 +182,8 @@ __global__ void __launch_bounds__(256, 1)
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   if (tid == 32) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(&bar[0])) : "memory");
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(&bar[1])) : "memory");
+    for (int i = 0; i <= MAX_SLICES; ++i)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(&bar[i])) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   tc_fence_before();
@@ -168,22 +192,32 @@ __global__ void __launch_bounds__(256, 1)
   const uint32_t tmem = tmem_sh;
 
   if (tid == 0) {
-    const uint32_t bytes = tile_bytes(g.a_mn, BM, g.K) + tile_bytes(g.b_mn, BN, g.K);
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(&bar[0])),
-                 "r"(bytes)
-                 : "memory");
-    load_tile(sa, &ta, g.a_mn, BM, g.K, m0, k0, &bar[0]);
-    load_tile(sb, &tb, g.b_mn, BN, g.K, n0, k0, &bar[0]);
-    int ok = bar_wait(&bar[0], 0) ? 1 : 0;
-    if (ok) {
+    /* every slice's loads in flight first, each on its own barrier */
+    for (int sl = 0; sl < ns; ++sl) {
+      const uint32_t bytes =
+          slice_bytes(g.a_mn, BM, g.K, ns) + slice_bytes(g.b_mn, BN, g.K, ns);
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
+                       su32(&bar[sl])),
+                   "r"(bytes)
+                   : "memory");
+      load_slice(sa, &ta, g.a_mn, BM, g.K, m0, k0, sl, ns, &bar[sl]);
+      load_slice(sb, &tb, g.b_mn, BN, g.K, n0, k0, sl, ns, &bar[sl]);
+    }
+    /* kind::f16 instruction descriptor: FP32 accumulator, BF16 A and B, majors, N >> 3,
+     * M >> 4 */
+    const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)g.a_mn << 15) |
+                           ((uint32_t)g.b_mn << 16) | ((uint32_t)(BN >> 3) << 17) |
+                           ((uint32_t)(BM >> 4) << 24);
+    const uint32_t a_s = su32(sa), b_s = su32(sb);
+    const int steps = g.K / 16, per = ns > 1 ? 4 : steps;
+    int ok = 1;
+    for (int sl = 0; sl < ns && ok; ++sl) {
+      if (!bar_wait(&bar[sl], 0)) {
+        ok = 0;
+        break;
+      }
       tc_fence_after();
-      /* kind::f16 instruction descriptor: FP32 accumulator, BF16 A and B, majors, N >> 3,
-       * M >> 4 */
-      const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)g.a_mn << 15) |
-                             ((uint32_t)g.b_mn << 16) | ((uint32_t)(BN >> 3) << 17) |
-                             ((uint32_t)(BM >> 4) << 24);
-      const uint32_t a_s = su32(sa), b_s = su32(sb);
-      for (int ks = 0; ks < g.K / 16; ++ks) {
+      for (int ks = sl * per; ks < min(steps, (sl + 1) * per); ++ks) {
         const uint64_t ad = op_desc(a_s, g.a_mn, BM, g.K, ks);
         const uint64_t bd = op_desc(b_s, g.b_mn, BN, g.K, ks);
         asm volatile(
@@ -192,18 +226,23 @@ __global__ void __launch_bounds__(256, 1)
             "l"(ad), "l"(bd), "r"(idesc), "r"(ks > 0 ? 1 : 0)
             : "memory");
       }
+    }
+    if (ok) {
       asm volatile(
           "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-              su32(&bar[1]))
+              su32(&bar[MAX_SLICES]))
           : "memory");
     } else {
+      /* a slice never landed: let the loads still in flight finish (bounded) before the CTA
+       * reuses or gives up its shared memory */
+      for (int sl = 0; sl < ns; ++sl) bar_wait(&bar[sl], 0);
       atomicExch(g.err, 1);
     }
     ok_sh = ok;
   }
   __syncthreads();
   bool ok = ok_sh != 0;
-  if (ok && !bar_wait(&bar[1], 0)) {
+  if (ok && !bar_wait(&bar[MAX_SLICES], 0)) {
     ok = false;
     if (lane == 0) atomicExch(g.err, 2);
   }
@@ -331,20 +370,23 @@ int launch(const UmmaOperand &A, const UmmaOperand &B, int M, int N, int K, int 
   /* the shared-memory limit is a per-device attribute: set once per device */
   static std::atomic<unsigned long long> attr_set{0};
   const size_t smem =
-      tile_bytes(A.mn_major, BM, K) + tile_bytes(B.mn_major, BN, K) + STAGE_BYTES + 1024;
+      std::max<size_t>(tile_bytes(A.mn_major, BM, K) + tile_bytes(B.mn_major, BN, K),
+                       (size_t)STAGE_BYTES) + 1024;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return -2;
   const unsigned long long bit = 1ull << (dev & 63);
   if (!(attr_set.load() & bit)) {
     if (cudaFuncSetAttribute(umma_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             256 * 256 + BN * 512 + STAGE_BYTES + 1024) != cudaSuccess)
+                             256 * 256 + BN * 512 + 1024) != cudaSuccess)
       return -2;
     attr_set.fetch_or(bit);
   }
   CUtensorMap ta, tb;
   int rc;
-  if ((rc = make_map(&ta, A, A.mn_major ? K : BM))) return rc;
-  if ((rc = make_map(&tb, B, B.mn_major ? K : BN))) return rc;
+  /* MN-major boxes are one K slice high (the whole chunk when it is not a multiple of 64) */
+  const int mn_box = k_slices(K) > 1 ? 64 : K;
+  if ((rc = make_map(&ta, A, A.mn_major ? mn_box : BM))) return rc;
+  if ((rc = make_map(&tb, B, B.mn_major ? mn_box : BN))) return rc;
   UmmaArgs g;
   g.M = M;
   g.N = N;
@@ -367,8 +409,20 @@ int umma_gemm(const UmmaOperand &A, const UmmaOperand &B, int M, int N, int K, i
   if ((e.kind == UMMA_FWD && (!e.bias || !e.Ob)) || (e.kind == UMMA_DGRAD && (!e.Zin || !e.Ob)) ||
       (e.kind == UMMA_F32 && !e.Of))
     return -1;
-  return N <= 64 ? launch<64>(A, B, M, N, K, splits, e, err, s)
-                 : launch<128>(A, B, M, N, K, splits, e, err, s);
+  /* 64-wide tiles when 128-wide ones would leave fewer than two CTAs per SM: two 64-wide CTAs
+   * share an SM, and one's epilogue overlaps the other's loads and products */
+  static int num_sms = 0;
+  if (!num_sms) {
+    int dev = 0, n = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && n > 0)
+      num_sms = n;
+    else
+      num_sms = 148;
+  }
+  const long long tiles128 = (long long)((M + BM - 1) / BM) * ((N + 127) / 128) * splits;
+  return (N <= 64 || tiles128 < 2LL * num_sms) ? launch<64>(A, B, M, N, K, splits, e, err, s)
+                                               : launch<128>(A, B, M, N, K, splits, e, err, s);
 }
 
 }  // namespace gd
