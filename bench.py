@@ -972,13 +972,72 @@ def profile_mc(args):
     cx = w.complexes[0].subset(n_lig=8, n_prt=2, n_tmp=8)
     params = w.params
     params.record = 0
+    tile = tuple(int(v) for v in args.tile.split(",")) if args.tile else (6, 1024, 2)
     with engine.Engine(w.ff, [cx], params) as e:
-        e.set_tile(6, 1024, 2)
+        e.set_tile(*tile)
         e.mc_init()
         for it in range(4):
             e.mc_run(0, it * params.steps_per_exchange)
         e.sync()
-    print(json.dumps({"profile_mc": {"replicas": cx.n_rep, "launches": 4}}), flush=True)
+    print(json.dumps({"profile_mc": {"replicas": cx.n_rep, "launches": 4, "tile": tile}}),
+          flush=True)
+
+
+def sweep(args):
+    """Device time of one 10-step gd_mc_run on the config-1 system (no records): for each tile
+    of --sweep-tiles over all replicas, and, at the first of them, over the first m protein-
+    conformer blocks of 620 replicas (m = 1..11), with L2 flushed before every timed launch;
+    and the fused graph as 1..4 concurrent chains. Medians of 5 launches."""
+    import torch
+    from geaxdock_gpu_b200 import engine
+    w = workload(42)
+    cx, ff, p = w.complexes[0], w.ff, w.params
+    p.record = 0
+    tiles = [tuple(int(v) for v in t.split(",")) for t in args.sweep_tiles.split(";")]
+    out = {"tiles": {}, "blocks": {}, "chains": {}}
+    with engine.Engine(ff, [cx], p) as e:
+        e.mc_init()
+        e.sync()
+        st = torch.cuda.ExternalStream(e.cuda_stream())
+        flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda")
+        s = [0]
+
+        def timed(fn, reps=5):
+            fn()
+            fn()
+            ms = []
+            for _ in range(reps):
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                with torch.cuda.stream(st):
+                    flush.add_(1.0)
+                a.record(st)
+                fn()
+                b.record(st)
+                e.sync()
+                ms.append(a.elapsed_time(b))
+            return round(float(np.median(ms)), 3)
+
+        def run(r1=None):
+            def f():
+                e.mc_run(0, s[0], 0, r1)
+                s[0] += 10
+            return f
+
+        for t in tiles:
+            e.set_tile(*t)
+            out["tiles"][",".join(map(str, t))] = timed(run())
+        e.set_tile(*tiles[0])
+        block = cx.n_tmp * cx.n_lig
+        for m in range(1, cx.n_prt + 1):
+            out["blocks"][m] = timed(run(m * block - 1))
+        for ch in (1, 2, 3, 4):
+            e.set_concurrency(ch, 3)
+
+            def g():
+                e.run_fused(s[0], 10, exchange=True)
+                s[0] += 10
+            out["chains"][ch] = timed(g)
+    print(json.dumps({"sweep": out}), flush=True)
 
 
 def main():
@@ -1009,6 +1068,12 @@ def main():
     ap.add_argument("--profile-mc", action="store_true",
                     help="only a short plain run on a 128-replica subset of the config-1 system "
                          "(four 10-step launches), for multi-pass profiler captures")
+    ap.add_argument("--sweep", action="store_true",
+                    help="only the launch-time sweep over --sweep-tiles, replica blocks and "
+                         "concurrent chains on the config-1 system; prints its own JSON line")
+    ap.add_argument("--sweep-tiles", default="6,1024,2,1,0,1;6,1024,1,1,0,1;6,1024,2,1,0,2;"
+                                               "6,512,1,1,0,2;6,1024,1,1,0,2;6,2048,1,1,0,2",
+                    help="';'-separated tiles for --sweep")
     ap.add_argument("--screen-da", action="store_true",
                     help="only the config-4 run (delayed acceptance on the config-2 screen); "
                          "prints its own JSON line")
@@ -1031,6 +1096,9 @@ def main():
         return
     if args.profile_mc:
         profile_mc(args)
+        return
+    if args.sweep:
+        sweep(args)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
