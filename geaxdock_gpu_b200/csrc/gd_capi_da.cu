@@ -45,6 +45,7 @@ struct DaState {
   float *d_loss_hist = nullptr;
   int loss_cap = 0;
   long long train_iter = 0;
+  int *d_train_ctr = nullptr; /* [2]: the batch draws' iteration count, this call's loss slot */
   float *d_pred_mm = nullptr;
   int pred_cap = 0;
   float *tr_s = nullptr, *tr_e = nullptr;
@@ -671,14 +672,54 @@ int gd_sur_train(gd_ctx *c, int iterations, float *losses) {
   }
   gd::GdDaDev a = da_args(c);
   const int B = d->prm.batch;
-  for (int it = 0; it < iterations; ++it) {
-    gd::da_gather(a, start, n_valid, B, (int)(d->train_iter++), d->d_t, c->stream);
-    if (gd::mlp_embed(d->net, B, c->stream) || gd::mlp_loss_backward(d->net, B, d->d_t, c->stream))
-      return fail(GD_ERR_CUDA, "training step failed: %s", cudaGetErrorString(cudaGetLastError()));
-    CK(cudaMemcpyAsync(d->d_loss_hist + it, d->net.loss, sizeof(float), cudaMemcpyDeviceToDevice,
-                       c->stream));
-    if (gd::mlp_adam(d->net, d->prm.lr, c->stream))
-      return fail(GD_ERR_CUDA, "Adam step failed");
+  if (!d->d_train_ctr && (rc = da_alloc(d, &d->d_train_ctr, 2))) return rc;
+  /* One Adam step: batch draw, forward, loss, backward, Adam, the BF16 weight copies (about 30
+   * launches). Its per-step values live on the device (the draw's iteration count and the
+   * loss slot in d_train_ctr, Adam's step count in the network), so the step is run once
+   * eagerly -- which sets up every allocation and kernel attribute it needs -- then captured in
+   * a CUDA graph and replayed for the other steps, each replay one launch. */
+  if (iterations > 0) {
+    const int ctr[2] = {(int)d->train_iter, 0};
+    CK(cudaMemcpyAsync(d->d_train_ctr, ctr, sizeof(ctr), cudaMemcpyHostToDevice, c->stream));
+    if (gd::mlp_adam_dev_sync(d->net, c->stream)) return fail(GD_ERR_CUDA, "Adam step count");
+    auto step = [&]() -> int {
+      gd::da_gather(a, start, n_valid, B, d->d_train_ctr, d->d_t, c->stream);
+      if (gd::mlp_embed(d->net, B, c->stream) ||
+          gd::mlp_loss_backward(d->net, B, d->d_t, c->stream))
+        return fail(GD_ERR_CUDA, "training step failed: %s",
+                    cudaGetErrorString(cudaGetLastError()));
+      gd::da_train_tick(d->d_loss_hist, d->net.loss, d->d_train_ctr, c->stream);
+      if (gd::mlp_adam_dev(d->net, d->prm.lr, c->stream))
+        return fail(GD_ERR_CUDA, "Adam step failed");
+      return GD_OK;
+    };
+    if ((rc = step())) return rc;
+    if (iterations > 1) {
+      CK(cudaStreamSynchronize(c->stream));
+      cudaGraph_t graph = nullptr;
+      CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+      rc = step();
+      const cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
+      if (rc || ce != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc ? rc : fail(GD_ERR_CUDA, "training graph capture: %s", cudaGetErrorString(ce));
+      }
+      cudaGraphExec_t exec = nullptr;
+      const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ie != cudaSuccess)
+        return fail(GD_ERR_CUDA, "training graph instantiate: %s", cudaGetErrorString(ie));
+      cudaError_t le = cudaSuccess;
+      for (int it = 1; it < iterations && le == cudaSuccess; ++it)
+        le = cudaGraphLaunch(exec, c->stream);
+      const cudaError_t se = cudaStreamSynchronize(c->stream);
+      cudaGraphExecDestroy(exec);
+      if (le != cudaSuccess || se != cudaSuccess)
+        return fail(GD_ERR_CUDA, "training graph: %s",
+                    cudaGetErrorString(le != cudaSuccess ? le : se));
+    }
+    d->train_iter += iterations;
+    d->net.adam_t += iterations;
   }
   CK(cudaStreamSynchronize(c->stream));
   CK(cudaGetLastError());

@@ -262,10 +262,11 @@ __global__ void __launch_bounds__(256) stats_kernel(GdDaDev d, GdDaEpi e, const 
 }
 
 /* 8 threads per row, 16 bytes each */
-__global__ void gather_kernel(GdDaDev d, long long start, long long n_valid, int rows, int iter,
-                              float *t) {
+__global__ void gather_kernel(GdDaDev d, long long start, long long n_valid, int rows,
+                              const int *ctr, float *t) {
   const int row = blockIdx.x * (blockDim.x >> 3) + (threadIdx.x >> 3), part = threadIdx.x & 7;
   if (row >= rows) return;
+  const int iter = ctr[0];
   const gd_u32x4 h = gd_philox4x32_10((uint32_t)row, (uint32_t)iter, 0u, GD_RNG_TRAIN,
                                       (uint32_t)d.seed, (uint32_t)(d.seed >> 32));
   const unsigned long long rnd = ((unsigned long long)h.v[0] << 32) | h.v[1];
@@ -308,6 +309,12 @@ __global__ void moments_kernel(GdDaDev d, long long start, long long n_valid, fl
 
 inline int nblk(long long n, int t) { return (int)((n + t - 1) / t); }
 
+__global__ void train_tick_kernel(float *hist, const float *loss, int *ctr) {
+  hist[ctr[1]] = *loss;
+  ctr[0] += 1;
+  ctr[1] += 1;
+}
+
 }  // namespace
 
 int da_prepare(int hidden) {
@@ -343,9 +350,13 @@ void da_stats(const GdDaDev &d, const GdDaEpi &e_host, const GdDevComplex *cx_de
   stats_kernel<<<n_complex, 256, 0, s>>>(d, e_host, cx_dev, stats, err);
 }
 
-void da_gather(const GdDaDev &d, long long start, long long n_valid, int rows, int iter,
+void da_gather(const GdDaDev &d, long long start, long long n_valid, int rows, const int *ctr,
                float *t, cudaStream_t s) {
-  gather_kernel<<<nblk(rows, 32), 256, 0, s>>>(d, start, n_valid, rows, iter, t);
+  gather_kernel<<<nblk(rows, 32), 256, 0, s>>>(d, start, n_valid, rows, ctr, t);
+}
+
+void da_train_tick(float *hist, const float *loss, int *ctr, cudaStream_t s) {
+  train_tick_kernel<<<1, 1, 0, s>>>(hist, loss, ctr);
 }
 
 void da_target_moments(const GdDaDev &d, long long start, long long n_valid, float lo, float hi,

@@ -150,6 +150,30 @@ __global__ void adam_kernel(float *__restrict__ th, const float *__restrict__ g,
   th[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
 }
 
+/* the Adam step with its bias corrections read from c[0], c[1] (device) */
+__global__ void adam_dev_kernel(float *__restrict__ th, const float *__restrict__ g,
+                                float *__restrict__ m, float *__restrict__ v, size_t n, float lr,
+                                float b1, float b2, float eps, const float *__restrict__ c) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float c1 = c[0], c2 = c[1];
+  const float gi = g[i];
+  const float mi = b1 * m[i] + (1.0f - b1) * gi;
+  const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  th[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+/* advances the device step count t = st[0] and writes 1 - b1^t, 1 - b2^t as floats at st[1..2] */
+__global__ void adam_tick(int *st, float b1, float b2) {
+  const int t = st[0] + 1;
+  st[0] = t;
+  float *c = reinterpret_cast<float *>(st + 1);
+  c[0] = 1.0f - powf(b1, (float)t);
+  c[1] = 1.0f - powf(b2, (float)t);
+}
+
 __global__ void to_bf16(const float *__restrict__ a, bf16 *__restrict__ b, size_t n) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) b[i] = __float2bfloat16_rn(a[i]);
@@ -252,7 +276,7 @@ int mlp_create(Mlp &n, int hidden, int n_emb, uint64_t seed, cudaStream_t s) {
   const size_t T = n.L.total;
   if (cudaMalloc(&n.theta, T * 4) || cudaMalloc(&n.grad, T * 4) || cudaMalloc(&n.m, T * 4) ||
       cudaMalloc(&n.v, T * 4) || cudaMalloc(&n.wh, n.L.b4 * 2) || cudaMalloc(&n.loss, 16) ||
-      cudaMalloc(&n.err, sizeof(int)))
+      cudaMalloc(&n.err, sizeof(int)) || cudaMalloc(&n.adam_dev, 3 * sizeof(int)))
     return -3;
   cudaMemsetAsync(n.err, 0, sizeof(int), s);
   if ((hidden == 128 || hidden == 256) &&
@@ -282,7 +306,7 @@ int mlp_create(Mlp &n, int hidden, int n_emb, uint64_t seed, cudaStream_t s) {
 }
 
 void mlp_destroy(Mlp &n) {
-  void *ps[] = {n.theta, n.grad, n.m, n.v, n.wh, n.wf, n.loss, n.err, n.X, n.A1, n.A2, n.A3, n.D, n.D2, n.Pb,
+  void *ps[] = {n.theta, n.grad, n.m, n.v, n.wh, n.wf, n.loss, n.err, n.adam_dev, n.X, n.A1, n.A2, n.A3, n.D, n.D2, n.Pb,
                 n.Z1, n.Z2, n.Z3, n.C, n.y, n.dy, n.conf, n.P};
   for (void *p : ps)
     if (p) cudaFree(p);
@@ -471,6 +495,22 @@ int mlp_adam(Mlp &n, float lr, cudaStream_t s) {
   const float c1 = 1.0f - powf(b1, (float)n.adam_t), c2 = 1.0f - powf(b2, (float)n.adam_t);
   adam_kernel<<<blocks(n.L.total), 256, 0, s>>>(n.theta, n.grad, n.m, n.v, n.L.total, lr, b1, b2,
                                                eps, c1, c2);
+  return mlp_refresh_bf16(n, s);
+}
+
+int mlp_adam_dev_sync(Mlp &n, cudaStream_t s) {
+  return cudaMemcpyAsync(n.adam_dev, &n.adam_t, sizeof(int), cudaMemcpyHostToDevice, s) ==
+                 cudaSuccess
+             ? 0
+             : -2;
+}
+
+int mlp_adam_dev(Mlp &n, float lr, cudaStream_t s) {
+  const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+  adam_tick<<<1, 1, 0, s>>>(n.adam_dev, b1, b2);
+  adam_dev_kernel<<<blocks(n.L.total), 256, 0, s>>>(
+      n.theta, n.grad, n.m, n.v, n.L.total, lr, b1, b2, eps,
+      reinterpret_cast<const float *>(n.adam_dev + 1));
   return mlp_refresh_bf16(n, s);
 }
 

@@ -65,6 +65,8 @@ struct Mlp {
   __nv_bfloat16 *wf = nullptr;        /* W1, W2, W3 in MMA fragment order (H = 128, 256) */
   float mu = 0.0f, sigma = 1.0f;      /* target normalisation */
   int adam_t = 0;
+  int *adam_dev = nullptr;            /* [1] Adam step count and [2] its bias corrections (as
+                                         floats) on the device, for graph-replayed steps */
   int cap = 0;                        /* rows of the work buffers */
   __nv_bfloat16 *X = nullptr, *A1 = nullptr, *A2 = nullptr, *A3 = nullptr, *D = nullptr;
   __nv_bfloat16 *D2 = nullptr;        /* second buffer of the back-propagated dZ (ping-pong) */
@@ -90,6 +92,11 @@ int mlp_embed(Mlp &n, int rows, cudaStream_t s);
 /* forward + MSE loss against t (normalised targets) + backward into n.grad (zeroed first) */
 int mlp_loss_backward(Mlp &n, int rows, const float *t, cudaStream_t s);
 int mlp_adam(Mlp &n, float lr, cudaStream_t s);
+/* the same Adam step with its step count and bias corrections kept on the device (adam_dev,
+ * loaded from adam_t by mlp_adam_dev_sync), so that one step can be captured in a CUDA graph and
+ * replayed; the host's adam_t is not advanced */
+int mlp_adam_dev(Mlp &n, float lr, cudaStream_t s);
+int mlp_adam_dev_sync(Mlp &n, cudaStream_t s);
 /* BF16 copies of the weight matrices from theta (row-major, and in fragment order) */
 int mlp_refresh_bf16(Mlp &n, cudaStream_t s);
 /* after a synchronisation: 0, or -6 (and the flag cleared) if a GEMM's bounded wait ran out */
@@ -178,9 +185,12 @@ void da_pose_features(const GdDaDev &d, int ci, int pc, int lc, const float *mm,
  * stats[ci*GD_DA_NSTAT + k], err[ci*GD_DA_NERR + k] */
 void da_stats(const GdDaDev &d, const GdDaEpi &e_host, const GdDevComplex *cx_dev, int n_complex,
               unsigned long long *stats, double *err, cudaStream_t s);
-/* training batch: rows drawn from the sample ring into X / conf / t (normalised, clipped) */
-void da_gather(const GdDaDev &d, long long start, long long n_valid, int rows, int iter,
+/* training batch: rows drawn from the sample ring into X / conf / t (normalised, clipped), the
+ * draw keyed by the iteration count at ctr[0] (device memory, so that the step replays) */
+void da_gather(const GdDaDev &d, long long start, long long n_valid, int rows, const int *ctr,
                float *t, cudaStream_t s);
+/* end of a training step: hist[ctr[1]] = *loss, then both counters advance */
+void da_train_tick(float *hist, const float *loss, int *ctr, cudaStream_t s);
 /* per-block sum, sum of squares and count of the sample targets inside [lo, hi]:
  * GD_DA_MOM_BLOCKS x 3 doubles into part (summed on the host in block order) */
 #define GD_DA_MOM_BLOCKS 256
