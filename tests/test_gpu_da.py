@@ -398,3 +398,22 @@ def test_training_steps_replayed_from_a_graph_are_deterministic(raw):
     assert np.all(np.isfinite(losses)) and np.all(losses > 0)
     assert losses[40:].mean() < losses[:5].mean()
     assert len(set(losses.tolist())) > 40  # every step wrote its own slot
+
+
+def test_collect_is_the_plain_trajectory_with_two_replicas_per_thread(raw):
+    """A context whose plain tile holds two replicas per thread (the autotuner may pick it)
+    still runs the delayed-acceptance pipeline, whose kernels hold one replica per lane: its
+    collect steps are the plain trajectory bit for bit."""
+    w = _small(raw)
+    cx, ff, params = w.complexes[0], w.ff, w.params
+    with engine.Engine(ff, [cx], params) as a, engine.Engine(ff, [cx], params) as b:
+        for e in (a, b):
+            e.set_tile(6, 512, 1, 1, 0, 2)
+            e.mc_init()
+        a.run_fused(0, 40, exchange=True)
+        sur = engine.Surrogate(b, hidden=128, batch=256, sample_cap=1 << 16)
+        sur.collect(0, 40, exchange=True)
+        a.sync()
+        b.sync()
+        assert a.state().tobytes() == b.state().tobytes()
+        _same_records(a, b)
