@@ -983,6 +983,28 @@ def profile_mc(args):
           flush=True)
 
 
+def profile_screen(args):
+    """A slice of the config-2 screen small enough for multi-pass profiler captures: the first
+    --screen-ligands ligands (uneven 10-64 atoms, 8 conformers) on their pockets (uneven
+    1,200-6,000 points, 4 conformers), 16 temperatures, no records, the 256-lane fill tile with
+    512-point chunks; four 10-step launches of gd_mc_run."""
+    from geaxdock_gpu_b200 import engine, system
+    w = system.config(2, load_raw(), n_ligands=args.screen_ligands)
+    p = w.params
+    p.record = 0
+    tile = tuple(int(v) for v in args.tile.split(",")) if args.tile else (0, 512, 1, 1, 256)
+    with engine.Engine(w.ff, w.complexes, p) as e:
+        e.set_tile(*tile)
+        e.mc_init()
+        for it in range(4):
+            e.mc_run(0, it * p.steps_per_exchange)
+        e.sync()
+        pairs = sum(c.n_rep * c.lna * c.pnp for c in w.complexes)
+    print(json.dumps({"profile_screen": {"ligands": len(w.complexes), "replicas": w.n_rep,
+                                         "pairs_per_step": pairs, "launches": 4,
+                                         "tile": tile}}), flush=True)
+
+
 def sweep(args):
     """Device time of one 10-step gd_mc_run on the config-1 system (no records): for each tile
     of --sweep-tiles over all replicas, and, at the first of them, over the first m protein-
@@ -1068,6 +1090,10 @@ def main():
     ap.add_argument("--profile-mc", action="store_true",
                     help="only a short plain run on a 128-replica subset of the config-1 system "
                          "(four 10-step launches), for multi-pass profiler captures")
+    ap.add_argument("--profile-screen", action="store_true",
+                    help="only a short plain run on a --screen-ligands slice of the config-2 "
+                         "screen (four 10-step launches), for multi-pass profiler captures")
+    ap.add_argument("--screen-ligands", type=int, default=64)
     ap.add_argument("--sweep", action="store_true",
                     help="only the launch-time sweep over --sweep-tiles, replica blocks and "
                          "concurrent chains on the config-1 system; prints its own JSON line")
@@ -1099,6 +1125,9 @@ def main():
         return
     if args.sweep:
         sweep(args)
+        return
+    if args.profile_screen:
+        profile_screen(args)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
