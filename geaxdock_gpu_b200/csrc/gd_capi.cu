@@ -517,6 +517,8 @@ int gd_destroy(gd_ctx *c) {
   if (c->d_mm_in) cudaFree(c->d_mm_in);
   if (c->d_lc_in) cudaFree(c->d_lc_in);
   if (c->d_e_out) cudaFree(c->d_e_out);
+  if (c->d_xyz_in) cudaFree(c->d_xyz_in);
+  if (c->d_ctr_in) cudaFree(c->d_ctr_in);
   if (c->d_eval_tiles) cudaFree(c->d_eval_tiles);
   if (c->h_cursor) cudaFreeHost(c->h_cursor);
   if (c->d_chain_tiles) cudaFree(c->d_chain_tiles);
@@ -1383,15 +1385,40 @@ int gd_set_state(gd_ctx *c, const gd_replica_state *st, int r0, int r1) {
   return GD_OK;
 }
 
-int gd_eval_energy(gd_ctx *c, int ci, int prt_conf, int lig_conf, const float *mm, int n,
-                   gd_energy *out) {
-  if (!c || !mm || !out) return fail(GD_ERR_INVALID, "null argument");
+}  // extern "C"
+
+namespace {
+
+/* Energies of n poses of one (complex, protein conformer, ligand conformer): moved by
+ * movematrix rows (mm, kernel mode 2), or given as placed coordinates and centres (xyz and
+ * center, mode 4). */
+int eval_poses(gd_ctx *c, int ci, int prt_conf, int lig_conf, const float *mm, const float *xyz,
+               const float *center, int n, gd_energy *out) {
+  if (!c || !out || (!mm && !(xyz && center))) return fail(GD_ERR_INVALID, "null argument");
   if (ci < 0 || ci >= c->n_complex) return fail(GD_ERR_INVALID, "bad complex index");
   const ComplexInfo &x = c->info[ci];
   if (prt_conf < 0 || prt_conf >= x.n_prt || lig_conf < 0 || lig_conf >= x.n_lig)
     return fail(GD_ERR_INVALID, "conformer index out of range");
   if (n < 1) return GD_OK;
   CK(cudaSetDevice(c->device));
+  const bool given = mm == nullptr;
+  if (given) {
+    const size_t need = (size_t)n * x.lna * 3;
+    if (need > c->xyz_cap) {
+      if (c->d_xyz_in) cudaFree(c->d_xyz_in);
+      c->d_xyz_in = nullptr;
+      c->xyz_cap = 0;
+      CK(cudaMalloc(&c->d_xyz_in, sizeof(float) * need));
+      c->xyz_cap = need;
+    }
+    if (n > c->ctr_cap) {
+      if (c->d_ctr_in) cudaFree(c->d_ctr_in);
+      c->d_ctr_in = nullptr;
+      c->ctr_cap = 0;
+      CK(cudaMalloc(&c->d_ctr_in, sizeof(float) * 3 * n));
+      c->ctr_cap = n;
+    }
+  }
   if (n > c->eval_cap) {
     if (c->d_mm_in) cudaFree(c->d_mm_in);
     if (c->d_lc_in) cudaFree(c->d_lc_in);
@@ -1419,14 +1446,22 @@ int gd_eval_energy(gd_ctx *c, int ci, int prt_conf, int lig_conf, const float *m
   }
   std::vector<int> lc(n, lig_conf);
   CK(cudaStreamSynchronize(c->stream));
-  CK(cudaMemcpy(c->d_mm_in, mm, sizeof(float) * 6 * n, cudaMemcpyHostToDevice));
+  if (given) {
+    CK(cudaMemcpy(c->d_xyz_in, xyz, sizeof(float) * (size_t)n * x.lna * 3,
+                  cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->d_ctr_in, center, sizeof(float) * 3 * n, cudaMemcpyHostToDevice));
+  } else {
+    CK(cudaMemcpy(c->d_mm_in, mm, sizeof(float) * 6 * n, cudaMemcpyHostToDevice));
+  }
   CK(cudaMemcpy(c->d_lc_in, lc.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(c->d_eval_tiles, tiles.data(), sizeof(GdTileDesc) * tiles.size(),
                 cudaMemcpyHostToDevice));
   GdMcArgs a = base_args(c);
-  a.mode = 2;
+  a.mode = given ? 4 : 2;
   a.n_steps = 1;
-  a.mm_in = c->d_mm_in;
+  a.mm_in = given ? nullptr : c->d_mm_in;
+  a.xyz_in = given ? c->d_xyz_in : nullptr;
+  a.center_in = given ? c->d_ctr_in : nullptr;
   a.lig_conf_in = c->d_lc_in;
   a.e_out = c->d_e_out;
   a.rec = nullptr;
@@ -1436,6 +1471,22 @@ int gd_eval_energy(gd_ctx *c, int ci, int prt_conf, int lig_conf, const float *m
   if ((rc = gd_sync(c))) return rc;
   CK(cudaMemcpy(out, c->d_e_out, sizeof(gd_energy) * n, cudaMemcpyDeviceToHost));
   return GD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gd_eval_energy(gd_ctx *c, int ci, int prt_conf, int lig_conf, const float *mm, int n,
+                   gd_energy *out) {
+  if (!mm) return fail(GD_ERR_INVALID, "null argument");
+  return eval_poses(c, ci, prt_conf, lig_conf, mm, nullptr, nullptr, n, out);
+}
+
+int gd_eval_energy_xyz(gd_ctx *c, int ci, int prt_conf, int lig_conf, const float *xyz,
+                       const float *center, int n, gd_energy *out) {
+  if (!xyz || !center) return fail(GD_ERR_INVALID, "null argument");
+  return eval_poses(c, ci, prt_conf, lig_conf, nullptr, xyz, center, n, out);
 }
 
 /* One thread per (pose, atom): the rotation of the pose and the placed atom, with the same

@@ -143,6 +143,9 @@ struct gd_ctx {
   int *d_lc_in = nullptr;
   gd_energy *d_e_out = nullptr;
   int eval_cap = 0;
+  float *d_xyz_in = nullptr, *d_ctr_in = nullptr; /* given coordinates and centres (mode 4) */
+  size_t xyz_cap = 0;                             /* floats of d_xyz_in */
+  int ctr_cap = 0;                                /* poses of d_ctr_in */
   GdTileDesc *d_eval_tiles = nullptr;
   int eval_tiles_cap = 0;
   long long timeout_ns = 2000000000LL;

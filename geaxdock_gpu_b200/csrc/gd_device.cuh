@@ -117,7 +117,8 @@ struct GdMcArgs {
   int n_tiles;
   int *tile_counter;          /* persistent-CTA work queue head */
   int mode;                   /* 0: MC steps, 1: init (energy at movematrix 0), 2: eval poses,
-                                 3: delayed-acceptance exact stage (eval + decision) */
+                                 3: delayed-acceptance exact stage (eval + decision), 4: eval
+                                 given placed coordinates */
   int n_steps;                /* steps in this launch (mode 0) */
   int step0;                  /* step number of the first step (s1 + s2), added to *step_base */
   const int *step_base;       /* device cursor for graph replays (null: 0) */
@@ -144,6 +145,10 @@ struct GdMcArgs {
   const float *mm_in;
   const int *lig_conf_in;     /* per pose ligand conformer (mode 2) */
   gd_energy *e_out;
+  /* mode 4: pose i's atoms at xyz_in[(i * lna + atom) * 3 + {0,1,2}], its centre at
+   * center_in[i * 3 + {0,1,2}] (the lab frame, as Ligand.coord_new) */
+  const float *xyz_in;
+  const float *center_in;
   unsigned *err;              /* device error word */
   long long timeout_ns;       /* bounded waits */
   /* mode 3: tile.count holds (group << 8) | capacity; the survivors come from da_cnt */

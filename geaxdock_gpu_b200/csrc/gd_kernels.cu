@@ -15,6 +15,7 @@
  *   CalcMcc_d     (src/kernel_cuda_l2_calcmcc.cu:148-206) contact count inside the pair loop,
  *                 true positives from the sparse reference-contact list;
  *   CalcRmsd_d, KDE, MCS, dst, CombineEnergy_d (src/kernel_cuda_l3_combineenergy.cu:23-37),
+ *                 of moved poses (modes 0-3) or of given placed coordinates (mode 4),
  *   Accept_d (src/kernel_cuda_l2_accept.cu:13-46), RecordLigand_d
  *   (src/kernel_cuda_l3_util.cu:74-106) in the per-replica epilogue run by one warp per slot.
  * gd_exchange_kernel: ExchangeReplicas_d (src/kernel_cuda_l1_exchangereplicas.cu:27-77), one
@@ -510,7 +511,7 @@ __global__ void __launch_bounds__(GD_MAX_TPB / PACK, GD_MIN_BLOCKS_PACK(UNROLL, 
                        (uint32_t)(step_first + s), a.move_kind, a.move_scale, delta, &u);
 #pragma unroll
           for (int i = 0; i < 6; ++i) mmn[i] = GD_ADD(sl.mm_old[i], delta[i]);
-        } else if (a.mode >= 2) {
+        } else if (a.mode == 2 || a.mode == 3) {
 #pragma unroll
           for (int i = 0; i < 6; ++i) mmn[i] = a.mm_in[(size_t)sl.rep * 6 + i];
         } else {
@@ -527,6 +528,12 @@ __global__ void __launch_bounds__(GD_MAX_TPB / PACK, GD_MIN_BLOCKS_PACK(UNROLL, 
         sl.tx = GD_ADD(mmn[0], lc[0]);
         sl.ty = GD_ADD(mmn[1], lc[1]);
         sl.tz = GD_ADD(mmn[2], lc[2]);
+        if (a.mode == 4) {
+          /* given coordinates: the ligand centre comes with them (Ligand.coord_new.center) */
+          sl.tx = a.center_in[(size_t)sl.rep * 3];
+          sl.ty = a.center_in[(size_t)sl.rep * 3 + 1];
+          sl.tz = a.center_in[(size_t)sl.rep * 3 + 2];
+        }
         sl.u = u;
       }
       __syncthreads();
@@ -536,8 +543,15 @@ __global__ void __launch_bounds__(GD_MAX_TPB / PACK, GD_MIN_BLOCKS_PACK(UNROLL, 
         ax[h] = ay[h] = az[h] = 0.0f;
         if (active) {
           const Slot &sl = slots[sl_of[h]];
-          gd_place_atom(sl.rot, sl.tx, sl.ty, sl.tz, orig[h].x, orig[h].y, orig[h].z, &ax[h],
-                        &ay[h], &az[h]);
+          if (a.mode == 4) {
+            const float *p = a.xyz_in + ((size_t)sl.rep * L + l) * 3;
+            ax[h] = p[0];
+            ay[h] = p[1];
+            az[h] = p[2];
+          } else {
+            gd_place_atom(sl.rot, sl.tx, sl.ty, sl.tz, orig[h].x, orig[h].y, orig[h].z, &ax[h],
+                          &ay[h], &az[h]);
+          }
           if (ok[h]) atoms[vl[h]] = make_float4(ax[h], ay[h], az[h], 0.0f);
         }
       }
@@ -744,7 +758,7 @@ __global__ void __launch_bounds__(GD_MAX_TPB / PACK, GD_MIN_BLOCKS_PACK(UNROLL, 
           }
           en.rmsd = (float)sqrt(tot[7 * T] / Ld);
           const int rid = sl.rep;
-          if (a.mode == 2) {
+          if (a.mode == 2 || a.mode == 4) {
             a.e_out[rid] = en;
           } else if (DA && a.mode == 3) {
             da_decide(a, cx, tile.complex_index, rid, en, sl.mm_new, step_first + s);

@@ -68,6 +68,7 @@ def lib() -> C.CDLL:
         "gd_set_state": [vp, vp, C.c_int, C.c_int],
         "gd_get_device_error": [vp, ip],
         "gd_eval_energy": [vp, C.c_int, C.c_int, C.c_int, fp, C.c_int, vp],
+        "gd_eval_energy_xyz": [vp, C.c_int, C.c_int, C.c_int, fp, fp, C.c_int, vp],
         "gd_place_ligand": [vp, C.c_int, C.c_int, fp, C.c_int, fp],
         "gd_trace_enable": [vp, C.c_int],
         "gd_trace_get": [vp, fp, ip, ip],
@@ -306,6 +307,18 @@ class Engine:
         out = np.zeros(mm.shape[0], abi.ENERGY_DTYPE)
         check(lib().gd_eval_energy(self.h, complex_index, prt_conf, lig_conf, abi.fptr(mm),
                                    mm.shape[0], _p(out)))
+        return out
+
+    def eval_energy_xyz(self, complex_index: int, prt_conf: int, lig_conf: int,
+                        xyz: np.ndarray, center: np.ndarray) -> np.ndarray:
+        """Energies of given placed coordinates: xyz [n_poses, lna, 3] and the ligand centres
+        [n_poses, 3], lab frame (CalcEnergy_d on Ligand.coord_new)."""
+        n = int(np.asarray(center).size // 3)
+        x = np.ascontiguousarray(xyz, np.float32).reshape(n, -1, 3)
+        c = np.ascontiguousarray(center, np.float32).reshape(n, 3)
+        out = np.zeros(n, abi.ENERGY_DTYPE)
+        check(lib().gd_eval_energy_xyz(self.h, complex_index, prt_conf, lig_conf, abi.fptr(x),
+                                       abi.fptr(c), n, _p(out)))
         return out
 
     def place_ligand(self, complex_index: int, lig_conf: int,

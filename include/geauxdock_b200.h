@@ -295,6 +295,15 @@ int gd_get_device_error(gd_ctx *ctx, int *code);
  * cms is measured against the complex's contact reference (built by gd_mc_init). */
 int gd_eval_energy(gd_ctx *ctx, int complex_index, int prt_conf, int lig_conf,
                    const float *movematrix, int n_poses, gd_energy *out);
+/* CalcEnergy_d + CalcMcc_d + CalcRmsd_d (src/kernel_cuda_l2_calcenergy.cu:19-360,
+ * src/kernel_cuda_l2_calcmcc.cu:148-206, src/kernel_cuda_l2_calcrmsd.cu:1-36) on given placed
+ * coordinates, as the reference's kernels read them from Ligand.coord_new: pose i's atoms at
+ * xyz[(i * lna + atom) * 3 + {0, 1, 2}] and its centre (coord_new.center, which gives dst) at
+ * center[i * 3 + {0, 1, 2}], lab frame; rmsd is taken against conformer lig_conf's reference
+ * pose. Same output as gd_eval_energy; placing movematrix poses with gd_place_ligand and their
+ * centres movematrix[0..2] + the conformer's centre gives gd_eval_energy's results bit for bit. */
+int gd_eval_energy_xyz(gd_ctx *ctx, int complex_index, int prt_conf, int lig_conf,
+                       const float *xyz, const float *center, int n_poses, gd_energy *out);
 
 /* Pose energies like gd_eval_energy, for callers that cannot allocate device memory when
  * they need the result (a framework that owns the whole device pool, a callback or

@@ -11,7 +11,7 @@ import pytest
 from geaxdock_gpu_b200 import abi, engine, system
 from oracle import pyoracle as po
 from tests.golden.fixtures import load_ref
-from tests.tolerance import plain_rel_errors, rel_errors, report
+from tests.tolerance import plain_rel_errors, rel_errors, report, scales
 
 pytestmark = pytest.mark.gpu
 
@@ -577,3 +577,36 @@ def test_largest_and_smallest_complexes_against_oracle(raw):
             eng.sync()
             assert np.all(np.isfinite(eng.etotal()))
     assert sumabs.max() <= TOL, sumabs
+
+
+def test_energies_of_the_references_own_placed_coordinates():
+    """gd_eval_energy_xyz on the coordinates the reference's own Move_d produced (the pin
+    fixtures' pose_xyz / pose_center, src/kernel_cuda_l2_move.cu run on the CPU): every term
+    within 1e-5 of the FP64 oracle on the same coordinates, and the total within 2e-5 of the
+    reference's own FP32 CalcEnergy_d on them (whose own error is up to 7.3e-6 by the same
+    metric); and placing poses with gd_place_ligand then evaluating the coordinates gives
+    gd_eval_energy's results bit for bit."""
+    for name in ("1a07C1", "1robA1"):
+        z, cx, ff = load_ref(name)
+        rm = z["ref_matrix"].astype(np.uint8)
+        with engine.Engine(ff, [cx], abi.mc_params()) as eng:
+            worst, vs_ref = np.zeros(10), 0.0
+            for i in range(z["pose_mm"].shape[0]):
+                ip, il = (int(v) for v in z["pose_idx"][i])
+                xyz = np.ascontiguousarray(z["pose_xyz"][i].T)  # [lna, 3]
+                got = eng.eval_energy_xyz(0, ip, il, xyz[None], z["pose_center"][i][None])[0]
+                o = po.energy_eval(ff, cx, ip, il, z["pose_xyz"][i][0], z["pose_xyz"][i][1],
+                                   z["pose_xyz"][i][2], z["pose_center"][i], rm, 64)
+                worst = np.maximum(worst, rel_errors(got["e"], o, ff))
+                assert abs(got["cms"] - o["cms"]) <= 2e-6
+                vs_ref = max(vs_ref, abs(float(got["e"][9]) - float(z["pose_energy"][i][9]))
+                             / scales(o, ff)[9])
+            assert worst.max() <= TOL, (name, worst)
+            assert vs_ref <= 2e-5, (name, vs_ref)
+            ip, il = 1, 3
+            mm = np.random.default_rng(4).normal(0, 1.0, (17, 6)).astype(np.float32)
+            xyz = eng.place_ligand(0, il, mm)
+            ctr = (mm[:, :3] + cx.lig_center[il][None, :].astype(np.float32)).astype(np.float32)
+            a = eng.eval_energy(0, ip, il, mm)
+            b = eng.eval_energy_xyz(0, ip, il, xyz, ctr)
+            assert a.tobytes() == b.tobytes(), name
