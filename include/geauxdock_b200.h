@@ -339,7 +339,7 @@ int gd_trace_get(gd_ctx *ctx, float *e_new_total, int *accepted, int *n_steps);
  * learned embedding per (complex, protein conformer, ligand conformer), per-pocket features)
  * with BF16 weights/activations on the tensor cores and FP32 accumulation, FP32 master
  * weights and Adam. It is the first stage of a delayed-acceptance Metropolis step; the exact
- * energy judges every surviving proposal with the corrected ratio, so the stationary
+ * energy decides on every surviving proposal with the corrected ratio, so the stationary
  * distribution is the plain method's. */
 
 typedef struct {
