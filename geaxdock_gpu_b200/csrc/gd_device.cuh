@@ -4,12 +4,17 @@
  * HBM layout (one context, all complexes of a batch):
  *   ligand conformers   float4 (x, y, z, charge) + int2 (type, MCS field) per atom,
  *                       conformer-major; placed coordinates never touch HBM.
- *   protein conformers  points sorted by (point type, kind) per conformer, every segment
- *                       starting on an even slot, stored as pairs of slots in three float4
- *                       streams (negated coordinates and ele; hydrophobic hpp or 0 and PSP
- *                       column) so one 16-byte shared load gives the two-lane register pairs
- *                       of the FP32x2 pair loop; a segment table (start, end, type, kind) per
- *                       conformer. kind bit 0: hydrophobic point, bit 1: class-2 (PSP) point.
+ *   protein conformers  two copies of every conformer's points:
+ *                       (1) for the all-pairs loop (vdw, ele, pmf, hdb), sorted by point type,
+ *                       every type segment starting on an even slot, stored as pairs of slots
+ *                       in two float4 streams (negated coordinates and ele / el1) so one
+ *                       16-byte shared load gives the two-lane register pairs of the FP32x2
+ *                       loop; a segment table (start, end, type, flags) per conformer, flag
+ *                       bit 2: the type has a live hydrogen-bond pair with the ligand;
+ *                       (2) for the short-range terms (contacts, psp, hpc, the electrostatic
+ *                       soft core), a cell list: points sorted by cell of a uniform grid (x
+ *                       fastest) as float4 (x, y, z, type and kind bits) + float4 (hpp, PSP
+ *                       column bits, ele / el1, 0), and the first point of every cell.
  *   pair parameters     per (ligand type, protein type) 12 floats, folded for the kernel.
  *   contact reference   per conformer and ligand atom, the list of reference contacts as
  *                       float4 (x, y, z, contact threshold): tp is counted over this sparse
@@ -26,7 +31,11 @@
 
 #include "../../include/geauxdock_b200.h"
 
-#define GD_MAX_SEG 96          /* (30 point types) x (3 kinds), rounded up */
+#define GD_MAX_SEG 32          /* point types (30), rounded up */
+#define GD_CELL 4.0f           /* edge of the short-range cell grid (A) */
+/* shared-memory bytes of the contact-threshold table at the front of the kernel's buffer */
+#define GD_THR_BYTES (GD_MAXTP2 * GD_MAXTP1 * 4)
+#define GD_MAX_CELLS (1 << 22) /* cells per conformer grid; a larger box widens the cells */
 #define GD_MAX_TPB 256         /* threads per CTA: 3 CTAs of 256 fit the register file */
 #define GD_SLOT_BYTES 192      /* shared-memory bytes per replica slot (sizeof gd::Slot) */
 /* resident 256-thread CTAs per SM the register budget is set for, per unroll depth */
@@ -55,15 +64,26 @@ struct GdDevComplex {
   int rep_offset, n_rep, psp_ld, mcs_ld;
   int stream, nref_total, pad0, pad1;
   float pocket[4];
+  /* short-range cell grid, one frame for every conformer of the complex: cell (ix, iy, iz)
+   * covers [org + i * cell, org + (i + 1) * cell) per axis, index (iz * ny + iy) * nx + ix */
+  float sr_org[3], sr_cell, sr_inv_cell;
+  float sr_r;                 /* search radius: every pair with d^2 <= sr_r2 lies inside it */
+  float sr_r2;                /* max(81 (hpc), largest contact threshold, (1 / el1)^2) */
+  float sr_pad;
+  int sr_n[4];                /* nx, ny, nz, cells */
   const float4 *lig_pos;      /* [n_lig*lna] */
   const int2 *lig_meta;       /* [n_lig*lna] type, MCS index (n + 1) */
   const float *lig_center;    /* [n_lig*3] */
   /* protein points in pairs (slots 2m, 2m+1), [n_prt*pnp_pad/2] each:
-   *   pt_a = (-x0, -x1, -y0, -y1), pt_b = (-z0, -z1, ele0, ele1),
-   *   pt_x = (hpp0 or 0, hpp1 or 0, psp column0 bits, psp column1 bits) */
+   *   pt_a = (-x0, -x1, -y0, -y1), pt_b = (-z0, -z1, ele0 / el1, ele1 / el1) */
   const float4 *pt_a;
   const float4 *pt_b;
-  const float4 *pt_x;
+  /* the cell list, [n_prt*pnp] points and [n_prt*(sr_n[3] + 1)] cell starts (conformer-local
+   * point indices): sr_a = (x, y, z, bits of type | 256 if hydrophobic | 512 if class 2),
+   * sr_b = (hpp, PSP column bits, ele / el1, 0) */
+  const float4 *sr_a;
+  const float4 *sr_b;
+  const int *sr_start;
   const int4 *seg;            /* [n_prt*GD_MAX_SEG] */
   const int *seg_count;       /* [n_prt] */
   const float4 *kde;          /* [pnk] x, y, z, type (exact small integer as float) */

@@ -104,26 +104,24 @@ __device__ __forceinline__ float dist2(float ax, float ay, float az, float px, f
 #define LOG2E_F 1.4426950408889634f
 
 struct Acc {
-  float2 vdw, ele, pmf, hdb, hsum;
-  float2 ncon; /* contact counts (exact small integers) */
-  float psp;
+  float2 vdw, ele, pmf, hdb;
 };
 
 /* Per-segment pair parameters, splatted over the two lanes of an FP32x2 register pair. */
 struct Pair2 {
   float2 p1a, mp2a, p1l, b2, c2, pmf1, hc1, hc0, hs;
-  float thr;
 };
 
 __device__ __forceinline__ float2 f2(float v) { return make_float2(v, v); }
 
-/* One pair of protein slots (2m, 2m+1) against the lane's atom. PAIR = false: only the
- * first slot is a point (the second is segment padding) and nothing of the second is kept. */
-template <int KIND, bool HDB, bool PAIR>
-__device__ __forceinline__ void pair_body(const float4 A, const float4 B,
-                                          const float4 *__restrict__ PX, int m, float2 ax,
-                                          float2 ay, float2 az, const Pair2 &q,
-                                          const float *__restrict__ psprow, const GdForceConst &f,
+/* One pair of protein slots (2m, 2m+1) against the lane's atom: the terms every pair has
+ * (vdw, the far form of ele, pmf; hdb on segments whose type has a live hydrogen-bond pair).
+ * The short-range terms (contacts, psp, hpc, the electrostatic soft core) come from the cell
+ * list pass, short_range(). PAIR = false: only the first slot is a point (the second is
+ * segment padding) and nothing of the second is kept. */
+template <bool HDB, bool PAIR>
+__device__ __forceinline__ void pair_body(const float4 A, const float4 B, float2 ax, float2 ay,
+                                          float2 az, const Pair2 &q, const GdForceConst &f,
                                           Acc &a) {
   const float2 one = f2(1.0f);
   /* squared distance, per lane exactly dist2(): a + (-p) == a - p */
@@ -140,22 +138,14 @@ __device__ __forceinline__ void pair_body(const float4 A, const float4 B,
   const float2 num = __fmul2_rn(r6i, __ffma2_rn(q.p1a, r3i, q.mp2a));
   const float2 t9 = __fmul2_rn(q.p1l, __fmul2_rn(r6i, r3i));
   const float2 p4 = __ffma2_rn(t9, __ffma2_rn(f2(f.lj1), d2, one), one);
-  /* ele: q_l ele_p g(el1 r), q_l applied once per atom. Shared memory holds ele_p / el1, so
-   * the far branch g = 1 / (el1 r) is one FMA with r^-1; inside r < 1 / el1 (d2 < near2,
-   * rare) the soft core adds ele_p (g_near - g_far). g is continuous at el1 r = 1. */
+  /* ele: q_l ele_p g(el1 r), q_l applied once per atom. The points hold ele_p / el1, so the
+   * far form g = 1 / (el1 r) is one FMA with r^-1; pairs inside r < 1 / el1 get the soft-core
+   * difference in short_range() */
   const float2 ep = make_float2(B.z, B.w);
   if constexpr (PAIR) {
     a.ele = __ffma2_rn(ep, ri, a.ele);
   } else {
     a.ele.x = __fmaf_rn(ep.x, ri.x, a.ele.x);
-  }
-  if ((PAIR ? fminf(d2.x, d2.y) : d2.x) < f.near2) {
-    const float2 s1 = __fmul2_rn(f2(f.el1), r);
-    const float2 gn =
-        __ffma2_rn(__fmul2_rn(s1, s1), __ffma2_rn(f2(f.b1), s1, f2(f.a1)), f2(f.el0));
-    /* ep (el1 gn) - ep ri = ele_p gn - ele_p g_far */
-    if (d2.x < f.near2) a.ele.x += __fmaf_rn(ep.x * f.el1, gn.x, -(ep.x * ri.x));
-    if (PAIR && d2.y < f.near2) a.ele.y += __fmaf_rn(ep.y * f.el1, gn.y, -(ep.y * ri.y));
   }
   /* pmf: pmf1 / (1 + exp((6 - r/2)(r - pmf0))) as exp2 of the expanded quadratic
    * cA d2 + b2 r + c2 (cA = -log2(e)/2, b2 = log2(e)(6 + pmf0/2), c2 = -6 log2(e) pmf0).
@@ -176,18 +166,6 @@ __device__ __forceinline__ void pair_body(const float4 A, const float4 B,
     a.vdw.x = __fmaf_rn(vn.x, inv.x, a.vdw.x);
     a.pmf.x = __fmaf_rn(pn.x, inv.x, a.pmf.x);
   }
-  /* contacts (mcc, psp): sqrtf(d2) <= pmf0  <=>  d2 <= thr, counted as 1.0 / 0.0 */
-  const bool c0 = d2.x <= q.thr, c1 = PAIR && d2.y <= q.thr;
-  if constexpr (PAIR) {
-    a.ncon = __fadd2_rn(a.ncon, make_float2(c0 ? 1.0f : 0.0f, c1 ? 1.0f : 0.0f));
-  } else {
-    a.ncon.x += c0 ? 1.0f : 0.0f;
-  }
-  if (KIND & 2) {
-    const float4 X = PX[m];
-    if (c0) a.psp += __ldg(psprow + __float_as_int(X.z));
-    if (c1) a.psp += __ldg(psprow + __float_as_int(X.w));
-  }
   if (HDB) {
     const float2 h = __ffma2_rn(r, q.hc1, q.hc0);
     const float2 hh = __fmul2_rn(h, h);
@@ -196,60 +174,139 @@ __device__ __forceinline__ void pair_body(const float4 A, const float4 B,
     else
       a.hdb.x = __fmaf_rn(q.hs.x, ex2_a(-hh.x), a.hdb.x);
   }
-  if (KIND & 1) {
-    const float4 X = PX[m];
-    float2 t = __ffma2_rn(d2, f2(HPC_C4), f2(-HPC_C3));
-    t = __ffma2_rn(d2, t, f2(HPC_C2));
-    t = __ffma2_rn(d2, t, f2(-HPC_C1));
-    const float2 pl = __ffma2_rn(d2, t, one);
-    if (d2.x <= 81.0f) a.hsum.x = __fmaf_rn(X.x, pl.x, a.hsum.x);
-    if (PAIR && d2.y <= 81.0f) a.hsum.y = __fmaf_rn(X.y, pl.y, a.hsum.y);
-  }
 }
 
-/* Pair loop over slots [i0, i1) of one (type, kind) segment held in shared memory; i0 is
- * even, an odd i1 leaves one point for a half iteration. KIND bit 0: hydrophobic point (hpc),
- * bit 1: class-2 point (psp). HDB: the segment's point type has a live hydrogen-bond pair
- * with some atom type of the ligand (decided per complex on the host, so every warp of the
- * CTA runs the same code). UNROLL: point pairs in flight per lane. */
-template <int KIND, bool HDB, int UNROLL>
+/* Pair loop over slots [i0, i1) of one point-type segment held in shared memory; i0 is even,
+ * an odd i1 leaves one point for a half iteration. HDB: the segment's point type has a live
+ * hydrogen-bond pair with some atom type of the ligand (decided per complex on the host, so
+ * every warp of the CTA runs the same code). UNROLL: point pairs in flight per lane. */
+template <bool HDB, int UNROLL>
 __device__ __forceinline__ void pair_range(const float4 *__restrict__ PA,
-                                           const float4 *__restrict__ PB,
-                                           const float4 *__restrict__ PX, int i0, int i1,
+                                           const float4 *__restrict__ PB, int i0, int i1,
                                            float ax, float ay, float az, const Pair2 &q,
-                                           const float *__restrict__ psprow,
                                            const GdForceConst &f, Acc &a) {
   const float2 ax2 = f2(ax), ay2 = f2(ay), az2 = f2(az);
   const int m0 = i0 >> 1, m1 = i1 >> 1;
 #pragma unroll UNROLL
-  for (int m = m0; m < m1; ++m)
-    pair_body<KIND, HDB, true>(PA[m], PB[m], PX, m, ax2, ay2, az2, q, psprow, f, a);
-  if (i1 & 1) pair_body<KIND, HDB, false>(PA[m1], PB[m1], PX, m1, ax2, ay2, az2, q, psprow, f, a);
+  for (int m = m0; m < m1; ++m) pair_body<HDB, true>(PA[m], PB[m], ax2, ay2, az2, q, f, a);
+  if (i1 & 1) pair_body<HDB, false>(PA[m1], PB[m1], ax2, ay2, az2, q, f, a);
 }
 
 /* The same range for the same atom of two replicas (the lane's two slots): one load of each
- * point pair, one loop, the segment's parameters and table rows shared; each atom's sums are
- * the operations of pair_range in the same order, so its energies are bit-identical. */
-template <int KIND, bool HDB, int UNROLL>
+ * point pair, one loop, the segment's parameters shared; each atom's sums are the operations
+ * of pair_range in the same order, so its energies are bit-identical. */
+template <bool HDB, int UNROLL>
 __device__ __forceinline__ void pair_range2(const float4 *__restrict__ PA,
-                                            const float4 *__restrict__ PB,
-                                            const float4 *__restrict__ PX, int i0, int i1,
+                                            const float4 *__restrict__ PB, int i0, int i1,
                                             const float *ax, const float *ay, const float *az,
-                                            const Pair2 &q, const float *__restrict__ psprow,
-                                            const GdForceConst &f, Acc *a) {
+                                            const Pair2 &q, const GdForceConst &f, Acc *a) {
   const float2 ax0 = f2(ax[0]), ay0 = f2(ay[0]), az0 = f2(az[0]);
   const float2 ax1 = f2(ax[1]), ay1 = f2(ay[1]), az1 = f2(az[1]);
   const int m0 = i0 >> 1, m1 = i1 >> 1;
 #pragma unroll UNROLL
   for (int m = m0; m < m1; ++m) {
     const float4 A = PA[m], B = PB[m];
-    pair_body<KIND, HDB, true>(A, B, PX, m, ax0, ay0, az0, q, psprow, f, a[0]);
-    pair_body<KIND, HDB, true>(A, B, PX, m, ax1, ay1, az1, q, psprow, f, a[1]);
+    pair_body<HDB, true>(A, B, ax0, ay0, az0, q, f, a[0]);
+    pair_body<HDB, true>(A, B, ax1, ay1, az1, q, f, a[1]);
   }
   if (i1 & 1) {
     const float4 A = PA[m1], B = PB[m1];
-    pair_body<KIND, HDB, false>(A, B, PX, m1, ax0, ay0, az0, q, psprow, f, a[0]);
-    pair_body<KIND, HDB, false>(A, B, PX, m1, ax1, ay1, az1, q, psprow, f, a[1]);
+    pair_body<HDB, false>(A, B, ax0, ay0, az0, q, f, a[0]);
+    pair_body<HDB, false>(A, B, ax1, ay1, az1, q, f, a[1]);
+  }
+}
+
+/* Sums of the short-range terms of one atom. */
+struct ShortSums {
+  double hsum;                /* sum of hpp * switch(d^2) over hydrophobic points, d^2 <= 81 */
+  float psp;                  /* sum of the PSP entries of class-2 points in contact */
+  float ele;                  /* soft-core minus far-form electrostatics, d^2 < (1 / el1)^2 */
+  int ncon;                   /* contacts: d^2 <= the pair's contact threshold */
+};
+
+/* The terms of CalcEnergy_d that only pairs within a few angstrom have (contacts for mcc and
+ * psp, hpc's switching polynomial, the soft core of ele), for one atom at (ax, ay, az), from
+ * the conformer's cell list: the rows of cells (fixed y, z) that reach within sr_r of the
+ * atom, each over the x range the remaining radius allows, so every point with
+ * d^2 <= sr_r2 is visited once and the tests use the same d^2 as the pair loop. The next
+ * row's bounds are read while the current row runs. thr: the contact thresholds of the atom's
+ * type against every point type (shared memory). */
+__device__ __forceinline__ void short_range(const GdDevComplex &cx, int pc,
+                                            const float *__restrict__ thr,
+                                            const float *__restrict__ psprow,
+                                            const GdForceConst &f, float ax, float ay, float az,
+                                            ShortSums &s) {
+  s.hsum = 0.0;
+  s.psp = 0.0f;
+  s.ele = 0.0f;
+  s.ncon = 0;
+  const int nx = cx.sr_n[0], ny = cx.sr_n[1], nz = cx.sr_n[2];
+  const float R = cx.sr_r, R2 = cx.sr_r * cx.sr_r, ic = cx.sr_inv_cell, e = cx.sr_cell;
+  const float r2max = cx.sr_r2;
+  const float ox = cx.sr_org[0], oy = cx.sr_org[1], oz = cx.sr_org[2];
+  const int y0 = max(0, (int)floorf((ay - R - oy) * ic));
+  const int y1 = min(ny - 1, (int)floorf((ay + R - oy) * ic));
+  const int z0 = max(0, (int)floorf((az - R - oz) * ic));
+  const int z1 = min(nz - 1, (int)floorf((az + R - oz) * ic));
+  if (y0 > y1 || z0 > z1) return;
+  const int *__restrict__ st = cx.sr_start + (size_t)pc * (cx.sr_n[3] + 1);
+  const float4 *__restrict__ PA = cx.sr_a + (size_t)pc * cx.pnp;
+  const float4 *__restrict__ PB = cx.sr_b + (size_t)pc * cx.pnp;
+  /* point range of row (iy, iz) within the remaining radius; empty when out of reach */
+  auto bounds = [&](int iy, int iz, int &b0, int &b1) {
+    b0 = b1 = 0;
+    const float zl = oz + (float)iz * e, yl = oy + (float)iy * e;
+    const float gz = fmaxf(0.0f, fmaxf(zl - az, az - (zl + e)));
+    const float gy = fmaxf(0.0f, fmaxf(yl - ay, ay - (yl + e)));
+    const float rem = R2 - gy * gy - gz * gz;
+    if (rem < 0.0f) return;
+    const float hx = sqrtf(rem);
+    const int x0 = max(0, (int)floorf((ax - hx - ox) * ic));
+    const int x1 = min(nx - 1, (int)floorf((ax + hx - ox) * ic));
+    if (x0 > x1) return;
+    const int row = (iz * ny + iy) * nx;
+    b0 = __ldg(st + row + x0);
+    b1 = __ldg(st + row + x1 + 1);
+  };
+  int iy = y0, iz = z0, n0, n1;
+  bounds(iy, iz, n0, n1);
+  for (;;) {
+    const int c0 = n0, c1 = n1;
+    if (++iy > y1) {
+      iy = y0;
+      ++iz;
+    }
+    const bool more = iz <= z1;
+    if (more) bounds(iy, iz, n0, n1);
+    for (int i = c0; i < c1; ++i) {
+      const float4 p = __ldg(PA + i);
+      const float d2 = dist2(ax, ay, az, p.x, p.y, p.z);
+      if (d2 > r2max) continue;
+      const int meta = __float_as_int(p.w);
+      const bool hpc = (meta & 256) && d2 <= 81.0f;
+      const bool con = d2 <= thr[meta & 255];
+      const bool cls2 = con && (meta & 512);
+      const bool near = d2 < f.near2;
+      s.ncon += con ? 1 : 0;
+      if (hpc || cls2 || near) {
+        const float4 b = __ldg(PB + i);
+        if (hpc) {
+          float t = __fmaf_rn(d2, HPC_C4, -HPC_C3);
+          t = __fmaf_rn(d2, t, HPC_C2);
+          t = __fmaf_rn(d2, t, -HPC_C1);
+          s.hsum += (double)__fmul_rn(b.x, __fmaf_rn(d2, t, 1.0f));
+        }
+        if (cls2) s.psp += __ldg(psprow + __float_as_int(b.y));
+        if (near) {
+          const float ri = rsqrt_a(d2);
+          const float s1 = __fmul_rn(f.el1, __fmul_rn(d2, ri));
+          const float gn = __fmaf_rn(__fmul_rn(s1, s1), __fmaf_rn(f.b1, s1, f.a1), f.el0);
+          /* ep (el1 gn) - ep ri = ele_p gn - ele_p g_far */
+          s.ele += __fmaf_rn(b.z * f.el1, gn, -(b.z * ri));
+        }
+      }
+    }
+    if (!more) break;
   }
 }
 
@@ -276,28 +333,22 @@ __device__ __forceinline__ double warp_sum(double v) {
 
 #define NQ 10 /* vdw ele pmf psp hdb hsum->hpc kde rmsd ncon tp */
 
-/* One segment range of the pair loop, dispatched on the segment kind: bits 0-1 point kind,
- * bit 2 live hydrogen-bond term. */
+/* One segment range of the pair loop, dispatched on the segment's flags (bit 2: live
+ * hydrogen-bond term). */
 template <int UNROLL, int PACK>
-__device__ __forceinline__ void pair_dispatch(int kind, const float4 *PA, const float4 *PB,
-                                              const float4 *PX, int i0, int i1, const float *ax,
-                                              const float *ay, const float *az, const Pair2 &pq,
-                                              const float *psprow, const GdForceConst &f,
-                                              Acc *acc) {
-#define GD_PR(K, H)                                                                          \
+__device__ __forceinline__ void pair_dispatch(int flags, const float4 *PA, const float4 *PB,
+                                              int i0, int i1, const float *ax, const float *ay,
+                                              const float *az, const Pair2 &pq,
+                                              const GdForceConst &f, Acc *acc) {
+#define GD_PR(H)                                                                             \
   if constexpr (PACK == 2)                                                                   \
-    pair_range2<K, H, UNROLL>(PA, PB, PX, i0, i1, ax, ay, az, pq, psprow, f, acc);          \
+    pair_range2<H, UNROLL>(PA, PB, i0, i1, ax, ay, az, pq, f, acc);                          \
   else                                                                                       \
-    pair_range<K, H, UNROLL>(PA, PB, PX, i0, i1, ax[0], ay[0], az[0], pq, psprow, f, acc[0])
-  switch (kind) {
-    case 0: GD_PR(0, false); break;
-    case 1: GD_PR(1, false); break;
-    case 2: GD_PR(2, false); break;
-    case 3: GD_PR(3, false); break;
-    case 4: GD_PR(0, true); break;
-    case 5: GD_PR(1, true); break;
-    case 6: GD_PR(2, true); break;
-    default: GD_PR(3, true); break;
+    pair_range<H, UNROLL>(PA, PB, i0, i1, ax[0], ay[0], az[0], pq, f, acc[0])
+  if (flags & 4) {
+    GD_PR(true);
+  } else {
+    GD_PR(false);
   }
 #undef GD_PR
 }
@@ -373,11 +424,12 @@ __global__ void __launch_bounds__(GD_MAX_TPB / PACK, GD_MIN_BLOCKS_PACK(UNROLL, 
   /* T: lanes of the tile (PACK per thread), the stride of the placed atoms and partials */
   const int NT = blockDim.x, T = NT * PACK, tid = threadIdx.x, D = a.chunk;
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem);
-  /* ring buffers: buffer b holds D slots as D/2 pairs in three float4 streams */
-  float4 *bpa = reinterpret_cast<float4 *>(smem + 16);
+  /* contact thresholds [ligand type][point type], then the ring buffers: buffer b holds D
+   * slots as D/2 pairs in two float4 streams */
+  float *thr_s = reinterpret_cast<float *>(smem + 16);
+  float4 *bpa = reinterpret_cast<float4 *>(smem + 16 + GD_THR_BYTES);
   float4 *bpb = bpa + D;
-  float4 *bpx = bpb + D;
-  float4 *atoms = bpx + D;
+  float4 *atoms = bpb + D;
   double *part = reinterpret_cast<double *>(atoms + T);
   Slot *slots = reinterpret_cast<Slot *>(part + NQ * T);
   __shared__ int s_tile, s_abort;
@@ -392,6 +444,7 @@ __global__ void __launch_bounds__(GD_MAX_TPB / PACK, GD_MIN_BLOCKS_PACK(UNROLL, 
     s_done[0] = s_done[1] = 0;
     s_issued[0] = s_issued[1] = 0;
   }
+  for (int i = tid; i < GD_MAXTP2 * GD_MAXTP1; i += NT) thr_s[i] = a.pp[i].thr;
   __syncthreads();
   uint32_t consumed0 = 0, consumed1 = 0; /* completed phases waited for, per buffer */
   const int step_first = a.step0 + (a.step_base ? *a.step_base : 0);
@@ -469,7 +522,7 @@ __global__ void __launch_bounds__(GD_MAX_TPB / PACK, GD_MIN_BLOCKS_PACK(UNROLL, 
     /* ---- protein tile pipeline ---- */
     const int pc = tile.prt_conf;
     const size_t pbase = (size_t)pc * (cx.pnp_pad >> 1);
-    const float4 *ga = cx.pt_a + pbase, *gb = cx.pt_b + pbase, *gx = cx.pt_x + pbase;
+    const float4 *ga = cx.pt_a + pbase, *gb = cx.pt_b + pbase;
     const int P = cx.pnp, pnp_pad = cx.pnp_pad;
     const int nch = (pnp_pad + D - 1) / D;
     const bool resident = nch <= 2;
@@ -480,10 +533,9 @@ __global__ void __launch_bounds__(GD_MAX_TPB / PACK, GD_MIN_BLOCKS_PACK(UNROLL, 
       for (int q = 0; q < min(2, total_q); ++q) {
         const int b = q & 1, c0 = q * D, n = min(D, pnp_pad - c0);
         s_issued[b] += 1;
-        mbar_expect_tx(&bar[b], (uint32_t)(n * 24));
+        mbar_expect_tx(&bar[b], (uint32_t)(n * 16));
         bulk_g2s(bpa + b * (D >> 1), ga + (c0 >> 1), (uint32_t)(n * 8), &bar[b]);
         bulk_g2s(bpb + b * (D >> 1), gb + (c0 >> 1), (uint32_t)(n * 8), &bar[b]);
-        bulk_g2s(bpx + b * (D >> 1), gx + (c0 >> 1), (uint32_t)(n * 8), &bar[b]);
       }
     }
     __syncthreads();
@@ -558,9 +610,6 @@ __global__ void __launch_bounds__(GD_MAX_TPB / PACK, GD_MIN_BLOCKS_PACK(UNROLL, 
 #pragma unroll
       for (int qi = 0; qi < NQ; ++qi)
         for (int i = tid; i < T; i += NT) part[qi * T + i] = 0.0;
-      int ncon[PACK];
-#pragma unroll
-      for (int h = 0; h < PACK; ++h) ncon[h] = 0;
 
       /* ---- CalcEnergy_d pair loop over the protein ring ---- */
       for (int ci = 0; ci < nch; ++ci) {
@@ -580,7 +629,6 @@ __global__ void __launch_bounds__(GD_MAX_TPB / PACK, GD_MIN_BLOCKS_PACK(UNROLL, 
         if (active) {
           const float4 *PA = bpa + b * (D >> 1); /* local slot = slot - c0 */
           const float4 *PB = bpb + b * (D >> 1);
-          const float4 *PX = bpx + b * (D >> 1);
           const int c0 = ci * D, c1 = min(pnp_pad, c0 + D);
           for (int sg = 0; sg < nseg; ++sg) {
             const int4 g = segs[sg];
@@ -597,14 +645,14 @@ __global__ void __launch_bounds__(GD_MAX_TPB / PACK, GD_MIN_BLOCKS_PACK(UNROLL, 
             const float4 *pr = reinterpret_cast<const float4 *>(pprow + g.z);
             const float4 q0 = __ldg(pr), q1 = __ldg(pr + 1), q2 = __ldg(pr + 2);
             Pair2 pq;
-            pq.p1a = f2(q0.x); pq.mp2a = f2(-q0.y); pq.p1l = f2(q0.z); pq.thr = q0.w;
+            pq.p1a = f2(q0.x); pq.mp2a = f2(-q0.y); pq.p1l = f2(q0.z);
             pq.pmf1 = f2(q1.y); pq.hc1 = f2(q1.z); pq.hc0 = f2(q1.w);
             pq.hs = f2(q2.x); pq.b2 = f2(q2.z); pq.c2 = f2(q2.w);
             const float2 z2 = f2(0.0f);
             Acc acc[PACK];
 #pragma unroll
-            for (int h = 0; h < PACK; ++h) acc[h] = {z2, z2, z2, z2, z2, z2, 0.0f};
-            pair_dispatch<UNROLL, PACK>(g.w, PA, PB, PX, i0, i1, ax, ay, az, pq, psprow, f, acc);
+            for (int h = 0; h < PACK; ++h) acc[h] = {z2, z2, z2, z2};
+            pair_dispatch<UNROLL, PACK>(g.w, PA, PB, i0, i1, ax, ay, az, pq, f, acc);
 #pragma unroll
             for (int h = 0; h < PACK; ++h) {
               if (!ok[h]) continue;
@@ -612,10 +660,7 @@ __global__ void __launch_bounds__(GD_MAX_TPB / PACK, GD_MIN_BLOCKS_PACK(UNROLL, 
               part[0 * T + v] += (double)acc[h].vdw.x + (double)acc[h].vdw.y;
               part[1 * T + v] += (double)acc[h].ele.x + (double)acc[h].ele.y;
               part[2 * T + v] += (double)acc[h].pmf.x + (double)acc[h].pmf.y;
-              part[3 * T + v] += (double)acc[h].psp;
               part[4 * T + v] += (double)acc[h].hdb.x + (double)acc[h].hdb.y;
-              part[5 * T + v] += (double)acc[h].hsum.x + (double)acc[h].hsum.y;
-              ncon[h] += (int)(acc[h].ncon.x + acc[h].ncon.y);
             }
           }
         }
@@ -631,34 +676,31 @@ __global__ void __launch_bounds__(GD_MAX_TPB / PACK, GD_MIN_BLOCKS_PACK(UNROLL, 
                 const int c0 = ((q + 2) % nch) * D, n = min(D, pnp_pad - c0);
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 s_issued[b] += 1;
-                mbar_expect_tx(&bar[b], (uint32_t)(n * 24));
+                mbar_expect_tx(&bar[b], (uint32_t)(n * 16));
                 bulk_g2s(bpa + b * (D >> 1), ga + (c0 >> 1), (uint32_t)(n * 8), &bar[b]);
                 bulk_g2s(bpb + b * (D >> 1), gb + (c0 >> 1), (uint32_t)(n * 8), &bar[b]);
-                bulk_g2s(bpx + b * (D >> 1), gx + (c0 >> 1), (uint32_t)(n * 8), &bar[b]);
               }
             }
           }
         }
       }
 
-      /* ---- per-atom tail: hpc, kde, rmsd, reference contacts (split 0 of each atom) ---- */
-      if (S > 1) {
-        /* hpc is nonlinear in the atom's hydrophobic sum: gather the splits' parts first */
-        __syncthreads();
-        if (active && sp == 0)
-          for (int q = 1; q < S; ++q) {
-            part[5 * T + tid] += part[5 * T + tid + q * L];
-            part[5 * T + tid + q * L] = 0.0;
-          }
-      }
+      /* ---- per-atom tail (split 0 of each atom): the short-range terms from the cell list,
+       * hpc, kde, rmsd, reference contacts ---- */
 #pragma unroll
       for (int h = 0; h < PACK; ++h) {
         if (!ok[h] || aborted) continue;
         const int v = vl[h];
-        part[1 * T + v] *= (double)orig[h].w;
-        part[8 * T + v] = (double)ncon[h];
-        if (sp != 0) continue;
-        const double hpc2 = (part[5 * T + v] - (double)f.hpl0[tl]) / (double)f.hpl1[tl];
+        if (sp != 0) {
+          part[1 * T + v] *= (double)orig[h].w;
+          continue;
+        }
+        ShortSums sr;
+        short_range(cx, pc, thr_s + tl * GD_MAXTP1, psprow, f, ax[h], ay[h], az[h], sr);
+        part[1 * T + v] = (part[1 * T + v] + (double)sr.ele) * (double)orig[h].w;
+        part[3 * T + v] = (double)sr.psp;
+        part[8 * T + v] = (double)sr.ncon;
+        const double hpc2 = (sr.hsum - (double)f.hpl0[tl]) / (double)f.hpl1[tl];
         part[5 * T + v] = 0.5 * hpc2 * hpc2 - (double)f.hpl2[tl];
         float ks = 0.0f;
         int kn = 0;
