@@ -964,12 +964,13 @@ def profile_da(args):
 
 
 def profile_mc(args):
-    """A short plain run on a 128-replica subset of the config-1 system (8 ligand conformers,
-    2 protein conformers, 8 temperatures, no records): four 10-step launches, small enough for
-    multi-pass profiler captures."""
+    """A short plain run on a subset of the config-1 system (--profile-subset ligand
+    conformers, protein conformers, temperatures; default 8, 2, 8 = 128 replicas; no records):
+    four 10-step launches, small enough for multi-pass profiler captures."""
     from geaxdock_gpu_b200 import engine
     w = workload(42)
-    cx = w.complexes[0].subset(n_lig=8, n_prt=2, n_tmp=8)
+    nl, npc, nt = (int(v) for v in args.profile_subset.split(","))
+    cx = w.complexes[0].subset(n_lig=nl, n_prt=npc, n_tmp=nt)
     params = w.params
     params.record = 0
     tile = tuple(int(v) for v in args.tile.split(",")) if args.tile else (6, 1024, 2)
@@ -1088,8 +1089,11 @@ def main():
     ap.add_argument("--move-mult", type=float, default=1.0,
                     help="--profile-da / --screen-da: move scales multiplied by this factor")
     ap.add_argument("--profile-mc", action="store_true",
-                    help="only a short plain run on a 128-replica subset of the config-1 system "
-                         "(four 10-step launches), for multi-pass profiler captures")
+                    help="only a short plain run on a subset of the config-1 system (four "
+                         "10-step launches), for multi-pass profiler captures")
+    ap.add_argument("--profile-subset", default="8,2,8",
+                    help="--profile-mc: ligand conformers, protein conformers and temperatures "
+                         "of the config-1 subset (default 128 replicas)")
     ap.add_argument("--profile-screen", action="store_true",
                     help="only a short plain run on a --screen-ligands slice of the config-2 "
                          "screen (four 10-step launches), for multi-pass profiler captures")

@@ -2,8 +2,9 @@
 
 The fused kernel's tile is (replicas per CTA, protein points per shared-memory chunk, point
 pairs in flight per lane, protein split, CTA lanes in fill mode, replicas per thread).
-`tune(engine)` times a candidate grid with gd_autotune (pose
-evaluation of the chains' current poses, chains untouched), applies the fastest and stores it
+`tune(engine)` times a candidate grid with gd_autotune (Monte Carlo
+steps of every replica from a copy of the chain state, which is put back), applies the fastest
+and stores it
 in a JSON cache keyed by (ligand atoms, protein points, replicas, device name); later engines
 with the same key reuse the entry without timing.
 """

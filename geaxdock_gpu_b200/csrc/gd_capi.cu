@@ -1048,20 +1048,21 @@ int gd_autotune(gd_ctx *c, const gd_tile *cand, int n_cand, int repeats, gd_tile
     return fail(GD_ERR_INVALID, "gd_autotune: bad arguments");
   CK(cudaSetDevice(c->device));
   CK(cudaStreamSynchronize(c->stream));
-  /* the probe evaluates pose id == replica id: poses are the chains' mm_old, ligand
-   * conformer per pose from the replica table */
-  std::vector<gd_replica> rep(c->n_rep);
-  CK(cudaMemcpy(rep.data(), c->d_replica, sizeof(gd_replica) * c->n_rep, cudaMemcpyDeviceToHost));
-  std::vector<int> lc(c->n_rep);
-  for (int r = 0; r < c->n_rep; ++r) lc[r] = rep[r].idx_lig;
-  int *d_lc = nullptr;
-  gd_energy *d_e = nullptr;
-  CK(cudaMalloc(&d_lc, sizeof(int) * c->n_rep));
-  if (cudaMalloc(&d_e, sizeof(gd_energy) * c->n_rep) != cudaSuccess) {
-    cudaFree(d_lc);
-    return fail(GD_ERR_NOMEM, "gd_autotune: no memory for the probe");
-  }
-  cudaMemcpy(d_lc, lc.data(), sizeof(int) * c->n_rep, cudaMemcpyHostToDevice);
+  /* the probe runs Monte Carlo steps of every replica (no records, no trace) from a copy of
+   * the chain state, which is put back afterwards: the chains are left as they were */
+  const size_t R = (size_t)c->n_rep;
+  const size_t bytes = R * (6 * sizeof(float) + sizeof(gd_energy) + sizeof(float) + sizeof(int));
+  char *keep = nullptr;
+  if (cudaMalloc(&keep, bytes) != cudaSuccess)
+    return fail(GD_ERR_NOMEM, "gd_autotune: no memory for the copy of the chain state");
+  float *k_mm = reinterpret_cast<float *>(keep);
+  gd_energy *k_e = reinterpret_cast<gd_energy *>(k_mm + R * 6);
+  float *k_et = reinterpret_cast<float *>(k_e + R);
+  int *k_na = reinterpret_cast<int *>(k_et + R);
+  cudaMemcpyAsync(k_mm, c->d_mm, R * 6 * sizeof(float), cudaMemcpyDeviceToDevice, c->stream);
+  cudaMemcpyAsync(k_e, c->d_eold, R * sizeof(gd_energy), cudaMemcpyDeviceToDevice, c->stream);
+  cudaMemcpyAsync(k_et, c->d_etotal, R * sizeof(float), cudaMemcpyDeviceToDevice, c->stream);
+  cudaMemcpyAsync(k_na, c->d_nacc, R * sizeof(int), cudaMemcpyDeviceToDevice, c->stream);
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
@@ -1072,6 +1073,9 @@ int gd_autotune(gd_ctx *c, const gd_tile *cand, int n_cand, int repeats, gd_tile
   const int keep_threads = c->threads;
   int best_i = -1, rc = GD_OK;
   float best_ms = 1e30f;
+  /* steps per probe launch: an exchange interval, fewer when one step of the first candidate
+   * already takes long (large batches), so that the probe stays short */
+  int probe_steps = 0;
   for (int i = 0; i < n_cand && rc == GD_OK; ++i) {
     if ((rc = gd_set_tile(c, -1, &cand[i])) != GD_OK) {
       /* a candidate that does not fit this batch is skipped */
@@ -1082,13 +1086,26 @@ int gd_autotune(gd_ctx *c, const gd_tile *cand, int n_cand, int repeats, gd_tile
     int n = 0;
     if ((rc = upload_tiles(c, 0, c->n_rep - 1, &n))) break;
     GdMcArgs a = base_args(c);
-    a.mode = 2;
-    a.n_steps = 1;
-    a.mm_in = c->d_mm;
-    a.lig_conf_in = d_lc;
-    a.e_out = d_e;
+    a.mode = 0;
+    a.step0 = 0;
     a.rec = nullptr;
     a.trace_e = nullptr;
+    a.trace_acc = nullptr;
+    if (probe_steps == 0) {
+      a.n_steps = 1;
+      if ((rc = launch_mc(c, a, c->d_tiles, n, c->d_counters))) break; /* loads the kernel */
+      cudaEventRecord(e0, c->stream);
+      if ((rc = launch_mc(c, a, c->d_tiles, n, c->d_counters))) break;
+      cudaEventRecord(e1, c->stream);
+      if (cudaEventSynchronize(e1) != cudaSuccess) {
+        rc = fail(GD_ERR_CUDA, "gd_autotune: probe failed");
+        break;
+      }
+      float t1 = 0.0f;
+      cudaEventElapsedTime(&t1, e0, e1);
+      probe_steps = std::max(1, std::min(c->mc.steps_per_exchange, (int)(20.0f / std::max(t1, 1e-3f))));
+    }
+    a.n_steps = probe_steps;
     if ((rc = launch_mc(c, a, c->d_tiles, n, c->d_counters))) break; /* warm-up */
     cudaEventRecord(e0, c->stream);
     for (int r = 0; r < repeats && rc == GD_OK; ++r)
@@ -1100,17 +1117,22 @@ int gd_autotune(gd_ctx *c, const gd_tile *cand, int n_cand, int repeats, gd_tile
     }
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, e0, e1);
-    ms /= (float)repeats;
+    ms /= (float)(repeats * probe_steps);
     if (ms_out) ms_out[i] = ms;
     if (ms < best_ms) {
       best_ms = ms;
       best_i = i;
     }
   }
+  cudaMemcpyAsync(c->d_mm, k_mm, R * 6 * sizeof(float), cudaMemcpyDeviceToDevice, c->stream);
+  cudaMemcpyAsync(c->d_eold, k_e, R * sizeof(gd_energy), cudaMemcpyDeviceToDevice, c->stream);
+  cudaMemcpyAsync(c->d_etotal, k_et, R * sizeof(float), cudaMemcpyDeviceToDevice, c->stream);
+  cudaMemcpyAsync(c->d_nacc, k_na, R * sizeof(int), cudaMemcpyDeviceToDevice, c->stream);
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess && rc == GD_OK)
+    rc = fail(GD_ERR_CUDA, "gd_autotune: restoring the chain state failed");
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  cudaFree(d_lc);
-  cudaFree(d_e);
+  cudaFree(keep);
   if (rc == GD_OK && best_i >= 0) {
     rc = gd_set_tile(c, -1, &cand[best_i]);
     *best = cand[best_i];

@@ -217,10 +217,11 @@ int gd_set_tile(gd_ctx *ctx, int complex_index, const gd_tile *tile);
 int gd_get_tile(const gd_ctx *ctx, int complex_index, gd_tile *tile);
 /* replicas per CTA the tile gives complex k (differs between complexes in fill mode) */
 int gd_get_replicas_per_cta(const gd_ctx *ctx, int complex_index, int *replicas);
-/* Autotuner: times each candidate tile by evaluating the energies of the replicas' current
- * poses (the pair loop of gd_mc_run, without touching the chains), `repeats` launches each,
- * applies the fastest to every complex and returns it with its mean launch time (ms) in
- * ms_out[i] per candidate (may be null). */
+/* Autotuner: times each candidate tile by Monte Carlo steps of every replica (gd_mc_run
+ * without records or trace; an exchange interval per launch, fewer for batches where one step
+ * takes over 2 ms), `repeats` launches each, from a copy of the chain state that is put back
+ * afterwards (the chains are left as they were); applies the fastest to every complex and
+ * returns it with its mean time per step (ms) in ms_out[i] per candidate (may be null). */
 int gd_autotune(gd_ctx *ctx, const gd_tile *candidates, int n_candidates, int repeats,
                 gd_tile *best, float *ms_out);
 /* Independent replica chains that gd_mc_run_fused (default 1) and the delayed-acceptance loops
