@@ -2,11 +2,11 @@
 
 The fused kernel's tile is (replicas per CTA, protein points per shared-memory chunk, point
 pairs in flight per lane, protein split, CTA lanes in fill mode, replicas per thread).
-`tune(engine)` times a candidate grid with gd_autotune (Monte Carlo
-steps of every replica from a copy of the chain state, which is put back), applies the fastest
-and stores it
-in a JSON cache keyed by (ligand atoms, protein points, replicas, device name); later engines
-with the same key reuse the entry without timing.
+`tune(engine)` times a candidate grid with gd_autotune (Monte Carlo steps of every replica,
+each candidate from the same copy of the chain state, which is put back afterwards), re-times
+the fastest few with more launches, applies the fastest and stores it in a JSON cache keyed by
+(ligand atoms, protein points, replicas, device name); later engines with the same key reuse
+the entry without timing.
 """
 from __future__ import annotations
 
@@ -80,7 +80,7 @@ def time_candidates(eng: Engine, cands: Sequence[Tuple[int, ...]], repeats: int 
 
 
 def tune(eng: Engine, cache_path: Optional[str] = DEFAULT_CACHE, device: int = 0,
-         repeats: int = 2, force: bool = False) -> Dict:
+         repeats: int = 2, force: bool = False, finalists: int = 4) -> Dict:
     name = _device_name(device)
     key = _key(eng, name)
     cache = {}
@@ -96,8 +96,17 @@ def tune(eng: Engine, cache_path: Optional[str] = DEFAULT_CACHE, device: int = 0
     ragged = len({c.lna for c in eng.complexes}) > 1
     cands = candidates(lna, ragged)
     best, ms = time_candidates(eng, cands, repeats)
+    # second round: the fastest few again with more launches each, since neighbours in the
+    # first round's ranking are often within its noise
+    ranked = sorted((m, i) for i, m in enumerate(ms) if m > 0)
+    final = [cands[i] for _, i in ranked[:finalists]]
+    final_ms = []
+    if len(final) > 1:
+        best, final_ms = time_candidates(eng, final, 3 * repeats)
     entry = {"tile": list(best),
-             "ms": {",".join(str(v) for v in c): round(m, 4) for c, m in zip(cands, ms)}}
+             "ms": {",".join(str(v) for v in c): round(m, 4) for c, m in zip(cands, ms)},
+             "final_ms": {",".join(str(v) for v in c): round(m, 4)
+                          for c, m in zip(final, final_ms)}}
     cache[key] = entry
     if cache_path:
         try:

@@ -1085,6 +1085,12 @@ int gd_autotune(gd_ctx *c, const gd_tile *cand, int n_cand, int repeats, gd_tile
     }
     int n = 0;
     if ((rc = upload_tiles(c, 0, c->n_rep - 1, &n))) break;
+    /* every candidate starts from the same chain state (the cost of a step depends on where
+     * the ligands are) */
+    cudaMemcpyAsync(c->d_mm, k_mm, R * 6 * sizeof(float), cudaMemcpyDeviceToDevice, c->stream);
+    cudaMemcpyAsync(c->d_eold, k_e, R * sizeof(gd_energy), cudaMemcpyDeviceToDevice, c->stream);
+    cudaMemcpyAsync(c->d_etotal, k_et, R * sizeof(float), cudaMemcpyDeviceToDevice, c->stream);
+    cudaMemcpyAsync(c->d_nacc, k_na, R * sizeof(int), cudaMemcpyDeviceToDevice, c->stream);
     GdMcArgs a = base_args(c);
     a.mode = 0;
     a.step0 = 0;
