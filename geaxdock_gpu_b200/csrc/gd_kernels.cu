@@ -607,9 +607,26 @@ __global__ void __launch_bounds__(GD_MAX_TPB / PACK, GD_MIN_BLOCKS_PACK(UNROLL, 
           if (ok[h]) atoms[vl[h]] = make_float4(ax[h], ay[h], az[h], 0.0f);
         }
       }
+      /* each lane clears its own partials (the only ones the epilogue reads) */
 #pragma unroll
-      for (int qi = 0; qi < NQ; ++qi)
-        for (int i = tid; i < T; i += NT) part[qi * T + i] = 0.0;
+      for (int h = 0; h < PACK; ++h)
+        if (ok[h])
+#pragma unroll
+          for (int qi = 0; qi < NQ; ++qi) part[qi * T + vl[h]] = 0.0;
+
+      /* ---- short-range terms from the cell list (split 0 of each atom), before the pair
+       * loop: warps whose walk is short start the loop while the others still walk ---- */
+#pragma unroll
+      for (int h = 0; h < PACK; ++h) {
+        if (!ok[h] || sp != 0) continue;
+        ShortSums sr;
+        short_range(cx, pc, thr_s + tl * GD_MAXTP1, psprow, f, ax[h], ay[h], az[h], sr);
+        const int v = vl[h];
+        part[1 * T + v] = (double)sr.ele;
+        part[3 * T + v] = (double)sr.psp;
+        part[5 * T + v] = sr.hsum;
+        part[8 * T + v] = (double)sr.ncon;
+      }
 
       /* ---- CalcEnergy_d pair loop over the protein ring ---- */
       for (int ci = 0; ci < nch; ++ci) {
@@ -685,22 +702,14 @@ __global__ void __launch_bounds__(GD_MAX_TPB / PACK, GD_MIN_BLOCKS_PACK(UNROLL, 
         }
       }
 
-      /* ---- per-atom tail (split 0 of each atom): the short-range terms from the cell list,
-       * hpc, kde, rmsd, reference contacts ---- */
+      /* ---- per-atom tail (split 0 of each atom): hpc, kde, rmsd, reference contacts ---- */
 #pragma unroll
       for (int h = 0; h < PACK; ++h) {
         if (!ok[h] || aborted) continue;
         const int v = vl[h];
-        if (sp != 0) {
-          part[1 * T + v] *= (double)orig[h].w;
-          continue;
-        }
-        ShortSums sr;
-        short_range(cx, pc, thr_s + tl * GD_MAXTP1, psprow, f, ax[h], ay[h], az[h], sr);
-        part[1 * T + v] = (part[1 * T + v] + (double)sr.ele) * (double)orig[h].w;
-        part[3 * T + v] = (double)sr.psp;
-        part[8 * T + v] = (double)sr.ncon;
-        const double hpc2 = (sr.hsum - (double)f.hpl0[tl]) / (double)f.hpl1[tl];
+        part[1 * T + v] *= (double)orig[h].w;
+        if (sp != 0) continue;
+        const double hpc2 = (part[5 * T + v] - (double)f.hpl0[tl]) / (double)f.hpl1[tl];
         part[5 * T + v] = 0.5 * hpc2 * hpc2 - (double)f.hpl2[tl];
         float ks = 0.0f;
         int kn = 0;
