@@ -78,6 +78,32 @@ cudaError_t d2h_rows(void *dst, size_t hpitch, const void *src, size_t dpitch, s
   return cudaMemcpy2D(dst, hpitch, src, dpitch, width, n, cudaMemcpyDeviceToHost);
 }
 
+namespace {
+std::mutex g_pool_mu;
+cudaMemPool_t g_pool[GD_MAX_DEVICES] = {};
+}  // namespace
+
+cudaMemPool_t ctx_pool(int device) {
+  if (device < 0 || device >= GD_MAX_DEVICES) return nullptr;
+  std::lock_guard<std::mutex> lock(g_pool_mu);
+  if (!g_pool[device]) {
+    cudaMemPoolProps props;
+    memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    g_pool[device] = pool;
+  }
+  return g_pool[device];
+}
+
 int check_complex(const gd_complex_desc &d, int idx) {
   if (d.n_lig < 1 || d.n_prt < 1 || d.n_tmp < 1)
     return fail(GD_ERR_INVALID, "complex %d: n_lig/n_prt/n_tmp must be >= 1", idx);
@@ -177,11 +203,34 @@ size_t smem_bytes(const gd_ctx *c) {
 
 int ensure_counters(gd_ctx *c, int n) {
   if (n <= c->counters_cap) return GD_OK;
+  if (c->d_counters) {
+    /* the captured graphs point at the old counters: finish them and drop them first */
+    CK(cudaStreamSynchronize(c->stream));
+    for (auto &g : c->graphs) cudaGraphExecDestroy(g.second);
+    c->graphs.clear();
+  }
   int *p = nullptr;
-  CK(cudaMalloc(&p, sizeof(int) * n));
-  if (c->d_counters) cudaFree(c->d_counters);
+  cudaMemPool_t pool = ctx_pool(c->device);
+  if (pool) {
+    CK(cudaMallocFromPoolAsync(reinterpret_cast<void **>(&p), sizeof(int) * n, pool,
+                               c->stream));
+  } else {
+    CK(cudaMalloc(&p, sizeof(int) * n));
+  }
+  if (c->d_counters) {
+    if (c->counters_pooled)
+      cudaFreeAsync(c->d_counters, c->stream);
+    else
+      cudaFree(c->d_counters);
+  }
   c->d_counters = p;
   c->counters_cap = n;
+  c->counters_pooled = pool != nullptr;
+  return GD_OK;
+}
+
+int ensure_cursor(gd_ctx *c) {
+  if (!c->h_cursor) CK(cudaMallocHost(&c->h_cursor, 2 * sizeof(int)));
   return GD_OK;
 }
 
@@ -524,8 +573,11 @@ int gd_destroy(gd_ctx *c) {
   rs_stop(c);
   drop_graphs(c);
   da_free(c);
+  for (void *p : c->pool_allocs) cudaFreeAsync(p, c->stream);
+  if (c->d_counters && c->counters_pooled) cudaFreeAsync(c->d_counters, c->stream);
+  if (!c->pool_allocs.empty() || c->counters_pooled) cudaStreamSynchronize(c->stream);
   for (void *p : c->allocs) cudaFree(p);
-  if (c->d_counters) cudaFree(c->d_counters);
+  if (c->d_counters && !c->counters_pooled) cudaFree(c->d_counters);
   if (c->d_trace_e) cudaFree(c->d_trace_e);
   if (c->d_trace_acc) cudaFree(c->d_trace_acc);
   if (c->d_mm_in) cudaFree(c->d_mm_in);
@@ -541,6 +593,16 @@ int gd_destroy(gd_ctx *c) {
   if (c->ev_fork) cudaEventDestroy(c->ev_fork);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
+  return GD_OK;
+}
+
+int gd_release_memory(int device) {
+  if (device < 0 || device >= GD_MAX_DEVICES) return fail(GD_ERR_INVALID, "device %d", device);
+  std::lock_guard<std::mutex> lock(g_pool_mu);
+  if (g_pool[device]) {
+    CK(cudaSetDevice(device));
+    CK(cudaMemPoolTrimTo(g_pool[device], 0));
+  }
   return GD_OK;
 }
 
@@ -570,11 +632,13 @@ int gd_create(const gd_enepara *ff, const gd_complex_desc *cxs, int n_complexes,
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1)
     return fail(GD_ERR_NODEVICE, "no CUDA device");
   if (device < 0 || device >= ndev) return fail(GD_ERR_NODEVICE, "device %d absent", device);
-  cudaDeviceProp prop;
-  CK(cudaGetDeviceProperties(&prop, device));
-  if (prop.major < 10)
+  int cc_major = 0, cc_minor = 0, n_sms = 0;
+  CK(cudaDeviceGetAttribute(&cc_major, cudaDevAttrComputeCapabilityMajor, device));
+  CK(cudaDeviceGetAttribute(&cc_minor, cudaDevAttrComputeCapabilityMinor, device));
+  CK(cudaDeviceGetAttribute(&n_sms, cudaDevAttrMultiProcessorCount, device));
+  if (cc_major < 10)
     return fail(GD_ERR_NODEVICE, "device %d is sm_%d%d; this library is built for sm_100a",
-                device, prop.major, prop.minor);
+                device, cc_major, cc_minor);
   CK(cudaSetDevice(device));
 
   {
@@ -585,7 +649,7 @@ int gd_create(const gd_enepara *ff, const gd_complex_desc *cxs, int n_complexes,
   gd_ctx *c = new gd_ctx();
   c->device = device;
   c->mc = *mc;
-  c->num_sms = prop.multiProcessorCount;
+  c->num_sms = n_sms;
   c->n_complex = n_complexes;
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
     delete c;
@@ -923,7 +987,9 @@ int gd_create(const gd_enepara *ff, const gd_complex_desc *cxs, int n_complexes,
   CK(cudaMemsetAsync(c->d_err, 0, sizeof(unsigned), c->stream));
   c->rec_cap = mc->steps_per_dump + 1;
   if (mc->record) {
+    /* cleared: rows past a replica's count read as zeros, not as an earlier context's data */
     if ((rc = dalloc(c, &c->d_rec, (size_t)R * c->rec_cap))) return bail(rc);
+    CK(cudaMemsetAsync(c->d_rec, 0, sizeof(gd_record_step) * R * c->rec_cap, c->stream));
   }
 
   /* ---- tiles ---- */
@@ -941,7 +1007,6 @@ int gd_create(const gd_enepara *ff, const gd_complex_desc *cxs, int n_complexes,
   if ((rc = dalloc(c, &c->d_tiles, c->tiles_cap))) return bail(rc);
   if ((rc = ensure_counters(c, 64))) return bail(rc);
   if ((rc = dalloc(c, &c->d_cursor, 2))) return bail(rc);
-  CK(cudaMallocHost(&c->h_cursor, 2 * sizeof(int)));
   CK(cudaStreamSynchronize(c->stream));
   *out = c;
   return GD_OK;
@@ -1329,6 +1394,7 @@ int gd_mc_run_fused(gd_ctx *c, int s1, int n_steps, int exchange) {
   }
   /* the graph reads its step and exchange-call bases from the device cursor */
   CK(cudaStreamSynchronize(c->stream));
+  if ((rc = ensure_cursor(c))) return rc;
   c->h_cursor[0] = s1;
   c->h_cursor[1] = c->exchange_calls;
   CK(cudaMemcpyAsync(c->d_cursor, c->h_cursor, 2 * sizeof(int), cudaMemcpyHostToDevice,

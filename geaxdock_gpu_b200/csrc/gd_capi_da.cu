@@ -320,7 +320,12 @@ int da_graph(gd_ctx *c, int n_steps, int exchange, bool collect, int S, cudaGrap
   if (rc) return rc;
   const int nch = (int)chains.size();
   if (n_steps * nch > d->counters_cap) {
-    if (d->d_counters) cudaFree(d->d_counters);
+    if (d->d_counters) {
+      /* the cached graphs point at the old counters: finish them and drop them first */
+      CK(cudaStreamSynchronize(c->stream));
+      da_drop_graphs(c);
+      cudaFree(d->d_counters);
+    }
     d->d_counters = nullptr;
     d->counters_cap = 0;
     CK(cudaMalloc(&d->d_counters, sizeof(int) * n_steps * nch));
@@ -393,6 +398,7 @@ int da_run_steps(gd_ctx *c, int s1, int n_steps, int exchange, bool collect) {
   cudaGraphExec_t g;
   if ((rc = da_graph(c, n_steps, exchange, collect, S, &g))) return rc;
   CK(cudaStreamSynchronize(c->stream));
+  if ((rc = ensure_cursor(c))) return rc;
   c->h_cursor[0] = s1;
   c->h_cursor[1] = c->exchange_calls;
   CK(cudaMemcpyAsync(c->d_cursor, c->h_cursor, 2 * sizeof(int), cudaMemcpyHostToDevice,

@@ -106,7 +106,8 @@ struct gd_ctx {
                    threads / pack threads */
   int fill_threads = 0, fill_cap = 0; /* the last gd_set_tile in fill mode (threads > 0) */
   std::vector<gdc::ComplexInfo> info;
-  std::vector<void *> allocs;
+  std::vector<void *> allocs;      /* cudaMalloc'd buffers */
+  std::vector<void *> pool_allocs; /* buffers from the device's context pool (ctx_pool) */
   GdForceConst fc{};
   GdDevComplex *d_cx = nullptr;
   GdPairParam *d_pp = nullptr;
@@ -127,6 +128,7 @@ struct gd_ctx {
   std::vector<GdTileDesc> full_tiles;
   int *d_counters = nullptr; /* [counters_cap] persistent-CTA queue heads */
   int counters_cap = 0;
+  bool counters_pooled = false; /* d_counters came from ctx_pool */
   int *d_cursor = nullptr;   /* [2]: step base, exchange call base (graph replays) */
   int *h_cursor = nullptr;   /* pinned staging */
   unsigned *d_err = nullptr;
@@ -164,20 +166,31 @@ struct gd_ctx {
   struct RecStream *rs = nullptr;
 };
 
+#define GD_MAX_DEVICES 64
+
 namespace gdc {
 
 /* ---- the context's helpers (gd_capi.cu) ---- */
 cudaError_t d2h_rows(void *dst, size_t hpitch, const void *src, size_t dpitch, size_t width,
                      int n);
+/* The device's stream-ordered pool for the buffers gd_create sets up: it keeps freed memory
+ * (no release threshold), so gd_destroy returns buffers without unmapping them and the next
+ * context of the process reuses them; gd_release_memory trims it. Null if it cannot be made. */
+cudaMemPool_t ctx_pool(int device);
+/* n elements on the context's device, stream-ordered on its stream (gd_create synchronises
+ * the stream before any other stream sees the buffer), freed by gd_destroy */
 template <class T>
 int dalloc(gd_ctx *c, T **p, size_t n) {
   *p = nullptr;
   if (n == 0) n = 1;
   void *q = nullptr;
-  cudaError_t e = cudaMalloc(&q, n * sizeof(T));
+  cudaMemPool_t pool = ctx_pool(c->device);
+  cudaError_t e = pool ? cudaMallocFromPoolAsync(&q, n * sizeof(T), pool, c->stream)
+                       : cudaMalloc(&q, n * sizeof(T));
   if (e != cudaSuccess)
-    return fail(GD_ERR_NOMEM, "cudaMalloc(%zu) failed: %s", n * sizeof(T), cudaGetErrorString(e));
-  c->allocs.push_back(q);
+    return fail(GD_ERR_NOMEM, "allocation of %zu bytes failed: %s", n * sizeof(T),
+                cudaGetErrorString(e));
+  (pool ? c->pool_allocs : c->allocs).push_back(q);
   *p = (T *)q;
   return GD_OK;
 }
@@ -195,6 +208,8 @@ int pick_threads(const std::vector<ComplexInfo> &info);
 void build_tiles(const gd_ctx *c, int r0, int r1, std::vector<GdTileDesc> &out);
 size_t smem_bytes(const gd_ctx *c);
 int ensure_counters(gd_ctx *c, int n);
+/* the pinned host cursor of the graph launches (made on first use) */
+int ensure_cursor(gd_ctx *c);
 typedef void (*McKernel)(GdMcArgs, GdForceConst);
 McKernel mc_kernel(int unroll, int split, bool da = false, int pack = 1);
 int launch_pack(const gd_ctx *c, int split, bool da);

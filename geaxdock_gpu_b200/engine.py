@@ -47,6 +47,7 @@ def lib() -> C.CDLL:
         "gd_create": [C.POINTER(abi.EnePara), C.POINTER(abi.ComplexDesc), C.c_int,
                       C.POINTER(abi.McParams), C.c_int, C.POINTER(vp)],
         "gd_destroy": [vp],
+        "gd_release_memory": [C.c_int],
         "gd_num_replicas": [vp, ip],
         "gd_replica_offset": [vp, C.c_int, ip],
         "gd_set_tile": [vp, C.c_int, C.POINTER(abi.Tile)],
@@ -130,6 +131,12 @@ def set_temperature(n: int, floor_t: float, ceil_t: float) -> np.ndarray:
     t = (abi.Temp * n)()
     check(lib().gd_set_temperature(n, floor_t, ceil_t, t))
     return np.frombuffer(bytes(t), dtype=abi.TEMP_DTYPE).copy()
+
+
+def release_memory(device: int = 0):
+    """gd_release_memory: gives the device memory that destroyed contexts left in the
+    library's pool back to the driver."""
+    check(lib().gd_release_memory(device))
 
 
 def _p(a: np.ndarray):

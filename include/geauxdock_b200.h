@@ -209,7 +209,13 @@ int gd_set_replica(int n_prt, int n_tmp, int n_lig, gd_replica *out);
  * [offset_k, offset_k + n_prt*n_tmp*n_lig), offsets in the order given. */
 int gd_create(const gd_enepara *ff, const gd_complex_desc *complexes, int n_complexes,
               const gd_mc_params *mc, int device, gd_ctx **out);
+/* Frees the context (Run's cudaFree calls, src/run.cu:250-283). The device buffers gd_create
+ * made come from one memory pool per device that keeps freed memory for the next context of
+ * the process (no unmapping on the way out, no mapping on the way in). */
 int gd_destroy(gd_ctx *ctx);
+/* Returns the memory the device's context pool holds without a live context to the driver
+ * (no reference counterpart). */
+int gd_release_memory(int device);
 int gd_num_replicas(const gd_ctx *ctx, int *n_rep);
 int gd_replica_offset(const gd_ctx *ctx, int complex_index, int *offset);
 /* Tile of the fused kernel for one complex (-1: all); one CTA size per context. */
