@@ -55,27 +55,77 @@ float host_dist2(float ax, float ay, float az, float px, float py, float pz) {
  * host page (one thread faults pages in at about a quarter of the copy rate of resident pages),
  * so above 32 MB the destination rows are first written by up to 8 host threads in parallel,
  * then copied in one call. */
+namespace {
+/* page-locked staging buffers of the large downloads, one per copy thread, made on the first
+ * large download of the process and kept */
+constexpr int kStageThreads = 8;
+constexpr size_t kStageBytes = (size_t)8 << 20;
+std::mutex g_stage_mu;
+void *g_stage[kStageThreads] = {};
+}  // namespace
+
+/* n rows of `width` bytes from device memory (row pitch dpitch) into host memory (row pitch
+ * hpitch). Into pageable memory, a large copy runs on up to kStageThreads host threads, each
+ * taking the next chunk of rows: its own stream copies the chunk into its page-locked staging
+ * buffer, then the thread copies it into the destination (touching those pages for the first
+ * time), so the DMA engine fills one buffer while other threads empty theirs. The device
+ * rows must be complete (the caller synchronised the stream that wrote them). */
 cudaError_t d2h_rows(void *dst, size_t hpitch, const void *src, size_t dpitch, size_t width,
                      int n) {
   if (n < 1 || width == 0) return cudaSuccess;
-  int T = (int)std::min(8u, std::max(1u, std::thread::hardware_concurrency()));
-  if (width * (size_t)n < ((size_t)32 << 20)) T = 1;
-  T = std::min(T, n);
-  if (T > 1) {
-    auto touch = [&](int t) {
-      const int a = (int)((long long)n * t / T), b = (int)((long long)n * (t + 1) / T);
+  cudaPointerAttributes at;
+  const bool pinned =
+      cudaPointerGetAttributes(&at, dst) == cudaSuccess && at.type == cudaMemoryTypeHost;
+  cudaGetLastError();
+  if (pinned || width * (size_t)n < ((size_t)32 << 20) || width > kStageBytes)
+    return cudaMemcpy2D(dst, hpitch, src, dpitch, width, n, cudaMemcpyDeviceToHost);
+  std::lock_guard<std::mutex> lock(g_stage_mu);
+  const int T = (int)std::min<unsigned>(kStageThreads,
+                                        std::max(1u, std::thread::hardware_concurrency()));
+  for (int t = 0; t < T; ++t)
+    if (!g_stage[t]) {
+      cudaError_t e = cudaHostAlloc(&g_stage[t], kStageBytes, cudaHostAllocPortable);
+      if (e != cudaSuccess) {
+        g_stage[t] = nullptr;
+        cudaGetLastError();
+        return cudaMemcpy2D(dst, hpitch, src, dpitch, width, n, cudaMemcpyDeviceToHost);
+      }
+    }
+  int dev = 0;
+  cudaError_t e0 = cudaGetDevice(&dev);
+  if (e0 != cudaSuccess) return e0;
+  const int rows = (int)(kStageBytes / width);
+  const int chunks = (n + rows - 1) / rows;
+  std::atomic<int> next{0};
+  std::atomic<int> err{(int)cudaSuccess};
+  auto work = [&](int t) {
+    cudaError_t e = cudaSetDevice(dev);
+    cudaStream_t st = nullptr;
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    char *stage = static_cast<char *>(g_stage[t]);
+    for (int k = next++; e == cudaSuccess && k < chunks && err.load() == (int)cudaSuccess;
+         k = next++) {
+      const int a = k * rows, b = std::min(n, a + rows);
+      e = cudaMemcpy2DAsync(stage, width, static_cast<const char *>(src) + (size_t)a * dpitch,
+                            dpitch, width, b - a, cudaMemcpyDeviceToHost, st);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+      if (e != cudaSuccess) break;
       char *d = static_cast<char *>(dst) + (size_t)a * hpitch;
-      if (hpitch == width)
-        memset(d, 0, (size_t)(b - a) * width);
-      else
-        for (int i = a; i < b; ++i, d += hpitch) memset(d, 0, width);
-    };
-    std::vector<std::thread> th;
-    for (int t = 1; t < T; ++t) th.emplace_back(touch, t);
-    touch(0);
-    for (auto &x : th) x.join();
-  }
-  return cudaMemcpy2D(dst, hpitch, src, dpitch, width, n, cudaMemcpyDeviceToHost);
+      if (hpitch == width) {
+        memcpy(d, stage, (size_t)(b - a) * width);
+      } else {
+        for (int i = a; i < b; ++i, d += hpitch) memcpy(d, stage + (size_t)(i - a) * width, width);
+      }
+    }
+    if (st) cudaStreamDestroy(st);
+    if (e != cudaSuccess) err = (int)e;
+  };
+  const int nt = std::min(T, chunks);
+  std::vector<std::thread> th;
+  for (int t = 1; t < nt; ++t) th.emplace_back(work, t);
+  work(0);
+  for (auto &x : th) x.join();
+  return (cudaError_t)err.load();
 }
 
 namespace {
