@@ -1014,7 +1014,9 @@ def sweep(args):
     """Device time of one 10-step gd_mc_run on the config-1 system (no records): for each tile
     of --sweep-tiles over all replicas, and, at the first of them, over the first m protein-
     conformer blocks of 620 replicas (m = 1..11), with L2 flushed before every timed launch;
-    and the fused graph as 1..4 concurrent chains. Medians of 5 launches."""
+    and the fused graph as 1..4 concurrent chains. Medians of 5 launches, every measurement
+    from the same chain state (the one after 5 warm-up intervals; the cost of a step depends on
+    where the ligands are)."""
     import torch
     from geaxdock_gpu_b200 import engine
     w = workload(42)
@@ -1050,15 +1052,27 @@ def sweep(args):
                 s[0] += 10
             return f
 
+        for _ in range(5):
+            run()()
+        e.sync()
+        saved, s0 = e.state(), s[0]
+
+        def restore():
+            e.set_state(saved)
+            s[0] = s0
+
         for t in tiles:
             e.set_tile(*t)
+            restore()
             out["tiles"][",".join(map(str, t))] = timed(run())
         e.set_tile(*tiles[0])
         block = cx.n_tmp * cx.n_lig
         for m in range(1, cx.n_prt + 1):
+            restore()
             out["blocks"][m] = timed(run(m * block - 1))
         for ch in (1, 2, 3, 4):
             e.set_concurrency(ch, 3)
+            restore()
 
             def g():
                 e.run_fused(s[0], 10, exchange=True)

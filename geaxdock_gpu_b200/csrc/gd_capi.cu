@@ -364,11 +364,27 @@ int set_kernel_attrs(const gd_ctx *c, size_t smem, int split, bool da) {
   CK(cudaGetDevice(&dev));
   CK(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
   CK(cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev));
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, launch_threads(c, split, da), smem));
+  const int threads = launch_threads(c, split, da);
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, threads, smem));
   if (nb >= 1 && per_sm > 0) {
-    const double need = (double)nb * (double)(smem + (size_t)reserved);
-    const int pct = std::min(100, (int)std::ceil(100.0 * need / (double)per_sm));
+    /* the driver rounds the carveout up to one of the SM's shared-memory sizes; aim at the
+     * smallest of them that holds the CTAs (a percentage rounded up could cross into the
+     * next size and take the L1 the walk needs) */
+    static const int kSizesKB[] = {0, 8, 16, 32, 64, 100, 132, 164, 196, 228};
+    const long long need = (long long)nb * (long long)(smem + (size_t)reserved);
+    long long size = per_sm;
+    for (int kb : kSizesKB)
+      if ((long long)kb * 1024 >= need) {
+        size = std::min<long long>((long long)kb * 1024, per_sm);
+        break;
+      }
+    const int pct = std::max(1, std::min(100, (int)(100 * size / per_sm)));
     CK(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
+    int nb2 = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb2, k, threads, smem) != cudaSuccess ||
+        nb2 < nb)
+      CK(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
+                              cudaSharedmemCarveoutMaxShared));
   }
   return GD_OK;
 }
