@@ -189,6 +189,10 @@ int check_complex(const gd_complex_desc &d, int idx) {
     if (d.prt_c[i] == 2 && (d.prt_seq3r[i] < 0 || d.prt_seq3r[i] >= d.psp_ld))
       return fail(GD_ERR_INVALID, "complex %d: PSP column %d outside 0..%d", idx, d.prt_seq3r[i],
                   d.psp_ld - 1);
+    /* the short-range cell grid is laid over the points' bounding box */
+    if (!std::isfinite(d.prt_x[i]) || !std::isfinite(d.prt_y[i]) || !std::isfinite(d.prt_z[i]))
+      return fail(GD_ERR_INVALID, "complex %d: protein point %d has a non-finite coordinate", idx,
+                  i);
   }
   for (int i = 0; i < d.pnk; ++i)
     if (d.kde_t[i] < 0 || d.kde_t[i] >= GD_MAXTP2)

@@ -1,5 +1,6 @@
 """The C ABI library: loads, exports what include/geauxdock_b200.h declares, keeps the
 reference's byte layouts, and its host-only entry points work without a GPU."""
+import copy
 import ctypes as C
 import os
 import re
@@ -102,6 +103,14 @@ def test_invalid_arguments_are_rejected_with_a_message():
     rc = lib.gd_create(C.byref(ff), C.byref(d), 1, C.byref(params), 0, C.byref(h))
     assert rc == abi.GD_ERR_CAPACITY
     assert b"log(0/0)" in lib.gd_last_error_string()
+    # a protein point off the number line: no cell grid can hold it (checked before any device
+    # work, so this runs without a GPU)
+    nan = copy.deepcopy(cx)
+    nan.prt_y[0, 7] = np.nan
+    d = nan.desc()
+    rc = lib.gd_create(C.byref(ff), C.byref(d), 1, C.byref(params), 0, C.byref(h))
+    assert rc == abi.GD_ERR_INVALID
+    assert b"non-finite" in lib.gd_last_error_string()
 
 
 @pytest.mark.skipif(have_gpu(), reason="checks the no-device path")
