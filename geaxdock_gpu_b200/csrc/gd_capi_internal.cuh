@@ -240,6 +240,12 @@ void rs_stop(gd_ctx *c);
 void da_free(gd_ctx *c);
 void da_drop_graphs(gd_ctx *c);
 
+/* ---- the device layout of one complex (gd_capi_layout.cu) ---- */
+/* builds complex ci's arrays on the host, uploads them (pool memory, synchronised) and fills g;
+ * thr: the contact thresholds [ligand type][point type] */
+int layout_complex(gd_ctx *c, const gd_enepara *ff, const float (*thr)[GD_MAXTP1],
+                   const gd_complex_desc &d, int ci, GdDevComplex &g);
+
 /* ---- allocation-free pose evaluation (gd_capi_noalloc.cu) ---- */
 int noalloc_prepare(int device);
 
