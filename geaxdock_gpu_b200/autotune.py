@@ -35,7 +35,8 @@ def candidates(lna: int, ragged: bool = False,
     out = []
     for p in packs:
         for chunk in (256, 512, 1024):
-            for unroll in (1, 2):
+            # four point pairs in flight only with one replica per lane (no packed variant)
+            for unroll in ((1, 2, 4) if p == 1 else (1, 2)):
                 for k in ks:
                     out.append((k, chunk, unroll, 1, 0, p))
                 if ragged:
