@@ -794,11 +794,15 @@ def run_ours(args, rank, world, local_rank):
         e.mc_init()
         it2 = 0
         d2h = 0
-        windows = []  # each dump window's records, downloaded before the counters reset
+        # each dump window's filled records, downloaded before the counters reset into one host
+        # array reused from window to window, as the reference's launcher reuses its host
+        # LigRecord array (the records held per window are kept)
+        rec_host = np.empty(e.n_rep * e.cap, abi.RECORD_DTYPE)
+        held = []
 
         def download():
-            steps, nxt = e.records()
-            windows.append((steps, nxt))
+            steps, nxt = e.records(out=rec_host)
+            held.append(int(nxt.sum()))
             return steps.nbytes + nxt.nbytes
 
         for _ in range(args.steps):
@@ -819,11 +823,13 @@ def run_ours(args, rank, world, local_rank):
             dt = max_over_ranks(dt, dist)
         e2e = {"value": n_total * spe * args.steps / dt, "unit": UNIT,
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+               "records_downloaded": sum(held),
                "scope": "gd_create + gd_mc_init + K x (gd_mc_run + gd_exchange + "
                         "gd_get_etotal) + the filled record rows of every dump window "
-                        "(gd_get_record_counts + gd_get_records_raw, as the reference's launcher "
-                        "downloads LigRecord per dump) + gd_destroy, host wall clock, every rank "
-                        "its shard of the batch, slowest rank"}
+                        "(gd_get_record_counts + gd_get_records_raw into one host array reused "
+                        "per window, as the reference's launcher downloads LigRecord per dump into "
+                        "its host array) + gd_destroy, host wall clock, every rank its shard of "
+                        "the batch, slowest rank"}
 
     if rank != 0:
         return

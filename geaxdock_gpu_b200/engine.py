@@ -244,15 +244,23 @@ class Engine:
                 t.replicas_per_lane)
 
     # ---- results ----
-    def records(self, r0=0, r1=None):
+    def records(self, r0=0, r1=None, out=None):
         """(steps [n, m], next_ptr [n]): the filled records of each replica, m = the largest
-        count (only those rows cross the bus)."""
+        count (only those rows cross the bus). out: a flat RECORD_DTYPE array of at least
+        n * m rows to reuse from one dump window to the next, as the reference reuses its host
+        LigRecord array; steps is then a view of it."""
         r1 = self.n_rep - 1 if r1 is None else r1
         n = r1 - r0 + 1
         nxt = np.zeros(n, np.int32)
         check(lib().gd_get_record_counts(self.h, _p(nxt), r0, r1))
         m = int(min(self.cap, max(1, nxt.max(initial=0))))
-        steps = np.empty((n, m), abi.RECORD_DTYPE)
+        if out is None:
+            steps = np.empty((n, m), abi.RECORD_DTYPE)
+        else:
+            if out.dtype != abi.RECORD_DTYPE or not out.flags.c_contiguous or out.size < n * m:
+                raise ValueError("out must be a contiguous RECORD_DTYPE array of >= %d rows"
+                                 % (n * m))
+            steps = out.reshape(-1)[:n * m].reshape(n, m)
         check(lib().gd_get_records_raw(self.h, _p(steps), _p(nxt), r0, r1, m))
         return steps, nxt
 
