@@ -92,10 +92,16 @@ def test_concurrent_chains_collect_is_plain(raw):
         _same_records(a, b)
 
 
-def test_stage_off_is_the_plain_step(raw):
+@pytest.mark.parametrize("unroll", [0, 4])
+def test_stage_off_is_the_plain_step(raw, unroll):
+    """unroll 4: the exact stage with four point pairs in flight per lane."""
     w = _small(raw)
     cx, ff, params = w.complexes[0], w.ff, w.params
     with engine.Engine(ff, [cx], params) as a, engine.Engine(ff, [cx], params) as b:
+        if unroll:
+            for e in (a, b):
+                t = e.tile()
+                e.set_tile(t[0], t[1], unroll)
         a.mc_init()
         b.mc_init()
         a.run_fused(0, 60, exchange=True)

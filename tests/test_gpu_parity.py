@@ -85,6 +85,26 @@ def test_chunk_pipeline_gives_same_energies(raw, chunk):
         assert worst.max() <= TOL
 
 
+def test_unroll_depths_give_identical_energies(raw):
+    """One, two or four point pairs in flight per lane: the accumulators take the pairs in the
+    same order, so the energies are bit-identical, and within the tolerance of the oracle."""
+    w = system.config(1, raw)
+    cx, ff = w.complexes[0], w.ff
+    rm = po.ref_map(ff, cx)
+    mm = np.random.default_rng(21).normal(0, 0.8, (12, 6)).astype(np.float32)
+    got = {}
+    with engine.Engine(ff, [cx], w.params) as eng:
+        k = eng.tile()[0]
+        for u in (1, 2, 4):
+            eng.set_tile(k, 1024, u)
+            assert eng.tile()[2] == u
+            got[u] = eng.eval_energy(0, 5, 7, mm)
+        worst = _energy_check(eng, ff, cx, 0, 5, 7, mm, rm)
+    for u in (1, 4):
+        assert got[u].tobytes() == got[2].tobytes(), u
+    assert worst.max() <= TOL, worst
+
+
 def _init_and_compare(eng, ff, cx, w_params):
     eng.mc_init()
     eng.sync()
