@@ -314,14 +314,14 @@ int launch_threads(const gd_ctx *c, int split, bool da) {
   return c->threads / launch_pack(c, split, da);
 }
 
-McKernel launch_kernel(const gd_ctx *c, int split, bool da) {
+McKernel launch_kernel(const gd_ctx *c, int split, bool da, int unroll) {
   const int S = split ? split : c->split;
-  return mc_kernel(c->unroll, S, da, launch_pack(c, split, da));
+  return mc_kernel(unroll ? unroll : c->unroll, S, da, launch_pack(c, split, da));
 }
 
-int grid_for(gd_ctx *c, int n_tiles, size_t smem, int split, bool da) {
+int grid_for(gd_ctx *c, int n_tiles, size_t smem, int split, bool da, int unroll) {
   int nb = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, launch_kernel(c, split, da),
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, launch_kernel(c, split, da, unroll),
                                                     launch_threads(c, split, da),
                                                     smem) != cudaSuccess ||
       nb < 1)
@@ -356,8 +356,8 @@ GdMcArgs base_args(gd_ctx *c) {
   return a;
 }
 
-int set_kernel_attrs(const gd_ctx *c, size_t smem, int split, bool da) {
-  const McKernel k = launch_kernel(c, split, da);
+int set_kernel_attrs(const gd_ctx *c, size_t smem, int split, bool da, int unroll) {
+  const McKernel k = launch_kernel(c, split, da, unroll);
   CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   /* shared memory for the CTAs an SM can hold and the rest as L1, which caches the cell
    * lists of the short-range pass: the carveout is the share of the SM's maximum shared

@@ -227,6 +227,15 @@ int da_choose_split(const gd_ctx *c, bool collect) {
   return std::max(c->split, std::min(S, mx));
 }
 
+/* unroll of the exact stage at split S: with one lane per atom (most proposals surviving:
+ * collect steps, or a pass rate above 0.4, da_choose_split) the stage is throughput-bound
+ * beside the other chains' front kernels, and the 80-register variant with two point pairs in
+ * flight leaves them room on the SMs; split over several lanes (few survivors) one tile's
+ * latency sets the step, and the tile's own unroll is kept (four pairs in flight shorten a
+ * tile). Config 1, DA / plain at pass 0.96 / 0.50 / 0.20 (splits 1 / 1 / 2): two pairs 1.08 /
+ * 1.91 / 3.08, four pairs 1.04 / 1.94 / 3.38. */
+int da_unroll(const gd_ctx *c, int S) { return S > 1 ? c->unroll : std::min(c->unroll, 2); }
+
 gd::GdDaDev da_args(gd_ctx *c) {
   DaState *d = c->da;
   gd::GdDaDev a;
@@ -276,7 +285,7 @@ gd::GdDaDev da_args(gd_ctx *c) {
 /* the exact stage of step j of one chain: gd_mc_kernel mode 3 over the chain's part of the
  * static tile list */
 void da_launch_exact(gd_ctx *c, const Chain &ch, int k, int n_steps, int j, bool collect,
-                     size_t smem, cudaStream_t st, int S) {
+                     size_t smem, cudaStream_t st, int S, int U) {
   DaState *d = c->da;
   const int ng = (int)d->groups.size();
   const int t0 = d->groups[ch.g0].tile_base;
@@ -300,15 +309,16 @@ void da_launch_exact(gd_ctx *c, const Chain &ch, int k, int n_steps, int j, bool
   a.da_g1 = ch.g1;
   a.da_collect = collect ? 1 : 0;
   a.split = S;
-  mc_kernel(c->unroll, S, true)<<<grid_for(c, t1 - t0, smem, S, true), c->threads, smem, st>>>(
+  mc_kernel(U, S, true)<<<grid_for(c, t1 - t0, smem, S, true, U), c->threads, smem, st>>>(
       a, c->fc);
 }
 
 /* the graph of n_steps steps (collect: plain steps that store samples), one chain per stream */
 int da_graph(gd_ctx *c, int n_steps, int exchange, bool collect, int S, cudaGraphExec_t *out) {
   DaState *d = c->da;
-  const long long key =
-      ((long long)n_steps << 7) | ((long long)S << 2) | (exchange ? 2 : 0) | (collect ? 1 : 0);
+  const int U = da_unroll(c, S);
+  const long long key = ((long long)U << 44) | ((long long)n_steps << 7) | ((long long)S << 2) |
+                        (exchange ? 2 : 0) | (collect ? 1 : 0);
   auto it = d->graphs.find(key);
   if (it != d->graphs.end()) {
     *out = it->second;
@@ -334,7 +344,7 @@ int da_graph(gd_ctx *c, int n_steps, int exchange, bool collect, int S, cudaGrap
   if ((rc = da_upload_epi(c))) return rc;
   CK(cudaStreamSynchronize(c->stream));
   const size_t smem = smem_bytes(c);
-  if ((rc = set_kernel_attrs(c, smem, S, true))) return rc;
+  if ((rc = set_kernel_attrs(c, smem, S, true, U))) return rc;
   const gd::GdDaDev a = da_args(c);
   const int spe = c->mc.steps_per_exchange;
   const int ng = (int)d->groups.size();
@@ -351,7 +361,7 @@ int da_graph(gd_ctx *c, int n_steps, int exchange, bool collect, int S, cudaGrap
     for (int j = 0; j < n_steps; ++j) {
       frc |= gd::da_front(a, collect ? GD_DA_COLLECT : GD_DA_STEP, j,
                           d->d_cnt + (size_t)(j & 1) * ng, ch.r0, ch.r1, st);
-      da_launch_exact(c, ch, k, n_steps, j, collect, smem, st, S);
+      da_launch_exact(c, ch, k, n_steps, j, collect, smem, st, S, U);
       if (exchange && (j + 1) % spe == 0) {
         const int i = (j + 1) / spe - 1;
         gd::gd_exchange_kernel<<<(ch.xg1 - ch.xg0 + 127) / 128, 128, 0, st>>>(

@@ -215,10 +215,12 @@ typedef void (*McKernel)(GdMcArgs, GdForceConst);
 McKernel mc_kernel(int unroll, int split, bool da = false, int pack = 1);
 int launch_pack(const gd_ctx *c, int split, bool da);
 int launch_threads(const gd_ctx *c, int split = 0, bool da = false);
-McKernel launch_kernel(const gd_ctx *c, int split = 0, bool da = false);
-int grid_for(gd_ctx *c, int n_tiles, size_t smem, int split = 0, bool da = false);
+/* unroll 0: the tile's */
+McKernel launch_kernel(const gd_ctx *c, int split = 0, bool da = false, int unroll = 0);
+int grid_for(gd_ctx *c, int n_tiles, size_t smem, int split = 0, bool da = false, int unroll = 0);
 GdMcArgs base_args(gd_ctx *c);
-int set_kernel_attrs(const gd_ctx *c, size_t smem, int split = 0, bool da = false);
+int set_kernel_attrs(const gd_ctx *c, size_t smem, int split = 0, bool da = false,
+                     int unroll = 0);
 int launch_mc(gd_ctx *c, GdMcArgs a, const GdTileDesc *d_tiles, int n_tiles, int *counter);
 int upload_tiles(gd_ctx *c, int r0, int r1, int *n_out);
 int check_range(const gd_ctx *c, int r0, int r1);

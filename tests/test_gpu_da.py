@@ -94,7 +94,7 @@ def test_concurrent_chains_collect_is_plain(raw):
 
 @pytest.mark.parametrize("unroll", [0, 4])
 def test_stage_off_is_the_plain_step(raw, unroll):
-    """unroll 4: the exact stage with four point pairs in flight per lane."""
+    """unroll 4: a tile with four point pairs in flight (the unsplit exact stage runs two)."""
     w = _small(raw)
     cx, ff, params = w.complexes[0], w.ff, w.params
     with engine.Engine(ff, [cx], params) as a, engine.Engine(ff, [cx], params) as b:
@@ -123,14 +123,18 @@ def _stage1_uniform(seed, stream, replica, step):
     return np.float32((w >> 8) * 2.0 ** -24)
 
 
-@pytest.mark.parametrize("split", [0, 3])
-def test_decisions_replay(raw, split):
-    """split 3: the exact stage walks each protein segment with 3 lanes per atom."""
+@pytest.mark.parametrize("split,unroll", [(0, 0), (3, 0), (3, 4)])
+def test_decisions_replay(raw, split, unroll):
+    """split 3: the exact stage walks each protein segment with 3 lanes per atom; unroll 4:
+    with four point pairs in flight (the exact stage keeps the tile's unroll when split)."""
     scale = (0.6, 0.6, 0.6, 0.3, 0.3, 0.3)  # larger moves: both stages reject
     w = _small(raw, move_scale=scale)
     cx, ff, params = w.complexes[0], w.ff, w.params
     s0, n = 100, 30
     with engine.Engine(ff, [cx], params) as eng:
+        if unroll:
+            t = eng.tile()
+            eng.set_tile(t[0], t[1], unroll)
         eng.mc_init()
         sur = engine.Surrogate(eng, hidden=128, batch=512, sample_cap=1 << 16,
                                fallback_accept=0.0, split=split)
