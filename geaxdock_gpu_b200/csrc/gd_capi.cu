@@ -56,13 +56,34 @@ float host_dist2(float ax, float ay, float az, float px, float py, float pz) {
  * so above 32 MB the destination rows are first written by up to 8 host threads in parallel,
  * then copied in one call. */
 namespace {
-/* page-locked staging buffers of the large downloads, one per copy thread, made on the first
- * large download of the process and kept */
+/* page-locked staging buffers of the large downloads, one per copy thread, made with the
+ * process's first recording context and kept */
 constexpr int kStageThreads = 8;
 constexpr size_t kStageBytes = (size_t)8 << 20;
 std::mutex g_stage_mu;
 void *g_stage[kStageThreads] = {};
+
+int stage_threads() {
+  return (int)std::min<unsigned>(kStageThreads, std::max(1u, std::thread::hardware_concurrency()));
+}
+
+/* with g_stage_mu held: false if a buffer could not be made */
+bool stage_ready_locked() {
+  for (int t = 0; t < stage_threads(); ++t)
+    if (!g_stage[t] && cudaHostAlloc(&g_stage[t], kStageBytes, cudaHostAllocPortable) !=
+                           cudaSuccess) {
+      g_stage[t] = nullptr;
+      cudaGetLastError();
+      return false;
+    }
+  return true;
+}
 }  // namespace
+
+void stage_prepare() {
+  std::lock_guard<std::mutex> lock(g_stage_mu);
+  stage_ready_locked();
+}
 
 /* n rows of `width` bytes from device memory (row pitch dpitch) into host memory (row pitch
  * hpitch). Into pageable memory, a large copy runs on up to kStageThreads host threads, each
@@ -80,17 +101,9 @@ cudaError_t d2h_rows(void *dst, size_t hpitch, const void *src, size_t dpitch, s
   if (pinned || width * (size_t)n < ((size_t)32 << 20) || width > kStageBytes)
     return cudaMemcpy2D(dst, hpitch, src, dpitch, width, n, cudaMemcpyDeviceToHost);
   std::lock_guard<std::mutex> lock(g_stage_mu);
-  const int T = (int)std::min<unsigned>(kStageThreads,
-                                        std::max(1u, std::thread::hardware_concurrency()));
-  for (int t = 0; t < T; ++t)
-    if (!g_stage[t]) {
-      cudaError_t e = cudaHostAlloc(&g_stage[t], kStageBytes, cudaHostAllocPortable);
-      if (e != cudaSuccess) {
-        g_stage[t] = nullptr;
-        cudaGetLastError();
-        return cudaMemcpy2D(dst, hpitch, src, dpitch, width, n, cudaMemcpyDeviceToHost);
-      }
-    }
+  const int T = stage_threads();
+  if (!stage_ready_locked())
+    return cudaMemcpy2D(dst, hpitch, src, dpitch, width, n, cudaMemcpyDeviceToHost);
   int dev = 0;
   cudaError_t e0 = cudaGetDevice(&dev);
   if (e0 != cudaSuccess) return e0;
@@ -715,6 +728,8 @@ int gd_create(const gd_enepara *ff, const gd_complex_desc *cxs, int n_complexes,
     const int rc0 = noalloc_prepare(device);
     if (rc0) return rc0;
   }
+  /* the record downloads' staging buffers, once per process */
+  if (mc->record) stage_prepare();
 
   gd_ctx *c = new gd_ctx();
   c->device = device;

@@ -174,6 +174,8 @@ namespace gdc {
 /* ---- the context's helpers (gd_capi.cu) ---- */
 cudaError_t d2h_rows(void *dst, size_t hpitch, const void *src, size_t dpitch, size_t width,
                      int n);
+/* makes d2h_rows' page-locked staging buffers (once per process) */
+void stage_prepare();
 /* The device's stream-ordered pool for the buffers gd_create sets up: it keeps freed memory
  * (no release threshold), so gd_destroy returns buffers without unmapping them and the next
  * context of the process reuses them; gd_release_memory trims it. Null if it cannot be made. */
