@@ -8,11 +8,14 @@
  * or with PACK = 2 the lanes of the same atom in two slots, which share every load):
  *   Move_d        (src/kernel_cuda_l2_move.cu:21-80)       placed in registers from a
  *                                                         Philox draw, no HBM traffic;
- *   CalcEnergy_d  (src/kernel_cuda_l2_calcenergy.cu:19-360) pair loop over protein points
- *                 staged by cp.async.bulk into a shared-memory double buffer, points sorted by
- *                 type so each lane keeps its pair parameters in registers per segment,
- *                 MUFU rsqrt / rcp / ex2 on the FP32 pipe, FP32 range sums folded into FP64;
- *   CalcMcc_d     (src/kernel_cuda_l2_calcmcc.cu:148-206) contact count inside the pair loop,
+ *   CalcEnergy_d  (src/kernel_cuda_l2_calcenergy.cu:19-360) the terms every pair has (vdw,
+ *                 ele in its far form, pmf, hdb) in a loop over all protein points staged by
+ *                 cp.async.bulk into a shared-memory double buffer, points sorted by type so
+ *                 each lane keeps its pair parameters in registers per segment, MUFU rsqrt /
+ *                 rcp / ex2, FP32 range sums folded into FP64; the short-range terms
+ *                 (contacts, psp, hpc, the ele soft core) from a walk of the conformer's cell
+ *                 list over the points within 9 A;
+ *   CalcMcc_d     (src/kernel_cuda_l2_calcmcc.cu:148-206) contact count in the cell walk,
  *                 true positives from the sparse reference-contact list;
  *   CalcRmsd_d, KDE, MCS, dst, CombineEnergy_d (src/kernel_cuda_l3_combineenergy.cu:23-37),
  *                 of moved poses (modes 0-3) or of given placed coordinates (mode 4),
