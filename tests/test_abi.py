@@ -111,6 +111,7 @@ def test_invalid_arguments_are_rejected_with_a_message():
     rc = lib.gd_create(C.byref(ff), C.byref(d), 1, C.byref(params), 0, C.byref(h))
     assert rc == abi.GD_ERR_INVALID
     assert b"non-finite" in lib.gd_last_error_string()
+    assert lib.gd_release_memory(-1) == abi.GD_ERR_INVALID
 
 
 @pytest.mark.skipif(have_gpu(), reason="checks the no-device path")
