@@ -796,7 +796,8 @@ def run_ours(args, rank, world, local_rank):
         d2h = 0
         # each dump window's filled records, downloaded before the counters reset into one host
         # array reused from window to window, as the reference's launcher reuses its host
-        # LigRecord array (the records held per window are kept)
+        # LigRecord array (the records held per window are kept). At 100 intervals and the
+        # default 2,000-step dump window there is one window, downloaded at the end.
         rec_host = np.empty(e.n_rep * e.cap, abi.RECORD_DTYPE)
         held = []
 

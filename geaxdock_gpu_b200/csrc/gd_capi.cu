@@ -654,6 +654,7 @@ int gd_destroy(gd_ctx *c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   rs_stop(c);
+  ra_free(c);
   drop_graphs(c);
   da_free(c);
   for (void *p : c->pool_allocs) cudaFreeAsync(p, c->stream);

@@ -95,6 +95,7 @@ struct Chain {
 }  // namespace gdc
 
 struct RecStream;
+struct RecAsync;
 struct DaState;
 
 struct gd_ctx {
@@ -165,6 +166,8 @@ struct gd_ctx {
   int chain_tiles_cap = 0;
   /* record streaming into host memory (gd_records_stream) */
   struct RecStream *rs = nullptr;
+  /* a dump window downloaded in the background (gd_get_records_async) */
+  struct RecAsync *ra = nullptr;
 };
 
 #define GD_MAX_DEVICES 64
@@ -239,6 +242,8 @@ int rs_enqueue(gd_ctx *c, int rows_per_rep);
 int rs_flush(gd_ctx *c);
 int rs_restart(gd_ctx *c, int r0, int r1);
 void rs_stop(gd_ctx *c);
+/* waits for, then frees, the background window download */
+void ra_free(gd_ctx *c);
 
 /* ---- delayed acceptance (gd_capi_da.cu) ---- */
 void da_free(gd_ctx *c);

@@ -154,6 +154,21 @@ struct RecStream {
   }
 };
 
+/* One dump window downloaded in the background (gd_get_records_async): the window's rows are
+ * snapshotted on the device in the context's stream order (one device-to-device copy, after
+ * which the stream may reset and overwrite the records), and a host thread waits for the
+ * snapshot and copies it out with the staged multi-threaded copy of d2h_rows. */
+struct RecAsync {
+  gd_record_step *d_snap = nullptr;                /* [n_rep * cap] */
+  int *d_next = nullptr;                           /* [n_rep] */
+  size_t snap_rows = 0;
+  cudaEvent_t ev = nullptr;
+  std::thread th;
+  bool busy = false;
+  int rows = 0;
+  cudaError_t err = cudaSuccess;
+};
+
 namespace gdc {
 
 /* queues a snapshot taken after the work queued on the context's stream so far: the copy plan
@@ -259,6 +274,32 @@ void rs_stop(gd_ctx *c) {
   c->rs = nullptr;
 }
 
+/* waits for the background download, if any (the thread's result in *rows) */
+int ra_wait(gd_ctx *c, int *rows) {
+  RecAsync *a = c->ra;
+  if (rows) *rows = 0;
+  if (!a || !a->busy) return GD_OK;
+  a->th.join();
+  a->busy = false;
+  if (rows) *rows = a->rows;
+  if (a->err != cudaSuccess)
+    return fail(GD_ERR_CUDA, "background record download: %s", cudaGetErrorString(a->err));
+  return GD_OK;
+}
+
+void ra_free(gd_ctx *c) {
+  RecAsync *a = c->ra;
+  if (!a) return;
+  ra_wait(c, nullptr);
+  /* the buffers came from the context pool on the context's stream */
+  if (a->d_snap) cudaFreeAsync(a->d_snap, c->stream);
+  if (a->d_next) cudaFreeAsync(a->d_next, c->stream);
+  if (a->d_snap || a->d_next) cudaStreamSynchronize(c->stream);
+  if (a->ev) cudaEventDestroy(a->ev);
+  delete a;
+  c->ra = nullptr;
+}
+
 }  // namespace gdc
 
 using namespace gdc;
@@ -323,6 +364,64 @@ int gd_records_stream_flush(gd_ctx *c, int *next_ptr) {
     std::copy(c->rs->snap.begin(), c->rs->snap.end(), next_ptr);
   }
   return GD_OK;
+}
+
+int gd_get_records_async(gd_ctx *c, gd_record_step *steps, int *next_ptr, int cap) {
+  if (!c || !steps || !next_ptr) return fail(GD_ERR_INVALID, "null argument");
+  if (!c->mc.record || !c->d_rec) return fail(GD_ERR_STATE, "records are disabled");
+  if (cap < 1 || cap > c->rec_cap)
+    return fail(GD_ERR_INVALID, "cap %d outside 1..record capacity %d", cap, c->rec_cap);
+  CK(cudaSetDevice(c->device));
+  if (!c->ra) c->ra = new RecAsync();
+  RecAsync *a = c->ra;
+  int rc = ra_wait(c, nullptr);
+  if (rc) return rc;
+  const int n = c->n_rep;
+  const size_t rows = (size_t)n * cap, rs = sizeof(gd_record_step);
+  /* the snapshot buffers come from the context pool, stream-ordered on the context's stream
+   * (the host thread reads them only after the event recorded behind the snapshot) */
+  cudaMemPool_t pool = ctx_pool(c->device);
+  if (!pool) return fail(GD_ERR_NOMEM, "gd_get_records_async: no memory pool");
+  if (a->snap_rows < rows) {
+    if (a->d_snap) cudaFreeAsync(a->d_snap, c->stream);
+    a->d_snap = nullptr;
+    a->snap_rows = 0;
+    CK(cudaMallocFromPoolAsync(reinterpret_cast<void **>(&a->d_snap), rows * rs, pool,
+                               c->stream));
+    a->snap_rows = rows;
+  }
+  if (!a->d_next)
+    CK(cudaMallocFromPoolAsync(reinterpret_cast<void **>(&a->d_next), sizeof(int) * n, pool,
+                               c->stream));
+  if (!a->ev) CK(cudaEventCreateWithFlags(&a->ev, cudaEventDisableTiming));
+  CK(cudaMemcpy2DAsync(a->d_snap, rs * cap, c->d_rec, rs * c->rec_cap, rs * cap, n,
+                       cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaMemcpyAsync(a->d_next, c->d_rec_next, sizeof(int) * n, cudaMemcpyDeviceToDevice,
+                     c->stream));
+  CK(cudaEventRecord(a->ev, c->stream));
+  a->busy = true;
+  a->err = cudaSuccess;
+  a->rows = 0;
+  const int dev = c->device;
+  a->th = std::thread([a, dev, n, cap, steps, next_ptr, rs] {
+    cudaError_t e = cudaSetDevice(dev);
+    if (e == cudaSuccess) e = cudaEventSynchronize(a->ev);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(next_ptr, a->d_next, sizeof(int) * n, cudaMemcpyDeviceToHost);
+    int m = 1;
+    if (e == cudaSuccess) {
+      for (int r = 0; r < n; ++r) m = std::max(m, std::min(next_ptr[r], cap));
+      e = d2h_rows(steps, rs * m, a->d_snap, rs * cap, rs * m, n);
+    }
+    a->rows = m;
+    a->err = e;
+  });
+  return GD_OK;
+}
+
+int gd_records_wait(gd_ctx *c, int *rows) {
+  if (!c) return fail(GD_ERR_INVALID, "null context");
+  return ra_wait(c, rows);
 }
 
 }  // extern "C"

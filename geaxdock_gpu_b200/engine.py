@@ -63,6 +63,8 @@ def lib() -> C.CDLL:
         "gd_get_record_counts": [vp, vp, C.c_int, C.c_int],
         "gd_records_stream": [vp, vp, C.c_int],
         "gd_records_stream_flush": [vp, vp],
+        "gd_get_records_async": [vp, vp, vp, C.c_int],
+        "gd_records_wait": [vp, ip],
         "gd_get_etotal": [vp, fp, C.c_int, C.c_int],
         "gd_get_replicas": [vp, vp, C.c_int, C.c_int],
         "gd_get_state": [vp, vp, C.c_int, C.c_int],
@@ -166,12 +168,14 @@ class Engine:
             self.offsets.append(o.value)
         self.cap = params.steps_per_dump + 1
         self._stream_buf = None
+        self._async = None
 
     def close(self):
         if getattr(self, "h", None):
-            lib().gd_destroy(self.h)
+            lib().gd_destroy(self.h)  # waits for a background download first
             self.h = None
         self._stream_buf = None
+        self._async = None
 
     def __del__(self):
         try:
@@ -263,6 +267,29 @@ class Engine:
             steps = out.reshape(-1)[:n * m].reshape(n, m)
         check(lib().gd_get_records_raw(self.h, _p(steps), _p(nxt), r0, r1, m))
         return steps, nxt
+
+    def records_async(self, out: np.ndarray, nxt: np.ndarray, cap=None):
+        """gd_get_records_async: the current window's records copied into out (a flat
+        RECORD_DTYPE array of at least n_rep * cap rows) and nxt (n_rep int32) in the
+        background; records_wait() completes it. Both arrays must stay alive and untouched
+        until then."""
+        cap = self.cap if cap is None else cap
+        if out.dtype != abi.RECORD_DTYPE or not out.flags.c_contiguous or \
+                out.size < self.n_rep * cap:
+            raise ValueError("out must be a contiguous RECORD_DTYPE array of >= %d rows"
+                             % (self.n_rep * cap))
+        if nxt.dtype != np.int32 or not nxt.flags.c_contiguous or nxt.size < self.n_rep:
+            raise ValueError("nxt must be a contiguous int32 array of >= %d values" % self.n_rep)
+        check(lib().gd_get_records_async(self.h, _p(out), _p(nxt), cap))
+        self._async = (out, nxt)
+
+    def records_wait(self):
+        """(steps [n_rep, m], next_ptr [n_rep]) of the last records_async, once copied."""
+        rows = C.c_int()
+        check(lib().gd_records_wait(self.h, C.byref(rows)))
+        out, nxt = self._async
+        m = max(1, rows.value)
+        return out.reshape(-1)[:self.n_rep * m].reshape(self.n_rep, m), nxt[:self.n_rep]
 
     def stream_records(self, cap: int) -> np.ndarray:
         """Starts gd_records_stream into a new host array [n_rep][cap] (RECORD_DTYPE): the

@@ -290,6 +290,16 @@ int gd_get_record_counts(gd_ctx *ctx, int *next_ptr, int rep_begin, int rep_end)
  * flush first (read the window before resetting it). steps = NULL flushes and stops. */
 int gd_records_stream(gd_ctx *ctx, gd_record_step *steps, int cap);
 int gd_records_stream_flush(gd_ctx *ctx, int *next_ptr);
+/* One dump window's records copied out while the next window runs (the reference copies its
+ * LigRecord array after each dump window and waits, src/kernel_cuda_lancher_siglegpu.cu:36-46):
+ * the first `cap` rows of every replica are snapshotted on the device in stream order (calls
+ * that follow, gd_reset_records included, may overwrite them), and a host thread copies the
+ * filled rows into steps[r * m + i] (m = min(cap, the largest count); any host memory of at
+ * least n_rep * cap rows) and the counts into next_ptr[n_rep]. Returns at once;
+ * gd_records_wait returns m in *rows once the copy is done, and neither array may be read or
+ * freed before. A second call first waits for the first. */
+int gd_get_records_async(gd_ctx *ctx, gd_record_step *steps, int *next_ptr, int cap);
+int gd_records_wait(gd_ctx *ctx, int *rows);
 int gd_get_etotal(gd_ctx *ctx, float *etotal, int rep_begin, int rep_end);
 int gd_get_replicas(gd_ctx *ctx, gd_replica *replicas, int rep_begin, int rep_end);
 int gd_get_state(gd_ctx *ctx, gd_replica_state *state, int rep_begin, int rep_end);

@@ -118,3 +118,39 @@ def test_stream_partial_reset(cx_ff):
         b, nxt = e.stream_flush()
         assert b is buf and nxt[:half].max() <= 20 and nxt[half:].max() >= nxt[:half].max()
         _same(e, buf, nxt)
+
+
+def test_async_window_download_is_the_download_at_that_point(cx_ff):
+    """gd_get_records_async snapshots the window in stream order: the reset and the steps queued
+    after it do not change what arrives, which equals a synchronous download taken at the same
+    point of an identical run; the runs go on identically."""
+    cx, ff = cx_ff
+    params = abi.mc_params(steps_per_exchange=10, steps_per_dump=100, seed=5)
+    with engine.Engine(ff, [cx], params) as a, engine.Engine(ff, [cx], params) as b:
+        for e in (a, b):
+            e.mc_init()
+            for it in range(10):
+                e.mc_run(0, it * 10)
+                e.exchange(int(not (it % 2)))
+        want, wnxt = a.records()
+        out = np.empty(b.n_rep * b.cap, abi.RECORD_DTYPE)
+        nxt = np.empty(b.n_rep, np.int32)
+        b.records_async(out, nxt)
+        for e in (a, b):
+            e.reset_records()
+            for it in range(3):
+                e.mc_run(100, it * 10)
+                e.exchange(int(not (it % 2)))
+        got, gnxt = b.records_wait()
+        assert np.array_equal(gnxt, wnxt) and wnxt.max() > 1
+        assert got.shape == want.shape
+        for r in range(b.n_rep):
+            assert got[r, :wnxt[r]].tobytes() == want[r, :wnxt[r]].tobytes(), r
+        assert a.state().tobytes() == b.state().tobytes()
+        # the next window, asynchronously again into the same arrays
+        b.records_async(out, nxt)
+        w2, n2 = a.records()
+        g2, m2 = b.records_wait()
+        assert np.array_equal(m2, n2)
+        for r in range(b.n_rep):
+            assert g2[r, :n2[r]].tobytes() == w2[r, :n2[r]].tobytes(), r
