@@ -114,9 +114,12 @@ int layout_complex(gd_ctx *c, const gd_enepara *ff, const float (*thr)[GD_MAXTP1
     }
     double cell = GD_CELL;
     long long n[3];
+    /* the cell starts of all conformers share one budget (GD_MAX_CELLS_ALL) */
+    const long long max_cells =
+        std::max(4096LL, std::min((long long)GD_MAX_CELLS, (long long)GD_MAX_CELLS_ALL / d.n_prt));
     for (;;) {
       for (int a = 0; a < 3; ++a) n[a] = (long long)std::floor((hi[a] - lo[a] + 1.0) / cell) + 1;
-      if (n[0] * n[1] * n[2] <= GD_MAX_CELLS) break;
+      if (n[0] * n[1] * n[2] <= max_cells) break;
       cell *= 1.25;
     }
     const int ncell = (int)(n[0] * n[1] * n[2]);

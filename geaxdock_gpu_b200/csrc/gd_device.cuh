@@ -36,6 +36,7 @@
 /* shared-memory bytes of the contact-threshold table at the front of the kernel's buffer */
 #define GD_THR_BYTES (GD_MAXTP2 * GD_MAXTP1 * 4)
 #define GD_MAX_CELLS (1 << 22) /* cells per conformer grid; a larger box widens the cells */
+#define GD_MAX_CELLS_ALL (1 << 25) /* cells of all conformers of a complex together */
 #define GD_MAX_TPB 256         /* threads per CTA: 3 CTAs of 256 fit the register file */
 #define GD_SLOT_BYTES 192      /* shared-memory bytes per replica slot (sizeof gd::Slot) */
 /* resident 256-thread CTAs per SM the register budget is set for, per unroll depth */
