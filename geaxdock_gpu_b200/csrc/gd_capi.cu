@@ -1221,7 +1221,9 @@ int gd_mc_run_fused(gd_ctx *c, int s1, int n_steps, int exchange) {
   if (rc) return rc;
   const int nch = (int)c->chain.size();
   const int chunks = n_steps / spe;
-  if ((rc = ensure_counters(c, chunks * nch))) return rc;
+  /* the persistent-CTA queue heads, then (with the exchange) one count per group and interval */
+  const int n_ctr = chunks * nch + (exchange ? chunks * c->n_groups : 0);
+  if ((rc = ensure_counters(c, n_ctr))) return rc;
   const long long key = ((long long)n_steps << 1) | (exchange ? 1 : 0);
   auto it = c->graphs.find(key);
   if (it == c->graphs.end()) {
@@ -1230,7 +1232,7 @@ int gd_mc_run_fused(gd_ctx *c, int s1, int n_steps, int exchange) {
     if ((rc = set_kernel_attrs(c, smem))) return rc;
     cudaGraph_t graph;
     CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    cudaMemsetAsync(c->d_counters, 0, sizeof(int) * chunks * nch, c->stream);
+    cudaMemsetAsync(c->d_counters, 0, sizeof(int) * n_ctr, c->stream);
     chains_fork(c, nch);
     for (int k = 0; k < nch; ++k) {
       const Chain &ch = c->chain[k];
@@ -1245,11 +1247,16 @@ int gd_mc_run_fused(gd_ctx *c, int s1, int n_steps, int exchange) {
         a.tiles = c->d_chain_tiles + ch.t_off;
         a.n_tiles = ch.t_cnt;
         a.tile_counter = c->d_counters + k * chunks + i;
+        if (exchange) {
+          /* the chain's groups are whole (chains are made of protein-conformer blocks) */
+          a.x_done = c->d_counters + chunks * nch + (size_t)i * c->n_groups;
+          a.x_group_base = c->d_group_base;
+          a.x_acs = c->d_acs;
+          a.x_call_base = c->d_cursor + 1;
+          a.x_call_off = i;
+          a.x_mode_t = !(i % 2);
+        }
         launch_kernel(c)<<<grid, launch_threads(c), smem, st>>>(a, c->fc);
-        if (exchange)
-          gd::gd_exchange_kernel<<<(ch.xg1 - ch.xg0 + 127) / 128, 128, 0, st>>>(
-              c->d_cx, c->d_group_base, c->n_complex, ch.xg0, ch.xg1, c->d_replica, c->d_etotal,
-              c->d_acs, c->mc.seed, c->d_cursor + 1, i, !(i % 2));
       }
     }
     chains_join(c, nch);

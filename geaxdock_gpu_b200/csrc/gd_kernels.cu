@@ -356,6 +356,43 @@ __device__ __forceinline__ void pair_dispatch(int flags, const float4 *PA, const
 #undef GD_PR
 }
 
+/* ExchangeReplicas_d (src/kernel_cuda_l1_exchangereplicas.cu:27-77) for one (protein
+ * conformer, ligand conformer) group lg of complex cx: temperature pairs (2 j + mode_t, its
+ * successor), accepted by the Metropolis test on their energies with one Philox draw per pair
+ * of this exchange call. The group's replica states are read with L2 loads (.cg): inside the
+ * Monte Carlo kernel other SMs wrote them in this launch. */
+__device__ __forceinline__ void gd_exchange_group(const GdDevComplex &cx, int lg,
+                                                  gd_replica *replica, const float *etotal,
+                                                  int *acs, uint64_t seed, int call, int mode_t) {
+  if (mode_t >= 2) return;
+  const int nl = cx.n_lig, nt = cx.n_tmp;
+  const int p = lg / nl, l = lg - p * nl;
+  int temps[GD_MAXTMP], orders[GD_MAXTMP];
+  float en[GD_MAXTMP];
+  for (int t = 0; t < nt; ++t) {
+    const int f = cx.rep_offset + nt * nl * p + nl * t + l;
+    temps[t] = __ldcg(&replica[f].idx_tmp);
+    en[t] = __ldcg(etotal + f);
+    orders[temps[t]] = t;
+  }
+  const int maxpair = nt / 2 - (nt % 2 == 0) * (mode_t == 1);
+  for (int pair = 0; pair < maxpair; ++pair) {
+    const int i1 = (pair << 1) + mode_t, i2 = i1 + 1;
+    const int o1 = orders[i1], o2 = orders[i2];
+    const int tt = temps[o1];
+    const float mb1 = cx.minus_beta[temps[o1]], mb2 = cx.minus_beta[temps[o2]];
+    const float u = gd_draw_exchange(seed, (uint32_t)cx.stream, (uint32_t)lg, (uint32_t)call,
+                                     (uint32_t)pair);
+    if (gd_exchange_accept(en[o1], en[o2], mb1, mb2, u)) {
+      temps[o1] = temps[o2];
+      temps[o2] = tt;
+      acs[cx.rep_offset + nt * nl * p + nl * o1 + l] += 1;
+      acs[cx.rep_offset + nt * nl * p + nl * o2 + l] += 1;
+    }
+  }
+  for (int t = 0; t < nt; ++t) replica[cx.rep_offset + nt * nl * p + nl * t + l].idx_tmp = temps[t];
+}
+
 /* Delayed acceptance, second stage, for the survivor in pose slot `pos` (mode 3): the
  * corrected Metropolis test u2 < exp(mb ((E_new - E_old) - (S_new - S_cur))) (gd_da_stage2),
  * surrogate-error sums, the collect step's training target, the trace, and on acceptance the
@@ -875,6 +912,19 @@ __global__ void __launch_bounds__(GD_MAX_TPB / PACK, GD_MIN_BLOCKS_PACK(UNROLL, 
       if (a.rec) a.rec_next[sl.rep] = sl.rec_next;
 #pragma unroll
       for (int i = 0; i < 6; ++i) a.mm_old[(size_t)sl.rep * 6 + i] = sl.mm_old[i];
+      /* ExchangeReplicas_d fused: the replica that completes its group in this launch (the
+       * group's last to be written back, counted with fences on both sides) exchanges the
+       * group's temperatures; no CTA waits for another */
+      if (a.mode == 0 && a.x_done) {
+        const int local = sl.rep - cx.rep_offset, nl = cx.n_lig, nt = cx.n_tmp;
+        const int lg = (local / (nt * nl)) * nl + local % nl;
+        __threadfence();
+        if (atomicAdd(a.x_done + a.x_group_base[tile.complex_index] + lg, 1) == nt - 1) {
+          __threadfence();
+          gd_exchange_group(cx, lg, a.replica, a.etotal, a.x_acs, a.seed,
+                            (a.x_call_base ? *a.x_call_base : 0) + a.x_call_off, a.x_mode_t);
+        }
+      }
     }
     __syncthreads();
   }
@@ -905,35 +955,8 @@ __global__ void gd_exchange_kernel(const GdDevComplex *cxs, const int *group_bas
     const int mid = (lo + hi + 1) >> 1;
     if (group_base[mid] <= g) lo = mid; else hi = mid - 1;
   }
-  const GdDevComplex &cx = cxs[lo];
-  const int lg = g - group_base[lo];
-  const int nl = cx.n_lig, nt = cx.n_tmp;
-  const int p = lg / nl, l = lg - p * nl;
-  const int call = (call_base ? *call_base : 0) + call_off;
-  int temps[GD_MAXTMP], orders[GD_MAXTMP];
-  float en[GD_MAXTMP];
-  for (int t = 0; t < nt; ++t) {
-    const int f = cx.rep_offset + nt * nl * p + nl * t + l;
-    temps[t] = replica[f].idx_tmp;
-    en[t] = etotal[f];
-    orders[temps[t]] = t;
-  }
-  const int maxpair = nt / 2 - (nt % 2 == 0) * (mode_t == 1);
-  for (int pair = 0; pair < maxpair; ++pair) {
-    const int i1 = (pair << 1) + mode_t, i2 = i1 + 1;
-    const int o1 = orders[i1], o2 = orders[i2];
-    const int tt = temps[o1];
-    const float mb1 = cx.minus_beta[temps[o1]], mb2 = cx.minus_beta[temps[o2]];
-    const float u = gd_draw_exchange(seed, (uint32_t)cx.stream, (uint32_t)lg, (uint32_t)call,
-                                     (uint32_t)pair);
-    if (gd_exchange_accept(en[o1], en[o2], mb1, mb2, u)) {
-      temps[o1] = temps[o2];
-      temps[o2] = tt;
-      acs[cx.rep_offset + nt * nl * p + nl * o1 + l] += 1;
-      acs[cx.rep_offset + nt * nl * p + nl * o2 + l] += 1;
-    }
-  }
-  for (int t = 0; t < nt; ++t) replica[cx.rep_offset + nt * nl * p + nl * t + l].idx_tmp = temps[t];
+  gd_exchange_group(cxs[lo], g - group_base[lo], replica, etotal, acs, seed,
+                    (call_base ? *call_base : 0) + call_off, mode_t);
 }
 
 /* ResetCounter_d (src/kernel_cuda_l1_resetcounter.cu:12-22). */
