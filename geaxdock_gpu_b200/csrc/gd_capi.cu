@@ -1254,7 +1254,8 @@ int gd_mc_run_fused(gd_ctx *c, int s1, int n_steps, int exchange) {
           a.x_acs = c->d_acs;
           a.x_call_base = c->d_cursor + 1;
           a.x_call_off = i;
-          a.x_mode_t = !(i % 2);
+          a.x_spd = c->mc.steps_per_dump;
+          a.x_spe = spe;
         }
         launch_kernel(c)<<<grid, launch_threads(c), smem, st>>>(a, c->fc);
       }

@@ -179,14 +179,16 @@ struct GdMcArgs {
                                  range [da_g0, da_g1) this launch serves */
   int da_g0, da_g1;
   int da_collect;             /* collect step: stage off everywhere, targets stored */
-  /* ExchangeReplicas_d fused into mode 0 (launches that cover whole groups): per-group counts
-   * of replicas written back in this launch, the complexes' first group, the exchange
-   * counters, and the exchange call (*x_call_base + x_call_off) with its mode_t */
+  /* ExchangeReplicas_d fused into mode 0 (launches that cover whole groups and one exchange
+   * interval): per-group counts of replicas written back in this launch, the complexes' first
+   * group, the exchange counters, and the exchange call (*x_call_base + x_call_off); mode_t
+   * = !(((s mod x_spd) / x_spe) % 2) for the interval starting at step s, as the reference's
+   * launcher derives it from the step within the dump window */
   int *x_done;                /* [n_groups] zeroed before the launch, or null */
   const int *x_group_base;    /* [n_complex] */
   int *x_acs;                 /* [n_rep] */
   const int *x_call_base;
-  int x_call_off, x_mode_t;
+  int x_call_off, x_spd, x_spe;
 };
 
 #endif

@@ -921,8 +921,9 @@ __global__ void __launch_bounds__(GD_MAX_TPB / PACK, GD_MIN_BLOCKS_PACK(UNROLL, 
         __threadfence();
         if (atomicAdd(a.x_done + a.x_group_base[tile.complex_index] + lg, 1) == nt - 1) {
           __threadfence();
+          const int mode_t = !(((step_first % a.x_spd) / a.x_spe) % 2);
           gd_exchange_group(cx, lg, a.replica, a.etotal, a.x_acs, a.seed,
-                            (a.x_call_base ? *a.x_call_base : 0) + a.x_call_off, a.x_mode_t);
+                            (a.x_call_base ? *a.x_call_base : 0) + a.x_call_off, mode_t);
         }
       }
     }

@@ -261,8 +261,9 @@ int gd_exchange(gd_ctx *ctx, int mode_l, int mode_t);
 /* The reference's per-dump loop body (src/kernel_cuda_lancher_siglegpu.cu:25-32) over
  * n_steps steps from step s1, captured once into a CUDA graph and replayed:
  * gd_mc_run + (if exchange) gd_exchange with mode_t = !((s2 / steps_per_exchange) % 2), s2 the
- * step offset within this call. The exchange runs inside the Monte Carlo kernel (the last
- * replica of each group to finish the interval exchanges the group), one launch per interval. */
+ * interval's first step within its dump window (s mod steps_per_dump), so a window may be run
+ * in several calls. The exchange runs inside the Monte Carlo kernel (the last replica of each
+ * group to finish the interval exchanges the group), one launch per interval. */
 int gd_mc_run_fused(gd_ctx *ctx, int s1, int n_steps, int exchange);
 int gd_sync(gd_ctx *ctx);
 /* The context's CUDA stream (a cudaStream_t), for callers that order or time work on it. */

@@ -185,6 +185,39 @@ def test_trajectory_replay_bit_exact(raw, move_kind):
         assert 0.05 < ta.mean() < 0.98
 
 
+def test_fused_window_in_pieces_equals_one_call(raw):
+    """The exchange inside the fused kernel takes mode_t from the interval's step within its
+    dump window, so a window run as one call, in 10-step calls or in uneven pieces gives the
+    same chains, and equals the stepwise loop across a window boundary (3 intervals per
+    window: the alternation restarts at each window, as in the reference's launcher)."""
+    w = system.config(0, raw)
+    cx, ff = w.complexes[0], w.ff
+    params = w.params
+    params.steps_per_dump = 30
+    engs = [engine.Engine(ff, [cx], params) for _ in range(4)]
+    try:
+        for e in engs:
+            e.mc_init()
+        a, b, c, d = engs
+        for e in range(6):  # two dump windows of three intervals
+            s1, s2 = (e // 3) * 30, (e % 3) * 10
+            a.mc_run(s1, s2)
+            a.exchange(int(not ((s2 // 10) % 2)))
+        b.run_fused(0, 30, exchange=True)
+        b.run_fused(30, 30, exchange=True)
+        for s in range(0, 60, 10):
+            c.run_fused(s, 10, exchange=True)
+        d.run_fused(0, 20, exchange=True)
+        d.run_fused(20, 30, exchange=True)
+        d.run_fused(50, 10, exchange=True)
+        want = a.state().tobytes()
+        for e in (b, c, d):
+            assert e.state().tobytes() == want
+    finally:
+        for e in engs:
+            e.close()
+
+
 def test_fused_graph_equals_stepwise(raw):
     w = system.config(0, raw)
     cx, ff = w.complexes[0], w.ff
