@@ -238,7 +238,7 @@ __device__ __forceinline__ void short_range(const GdDevComplex &cx, int pc,
                                             const float *__restrict__ thr,
                                             const float *__restrict__ psprow,
                                             const GdForceConst &f, float ax, float ay, float az,
-                                            ShortSums &s) {
+                                            int part, int parts, ShortSums &s) {
   s.hsum = 0.0;
   s.psp = 0.0f;
   s.ele = 0.0f;
@@ -271,15 +271,23 @@ __device__ __forceinline__ void short_range(const GdDevComplex &cx, int pc,
     b0 = __ldg(st + row + x0);
     b1 = __ldg(st + row + x1 + 1);
   };
-  int iy = y0, iz = z0, n0, n1;
-  bounds(iy, iz, n0, n1);
-  for (;;) {
+  /* rows part, part + parts, ... of the (iy, iz) order: the lanes of a split atom share them */
+  const int ny_span = y1 - y0 + 1;
+  int iy = y0 + part, iz = z0, n0 = 0, n1 = 0;
+  while (iy > y1) {
+    iy -= ny_span;
+    ++iz;
+  }
+  bool more = iz <= z1;
+  if (more) bounds(iy, iz, n0, n1);
+  while (more) {
     const int c0 = n0, c1 = n1;
-    if (++iy > y1) {
-      iy = y0;
+    iy += parts;
+    while (iy > y1) {
+      iy -= ny_span;
       ++iz;
     }
-    const bool more = iz <= z1;
+    more = iz <= z1;
     if (more) bounds(iy, iz, n0, n1);
     for (int i = c0; i < c1; ++i) {
       const float4 p = __ldg(PA + i);
@@ -309,7 +317,6 @@ __device__ __forceinline__ void short_range(const GdDevComplex &cx, int pc,
         }
       }
     }
-    if (!more) break;
   }
 }
 
@@ -654,13 +661,14 @@ __global__ void __launch_bounds__(GD_MAX_TPB / PACK, GD_MIN_BLOCKS_PACK(UNROLL, 
 #pragma unroll
           for (int qi = 0; qi < NQ; ++qi) part[qi * T + vl[h]] = 0.0;
 
-      /* ---- short-range terms from the cell list (split 0 of each atom), before the pair
-       * loop: warps whose walk is short start the loop while the others still walk ---- */
+      /* ---- short-range terms from the cell list (the S lanes of an atom take every S-th row
+       * of its walk), before the pair loop: warps whose walk is short start the loop while
+       * the others still walk ---- */
 #pragma unroll
       for (int h = 0; h < PACK; ++h) {
-        if (!ok[h] || sp != 0) continue;
+        if (!ok[h]) continue;
         ShortSums sr;
-        short_range(cx, pc, thr_s + tl * GD_MAXTP1, psprow, f, ax[h], ay[h], az[h], sr);
+        short_range(cx, pc, thr_s + tl * GD_MAXTP1, psprow, f, ax[h], ay[h], az[h], sp, S, sr);
         const int v = vl[h];
         part[1 * T + v] = (double)sr.ele;
         part[3 * T + v] = (double)sr.psp;
@@ -743,6 +751,15 @@ __global__ void __launch_bounds__(GD_MAX_TPB / PACK, GD_MIN_BLOCKS_PACK(UNROLL, 
       }
 
       /* ---- per-atom tail (split 0 of each atom): hpc, kde, rmsd, reference contacts ---- */
+      if (S > 1) {
+        /* hpc is nonlinear in the atom's hydrophobic sum: gather the splits' parts first */
+        __syncthreads();
+        if (ok[0] && sp == 0)
+          for (int q = 1; q < S; ++q) {
+            part[5 * T + vl[0]] += part[5 * T + vl[0] + q * L];
+            part[5 * T + vl[0] + q * L] = 0.0;
+          }
+      }
 #pragma unroll
       for (int h = 0; h < PACK; ++h) {
         if (!ok[h] || aborted) continue;
