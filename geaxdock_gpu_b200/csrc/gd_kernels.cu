@@ -112,7 +112,7 @@ struct Acc {
 
 /* Per-segment pair parameters, splatted over the two lanes of an FP32x2 register pair. */
 struct Pair2 {
-  float2 p1a, mp2a, p1l, b2, c2, pmf1, hc1, hc0, hs;
+  float2 p1a, mp2a, p1l, p1ll, b2, c2, hc1, hc0, hs;
 };
 
 __device__ __forceinline__ float2 f2(float v) { return make_float2(v, v); }
@@ -133,14 +133,13 @@ __device__ __forceinline__ void pair_body(const float4 A, const float4 B, float2
   const float2 dz = __fadd2_rn(az, make_float2(B.x, B.y));
   const float2 d2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
   const float2 ri = make_float2(rsqrt_a(d2.x), rsqrt_a(d2.y));
-  const float2 r = __fmul2_rn(d2, ri);
-  /* vdw: (p1 - p2) / (p1 lj0 (1 + lj1 d2) + 1), p1 = p1a r^-9, p2 = p2a r^-6 */
+  /* vdw: (p1 - p2) / (p1 lj0 (1 + lj1 d2) + 1), p1 = p1a r^-9, p2 = p2a r^-6; the
+   * denominator is (p1l + p1ll d2) r^-9 + 1 with p1l = p1a lj0, p1ll = p1l lj1 */
   const float2 r2i = __fmul2_rn(ri, ri);
   const float2 r3i = __fmul2_rn(r2i, ri);
   const float2 r6i = __fmul2_rn(r3i, r3i);
   const float2 num = __fmul2_rn(r6i, __ffma2_rn(q.p1a, r3i, q.mp2a));
-  const float2 t9 = __fmul2_rn(q.p1l, __fmul2_rn(r6i, r3i));
-  const float2 p4 = __ffma2_rn(t9, __ffma2_rn(f2(f.lj1), d2, one), one);
+  const float2 p4 = __ffma2_rn(__ffma2_rn(q.p1ll, d2, q.p1l), __fmul2_rn(r6i, r3i), one);
   /* ele: q_l ele_p g(el1 r), q_l applied once per atom. The points hold ele_p / el1, so the
    * far form g = 1 / (el1 r) is one FMA with r^-1; pairs inside r < 1 / el1 get the soft-core
    * difference in short_range() */
@@ -151,26 +150,27 @@ __device__ __forceinline__ void pair_body(const float4 A, const float4 B, float2
     a.ele.x = __fmaf_rn(ep.x, ri.x, a.ele.x);
   }
   /* pmf: pmf1 / (1 + exp((6 - r/2)(r - pmf0))) as exp2 of the expanded quadratic
-   * cA d2 + b2 r + c2 (cA = -log2(e)/2, b2 = log2(e)(6 + pmf0/2), c2 = -6 log2(e) pmf0).
-   * Its maximum over r is log2(e) (12 - pmf0)^2 / 8 < 100 for pmf0 > -10 (checked when the
-   * force field is loaded), so den stays finite and p4 den does wherever p4 does. */
-  const float2 tt = __ffma2_rn(q.b2, r, __ffma2_rn(f2(-0.5f * LOG2E_F), d2, q.c2));
+   * cA d2 + b2 r + c2 = d2 (b2 r^-1 + cA) + c2 (cA = -log2(e)/2, b2 = log2(e)(6 + pmf0/2),
+   * c2 = -6 log2(e) pmf0). Its maximum over r is log2(e) (12 - pmf0)^2 / 8 < 100 for
+   * pmf0 > -10 (checked when the force field is loaded), so den stays finite and p4 den does
+   * wherever p4 does. */
+  const float2 tt = __ffma2_rn(d2, __ffma2_rn(q.b2, ri, f2(-0.5f * LOG2E_F)), q.c2);
   const float2 ee = make_float2(ex2_a(tt.x), ex2_a(tt.y));
   /* one reciprocal for both quotients, den = 1 + ee: num / p4 = num den / (p4 den),
-   * pmf1 / den = pmf1 p4 / (p4 den), with p4 den = p4 + p4 ee and num den = num + num ee */
+   * 1 / den = p4 / (p4 den), with p4 den = p4 + p4 ee and num den = num + num ee; the
+   * segment's pmf1 multiplies the pmf sum when it is folded */
   const float2 pd = __ffma2_rn(p4, ee, p4);
   const float2 inv = make_float2(rcp_a(pd.x), rcp_a(pd.y));
   const float2 vn = __ffma2_rn(num, ee, num);
-  const float2 pn = __fmul2_rn(q.pmf1, p4);
   if constexpr (PAIR) {
     a.vdw = __ffma2_rn(vn, inv, a.vdw);
-    a.pmf = __ffma2_rn(pn, inv, a.pmf);
+    a.pmf = __ffma2_rn(p4, inv, a.pmf);
   } else {
     a.vdw.x = __fmaf_rn(vn.x, inv.x, a.vdw.x);
-    a.pmf.x = __fmaf_rn(pn.x, inv.x, a.pmf.x);
+    a.pmf.x = __fmaf_rn(p4.x, inv.x, a.pmf.x);
   }
   if (HDB) {
-    const float2 h = __ffma2_rn(r, q.hc1, q.hc0);
+    const float2 h = __ffma2_rn(__fmul2_rn(d2, ri), q.hc1, q.hc0);
     const float2 hh = __fmul2_rn(h, h);
     if constexpr (PAIR)
       a.hdb = __ffma2_rn(q.hs, make_float2(ex2_a(-hh.x), ex2_a(-hh.y)), a.hdb);
@@ -711,7 +711,7 @@ __global__ void __launch_bounds__(GD_MAX_TPB / PACK, GD_MIN_BLOCKS_PACK(UNROLL, 
             const float4 q0 = __ldg(pr), q1 = __ldg(pr + 1), q2 = __ldg(pr + 2);
             Pair2 pq;
             pq.p1a = f2(q0.x); pq.mp2a = f2(-q0.y); pq.p1l = f2(q0.z);
-            pq.pmf1 = f2(q1.y); pq.hc1 = f2(q1.z); pq.hc0 = f2(q1.w);
+            pq.p1ll = f2(q0.z * f.lj1); pq.hc1 = f2(q1.z); pq.hc0 = f2(q1.w);
             pq.hs = f2(q2.x); pq.b2 = f2(q2.z); pq.c2 = f2(q2.w);
             const float2 z2 = f2(0.0f);
             Acc acc[PACK];
@@ -724,7 +724,7 @@ __global__ void __launch_bounds__(GD_MAX_TPB / PACK, GD_MIN_BLOCKS_PACK(UNROLL, 
               const int v = vl[h];
               part[0 * T + v] += (double)acc[h].vdw.x + (double)acc[h].vdw.y;
               part[1 * T + v] += (double)acc[h].ele.x + (double)acc[h].ele.y;
-              part[2 * T + v] += (double)acc[h].pmf.x + (double)acc[h].pmf.y;
+              part[2 * T + v] += (double)q1.y * ((double)acc[h].pmf.x + (double)acc[h].pmf.y);
               part[4 * T + v] += (double)acc[h].hdb.x + (double)acc[h].hdb.y;
             }
           }
