@@ -39,6 +39,16 @@ float contact_threshold(float pmf0) {
   return t;
 }
 
+double pmf_far_radius(float pmf0) {
+  /* Beyond the larger root r* of (r/2 - 6)(r - pmf0) = 26 / log2(e), which lies past
+   * max(12, pmf0), the product only grows, so the pmf exponent in base 2 stays below -26
+   * (below -25.5 as the kernel computes it in FP32, whose rounding there is under 0.01) */
+  const double k = 26.0 / 1.4426950408889634;
+  const double a = 6.0 + 0.5 * (double)pmf0;
+  const double r = a + std::sqrt(std::max(0.0, a * a - 2.0 * (6.0 * (double)pmf0 - k)));
+  return std::max(r, std::max(12.0, (double)pmf0));
+}
+
 float bits_as_float(int v) {
   float f;
   memcpy(&f, &v, sizeof(f));

@@ -71,6 +71,8 @@ int fail(int code, const char *fmt, ...);
 constexpr float kPi = 3.1415926535f; /* reference src/size.h:67 */
 
 float contact_threshold(float pmf0);
+/* Distance beyond which the pair loop's far form gives its full form's result. */
+double pmf_far_radius(float pmf0);
 float bits_as_float(int v);
 float host_dist2(float ax, float ay, float az, float px, float py, float pz);
 

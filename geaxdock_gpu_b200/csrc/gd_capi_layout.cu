@@ -33,7 +33,8 @@ int layout_complex(gd_ctx *c, const gd_enepara *ff, const float (*thr)[GD_MAXTP1
   std::vector<int> sr_start;
 
   /* protein, all-pairs copy: sort by point type into segments that start on even slots (one
-   * padding slot after an odd-length segment), then write slot pairs */
+   * padding slot after an odd-length segment), each segment by distance from the pocket
+   * centre, then write slot pairs */
   std::vector<int4> seg((size_t)d.n_prt * GD_MAX_SEG, make_int4(0, 0, 0, 0));
   std::vector<int> seg_count(d.n_prt, 0);
   std::vector<std::vector<int>> slot_point(d.n_prt); /* point index per slot, -1: padding */
@@ -46,12 +47,24 @@ int layout_complex(gd_ctx *c, const gd_enepara *ff, const float (*thr)[GD_MAXTP1
   for (int tp = 0; tp < GD_MAXTP1; ++tp)
     for (int tl = 0; tl < GD_MAXTP2; ++tl)
       if (lt_used[tl] && ff->hdb0[tl][tp] > 0.1f) hdb_live[tp] = true;
+  /* distance of every point from the pocket centre (the kernel's float centre) */
+  std::vector<double> rad((size_t)d.n_prt * P);
+  double rad_max = 0.0;
+  for (size_t i = 0; i < rad.size(); ++i) {
+    const double dx = (double)d.prt_x[i] - (double)g.pocket[0];
+    const double dy = (double)d.prt_y[i] - (double)g.pocket[1];
+    const double dz = (double)d.prt_z[i] - (double)g.pocket[2];
+    rad[i] = std::sqrt(dx * dx + dy * dy + dz * dz);
+    rad_max = std::max(rad_max, rad[i]);
+  }
   for (int pc = 0; pc < d.n_prt; ++pc) {
     const int o = pc * P;
     std::vector<int> order(P);
     for (int p = 0; p < P; ++p) order[p] = p;
-    std::stable_sort(order.begin(), order.end(),
-                     [&](int a, int b) { return d.prt_t[o + a] < d.prt_t[o + b]; });
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+      const int ta = d.prt_t[o + a], tb = d.prt_t[o + b];
+      return ta != tb ? ta < tb : rad[o + a] < rad[o + b];
+    });
     std::vector<int> &sp = slot_point[pc];
     int ns = 0;
     for (int i = 0; i < P; ++i) {
@@ -69,6 +82,34 @@ int layout_complex(gd_ctx *c, const gd_enepara *ff, const float (*thr)[GD_MAXTP1
     }
     seg_count[pc] = ns;
     max_slots = std::max(max_slots, (int)sp.size());
+  }
+  /* far-point counts per (conformer, segment, radius bin), and the pmf far radius: the largest
+   * pmf_far_radius of the complex's type pairs plus 0.01 A for the kernel's FP32 distances */
+  const double bin_w = (rad_max + 1e-3) / (GD_FAR_BINS - 1);
+  std::vector<unsigned short> far_cnt((size_t)d.n_prt * GD_MAX_SEG * GD_FAR_BINS, 0);
+  for (int pc = 0; pc < d.n_prt; ++pc)
+    for (int sg = 0; sg < seg_count[pc]; ++sg) {
+      const int4 gs = seg[(size_t)pc * GD_MAX_SEG + sg];
+      if (gs.y - gs.x > 65535) return fail(GD_ERR_CAPACITY, "point segment too long");
+      unsigned short *fc = &far_cnt[((size_t)pc * GD_MAX_SEG + sg) * GD_FAR_BINS];
+      int n = 0;
+      for (int b = 0; b < GD_FAR_BINS; ++b) {
+        const double lim = (b + 1) * bin_w;
+        while (gs.x + n < gs.y && (b == GD_FAR_BINS - 1 ||
+                                   rad[(size_t)pc * P + slot_point[pc][gs.x + n]] < lim))
+          ++n;
+        fc[b] = (unsigned short)n;
+      }
+    }
+  {
+    bool pt_used[GD_MAXTP1] = {false};
+    for (int i = 0; i < d.n_prt * P; ++i) pt_used[d.prt_t[i]] = true;
+    double rfar = 0.0;
+    for (int tl = 0; tl < GD_MAXTP2; ++tl)
+      for (int tp = 0; tp < GD_MAXTP1; ++tp)
+        if (lt_used[tl] && pt_used[tp]) rfar = std::max(rfar, pmf_far_radius(ff->pmf0[tl][tp]));
+    g.far_r = (float)(rfar + 0.01);
+    g.far_inv_w = (float)(1.0 / bin_w);
   }
   const int PP = (max_slots + 3) & ~3;
   c->info[ci].pnp_pad = PP;
@@ -212,13 +253,13 @@ int layout_complex(gd_ctx *c, const gd_enepara *ff, const float (*thr)[GD_MAXTP1
 
   float4 *p_lig_pos; int2 *p_lig_meta; float *p_lig_center; float4 *p_pt_a, *p_pt_b;
   float4 *p_sr_a, *p_sr_b; int *p_sr_start;
-  int4 *p_seg; int *p_seg_count; float4 *p_kde; float *p_mx, *p_my, *p_mz, *p_mt, *p_psp, *p_mb;
+  int4 *p_seg; int *p_seg_count; unsigned short *p_far_cnt; float4 *p_kde; float *p_mx, *p_my, *p_mz, *p_mt, *p_psp, *p_mb;
   int *p_ref_start; float4 *p_ref_pts;
   if ((rc = upload(c, &p_lig_pos, lig_pos)) || (rc = upload(c, &p_lig_meta, lig_meta)) ||
       (rc = upload(c, &p_lig_center, lig_center)) || (rc = upload(c, &p_pt_a, pt_a)) ||
       (rc = upload(c, &p_pt_b, pt_b)) || (rc = upload(c, &p_sr_a, sr_a)) ||
       (rc = upload(c, &p_sr_b, sr_b)) || (rc = upload(c, &p_sr_start, sr_start)) ||
-      (rc = upload(c, &p_seg, seg)) ||
+      (rc = upload(c, &p_seg, seg)) || (rc = upload(c, &p_far_cnt, far_cnt)) ||
       (rc = upload(c, &p_seg_count, seg_count)) || (rc = upload(c, &p_kde, kde)) ||
       (rc = upload(c, &p_mx, mx)) || (rc = upload(c, &p_my, my)) ||
       (rc = upload(c, &p_mz, mz)) || (rc = upload(c, &p_mt, mt)) ||
@@ -230,6 +271,7 @@ int layout_complex(gd_ctx *c, const gd_enepara *ff, const float (*thr)[GD_MAXTP1
     return fail(GD_ERR_CUDA, "upload failed: %s", cudaGetErrorString(cudaGetLastError()));
   g.lig_pos = p_lig_pos; g.lig_meta = p_lig_meta; g.lig_center = p_lig_center;
   g.pt_a = p_pt_a; g.pt_b = p_pt_b; g.seg = p_seg; g.seg_count = p_seg_count;
+  g.far_cnt = p_far_cnt;
   g.sr_a = p_sr_a; g.sr_b = p_sr_b; g.sr_start = p_sr_start;
   g.kde = p_kde; g.mcs_x = p_mx; g.mcs_y = p_my; g.mcs_z = p_mz; g.mcs_tcc = p_mt;
   g.psp = p_psp; g.minus_beta = p_mb; g.ref_start = p_ref_start; g.ref_pts = p_ref_pts;

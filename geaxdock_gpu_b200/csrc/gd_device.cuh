@@ -32,6 +32,7 @@
 #include "../../include/geauxdock_b200.h"
 
 #define GD_MAX_SEG 32          /* point types (30), rounded up */
+#define GD_FAR_BINS 64         /* radius bins of the far-point counts (GdDevComplex.far_cnt) */
 #define GD_CELL 4.0f           /* edge of the short-range cell grid (A) */
 /* shared-memory bytes of the contact-threshold table at the front of the kernel's buffer */
 #define GD_THR_BYTES (GD_MAXTP2 * GD_MAXTP1 * 4)
@@ -94,6 +95,13 @@ struct GdDevComplex {
   const float *minus_beta;    /* [n_tmp] */
   const int *ref_start;       /* [n_prt*(lna+1)] */
   const float4 *ref_pts;      /* [ref_start[n_prt*(lna+1)-1]] */
+  /* Within each segment the points run by distance from the pocket centre. far_cnt[(pc *
+   * GD_MAX_SEG + seg) * GD_FAR_BINS + b]: how many of the segment's points lie closer than
+   * (b + 1) / far_inv_w to the centre (all of them at the last bin). A point further than
+   * far_r + (an atom's distance from the centre) from the centre is further than far_r from
+   * the atom, where every type pair's pmf exponent is below -25.5 in base 2. */
+  const unsigned short *far_cnt;
+  float far_r, far_inv_w;
 };
 
 /* One CTA's unit of work: `count` consecutive replicas of one protein conformer. */

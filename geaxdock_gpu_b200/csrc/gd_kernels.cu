@@ -121,8 +121,13 @@ __device__ __forceinline__ float2 f2(float v) { return make_float2(v, v); }
  * (vdw, the far form of ele, pmf; hdb on segments whose type has a live hydrogen-bond pair).
  * The short-range terms (contacts, psp, hpc, the electrostatic soft core) come from the cell
  * list pass, short_range(). PAIR = false: only the first slot is a point (the second is
- * segment padding) and nothing of the second is kept. */
-template <bool HDB, bool PAIR>
+ * segment padding) and nothing of the second is kept. FAR: both points lie beyond the atom's
+ * far radius, where the pmf exponent is below -25.5 in base 2 (the host's radius has a margin
+ * of 0.5 over the FP32 rounding of tt). There ee < 2^-25, so p4 + p4 ee rounds to p4 and
+ * num + num ee to num: the full body's terms are num rcp(p4) and p4 rcp(p4), which the far
+ * form computes without tt, ee, pd and vn, bit for bit; where a warp splits a segment into
+ * its near and far parts therefore changes no result. */
+template <bool HDB, bool PAIR, bool FAR>
 __device__ __forceinline__ void pair_body(const float4 A, const float4 B, float2 ax, float2 ay,
                                           float2 az, const Pair2 &q, const GdForceConst &f,
                                           Acc &a) {
@@ -149,6 +154,16 @@ __device__ __forceinline__ void pair_body(const float4 A, const float4 B, float2
   } else {
     a.ele.x = __fmaf_rn(ep.x, ri.x, a.ele.x);
   }
+  if constexpr (FAR) {
+    const float2 inv = make_float2(rcp_a(p4.x), rcp_a(p4.y));
+    if constexpr (PAIR) {
+      a.vdw = __ffma2_rn(num, inv, a.vdw);
+      a.pmf = __ffma2_rn(p4, inv, a.pmf);
+    } else {
+      a.vdw.x = __fmaf_rn(num.x, inv.x, a.vdw.x);
+      a.pmf.x = __fmaf_rn(p4.x, inv.x, a.pmf.x);
+    }
+  } else {
   /* pmf: pmf1 / (1 + exp((6 - r/2)(r - pmf0))) as exp2 of the expanded quadratic
    * cA d2 + b2 r + c2 = d2 (b2 r^-1 + cA) + c2 (cA = -log2(e)/2, b2 = log2(e)(6 + pmf0/2),
    * c2 = -6 log2(e) pmf0). Its maximum over r is log2(e) (12 - pmf0)^2 / 8 < 100 for
@@ -169,6 +184,7 @@ __device__ __forceinline__ void pair_body(const float4 A, const float4 B, float2
     a.vdw.x = __fmaf_rn(vn.x, inv.x, a.vdw.x);
     a.pmf.x = __fmaf_rn(p4.x, inv.x, a.pmf.x);
   }
+  }
   if (HDB) {
     const float2 h = __ffma2_rn(__fmul2_rn(d2, ri), q.hc1, q.hc0);
     const float2 hh = __fmul2_rn(h, h);
@@ -183,7 +199,7 @@ __device__ __forceinline__ void pair_body(const float4 A, const float4 B, float2
  * an odd i1 leaves one point for a half iteration. HDB: the segment's point type has a live
  * hydrogen-bond pair with some atom type of the ligand (decided per complex on the host, so
  * every warp of the CTA runs the same code). UNROLL: point pairs in flight per lane. */
-template <bool HDB, int UNROLL>
+template <bool HDB, int UNROLL, bool FAR>
 __device__ __forceinline__ void pair_range(const float4 *__restrict__ PA,
                                            const float4 *__restrict__ PB, int i0, int i1,
                                            float ax, float ay, float az, const Pair2 &q,
@@ -191,14 +207,15 @@ __device__ __forceinline__ void pair_range(const float4 *__restrict__ PA,
   const float2 ax2 = f2(ax), ay2 = f2(ay), az2 = f2(az);
   const int m0 = i0 >> 1, m1 = i1 >> 1;
 #pragma unroll UNROLL
-  for (int m = m0; m < m1; ++m) pair_body<HDB, true>(PA[m], PB[m], ax2, ay2, az2, q, f, a);
-  if (i1 & 1) pair_body<HDB, false>(PA[m1], PB[m1], ax2, ay2, az2, q, f, a);
+  for (int m = m0; m < m1; ++m)
+    pair_body<HDB, true, FAR>(PA[m], PB[m], ax2, ay2, az2, q, f, a);
+  if (i1 & 1) pair_body<HDB, false, FAR>(PA[m1], PB[m1], ax2, ay2, az2, q, f, a);
 }
 
 /* The same range for the same atom of two replicas (the lane's two slots): one load of each
  * point pair, one loop, the segment's parameters shared; each atom's sums are the operations
  * of pair_range in the same order, so its energies are bit-identical. */
-template <bool HDB, int UNROLL>
+template <bool HDB, int UNROLL, bool FAR>
 __device__ __forceinline__ void pair_range2(const float4 *__restrict__ PA,
                                             const float4 *__restrict__ PB, int i0, int i1,
                                             const float *ax, const float *ay, const float *az,
@@ -209,13 +226,13 @@ __device__ __forceinline__ void pair_range2(const float4 *__restrict__ PA,
 #pragma unroll UNROLL
   for (int m = m0; m < m1; ++m) {
     const float4 A = PA[m], B = PB[m];
-    pair_body<HDB, true>(A, B, ax0, ay0, az0, q, f, a[0]);
-    pair_body<HDB, true>(A, B, ax1, ay1, az1, q, f, a[1]);
+    pair_body<HDB, true, FAR>(A, B, ax0, ay0, az0, q, f, a[0]);
+    pair_body<HDB, true, FAR>(A, B, ax1, ay1, az1, q, f, a[1]);
   }
   if (i1 & 1) {
     const float4 A = PA[m1], B = PB[m1];
-    pair_body<HDB, false>(A, B, ax0, ay0, az0, q, f, a[0]);
-    pair_body<HDB, false>(A, B, ax1, ay1, az1, q, f, a[1]);
+    pair_body<HDB, false, FAR>(A, B, ax0, ay0, az0, q, f, a[0]);
+    pair_body<HDB, false, FAR>(A, B, ax1, ay1, az1, q, f, a[1]);
   }
 }
 
@@ -345,16 +362,16 @@ __device__ __forceinline__ double warp_sum(double v) {
 
 /* One segment range of the pair loop, dispatched on the segment's flags (bit 2: live
  * hydrogen-bond term). */
-template <int UNROLL, int PACK>
+template <int UNROLL, int PACK, bool FAR>
 __device__ __forceinline__ void pair_dispatch(int flags, const float4 *PA, const float4 *PB,
                                               int i0, int i1, const float *ax, const float *ay,
                                               const float *az, const Pair2 &pq,
                                               const GdForceConst &f, Acc *acc) {
 #define GD_PR(H)                                                                             \
   if constexpr (PACK == 2)                                                                   \
-    pair_range2<H, UNROLL>(PA, PB, i0, i1, ax, ay, az, pq, f, acc);                          \
+    pair_range2<H, UNROLL, FAR>(PA, PB, i0, i1, ax, ay, az, pq, f, acc);                     \
   else                                                                                       \
-    pair_range<H, UNROLL>(PA, PB, i0, i1, ax[0], ay[0], az[0], pq, f, acc[0])
+    pair_range<H, UNROLL, FAR>(PA, PB, i0, i1, ax[0], ay[0], az[0], pq, f, acc[0])
   if (flags & 4) {
     GD_PR(true);
   } else {
@@ -676,6 +693,21 @@ __global__ void __launch_bounds__(GD_MAX_TPB / PACK, GD_MIN_BLOCKS_PACK(UNROLL, 
         part[8 * T + v] = (double)sr.ncon;
       }
 
+      /* ---- far-point bin of the warp: a point further from the pocket centre than far_r +
+       * the largest distance of the warp's atoms from it is beyond far_r of each of them, and
+       * takes the far form of the pair body (the same result, fewer operations) ---- */
+      int fbin = 0;
+#pragma unroll
+      for (int h = 0; h < PACK; ++h) {
+        if (!ok[h]) continue;
+        const float dx = ax[h] - cx.pocket[0], dy = ay[h] - cx.pocket[1],
+                    dz = az[h] - cx.pocket[2];
+        const float rho = sqrtf(dx * dx + dy * dy + dz * dz) + cx.far_r;
+        fbin = max(fbin, (int)fminf(rho * cx.far_inv_w, (float)(GD_FAR_BINS - 1)));
+      }
+      fbin = (int)__reduce_max_sync(0xffffffffu, (unsigned)fbin);
+      const unsigned short *fcnt = cx.far_cnt + (size_t)pc * GD_MAX_SEG * GD_FAR_BINS + fbin;
+
       /* ---- CalcEnergy_d pair loop over the protein ring ---- */
       for (int ci = 0; ci < nch; ++ci) {
         const int q = resident ? ci : s * nch + ci;
@@ -717,7 +749,14 @@ __global__ void __launch_bounds__(GD_MAX_TPB / PACK, GD_MIN_BLOCKS_PACK(UNROLL, 
             Acc acc[PACK];
 #pragma unroll
             for (int h = 0; h < PACK; ++h) acc[h] = {z2, z2, z2, z2};
-            pair_dispatch<UNROLL, PACK>(g.w, PA, PB, i0, i1, ax, ay, az, pq, f, acc);
+            /* the segment's near points [i0, im) and far points [im, i1); the split slot is
+             * even (the segment starts on one), so the near part keeps whole slot pairs */
+            const int fs = g.x + ((__ldg(fcnt + sg * GD_FAR_BINS) + 1) & ~1) - c0;
+            const int im = min(i1, max(i0, fs));
+            if (i0 < im)
+              pair_dispatch<UNROLL, PACK, false>(g.w, PA, PB, i0, im, ax, ay, az, pq, f, acc);
+            if (im < i1)
+              pair_dispatch<UNROLL, PACK, true>(g.w, PA, PB, im, i1, ax, ay, az, pq, f, acc);
 #pragma unroll
             for (int h = 0; h < PACK; ++h) {
               if (!ok[h]) continue;
