@@ -40,11 +40,15 @@
 #define GD_MAX_CELLS_ALL (1 << 25) /* cells of all conformers of a complex together */
 #define GD_MAX_TPB 256         /* threads per CTA: 3 CTAs of 256 fit the register file */
 #define GD_SLOT_BYTES 192      /* shared-memory bytes per replica slot (sizeof gd::Slot) */
-/* resident 256-thread CTAs per SM the register budget is set for, per unroll depth */
-#define GD_MIN_BLOCKS(u) ((u) >= 4 ? 2 : ((u) >= 2 ? 3 : 4))
+/* resident 256-thread CTAs per SM the register budget is set for, per unroll depth: 80
+ * registers at four point pairs in flight, 64 below (no spills); the delayed-acceptance
+ * variants keep one CTA fewer (80 at two pairs, 128 at four), where 64 and 80 would spill */
+#define GD_MIN_BLOCKS(u) ((u) >= 4 ? 3 : 4)
+#define GD_MIN_BLOCKS_DA(u) ((u) >= 4 ? 2 : ((u) >= 2 ? 3 : 4))
 /* two replicas per thread: CTAs of at most GD_MAX_TPB / 2 threads (the tile's lanes over two),
  * 4 resident per SM with one point pair in flight per replica, 3 with two */
-#define GD_MIN_BLOCKS_PACK(u, p) ((p) == 2 ? ((u) >= 2 ? 3 : 4) : GD_MIN_BLOCKS(u))
+#define GD_MIN_BLOCKS_PACK(u, p, da) \
+  ((p) == 2 ? ((u) >= 2 ? 3 : 4) : ((da) ? GD_MIN_BLOCKS_DA(u) : GD_MIN_BLOCKS(u)))
 #define GD_MAX_SLOTS 128       /* replicas per CTA */
 #define GD_NQ 12               /* per-lane partial sums handed to the reducer */
 

@@ -480,7 +480,7 @@ __device__ __forceinline__ void da_decide(const GdMcArgs &a, const GdDevComplex 
  * word, the CTA leaves at the next step barrier after letting its copies in flight land.
  */
 template <int UNROLL, bool SPLIT, bool DA, int PACK>
-__global__ void __launch_bounds__(GD_MAX_TPB / PACK, GD_MIN_BLOCKS_PACK(UNROLL, PACK))
+__global__ void __launch_bounds__(GD_MAX_TPB / PACK, GD_MIN_BLOCKS_PACK(UNROLL, PACK, DA))
     gd_mc_kernel(GdMcArgs a, GdForceConst f) {
   static_assert(PACK == 1 || (PACK == 2 && !SPLIT && !DA),
                 "two replicas per lane: plain modes with one lane per atom");
