@@ -212,6 +212,32 @@ __device__ __forceinline__ void pair_range(const float4 *__restrict__ PA,
   if (i1 & 1) pair_body<HDB, false, FAR>(PA[m1], PB[m1], ax2, ay2, az2, q, f, a);
 }
 
+/* Pair loop of one of the S lanes of an atom (split sp) over slots [i0, i1) of a segment:
+ * every S-th point pair from pair i0 / 2 + sp, the pairs before slot im (even, or i1) in the
+ * full form and the rest in the far form; the odd tail point goes to the lane whose turn it
+ * is. Each lane's pairs and their order do not depend on im, and the two forms give the same
+ * result on far pairs, so neither does its sum. */
+template <bool HDB, int UNROLL>
+__device__ __forceinline__ void pair_range_split(const float4 *__restrict__ PA,
+                                                 const float4 *__restrict__ PB, int i0, int im,
+                                                 int i1, int sp, int S, float ax, float ay,
+                                                 float az, const Pair2 &q,
+                                                 const GdForceConst &f, Acc &a) {
+  const float2 ax2 = f2(ax), ay2 = f2(ay), az2 = f2(az);
+  const int mm = im >> 1, m1 = i1 >> 1;
+  int m = (i0 >> 1) + sp;
+#pragma unroll UNROLL
+  for (; m < mm; m += S) pair_body<HDB, true, false>(PA[m], PB[m], ax2, ay2, az2, q, f, a);
+#pragma unroll UNROLL
+  for (; m < m1; m += S) pair_body<HDB, true, true>(PA[m], PB[m], ax2, ay2, az2, q, f, a);
+  if ((i1 & 1) && m == m1) {
+    if (2 * m1 >= im)
+      pair_body<HDB, false, true>(PA[m1], PB[m1], ax2, ay2, az2, q, f, a);
+    else
+      pair_body<HDB, false, false>(PA[m1], PB[m1], ax2, ay2, az2, q, f, a);
+  }
+}
+
 /* The same range for the same atom of two replicas (the lane's two slots): one load of each
  * point pair, one loop, the segment's parameters shared; each atom's sums are the operations
  * of pair_range in the same order, so its energies are bit-identical. */
@@ -535,8 +561,8 @@ __global__ void __launch_bounds__(GD_MAX_TPB / PACK, GD_MIN_BLOCKS_PACK(UNROLL, 
       continue;
     }
     const GdDevComplex &cx = a.cx[tile.complex_index];
-    /* lane = (slot j, protein split sp, ligand atom l): the S copies of an atom each walk
-     * 1/S of every protein segment; S = 1 is one lane per atom */
+    /* lane = (slot j, protein split sp, ligand atom l): the S copies of an atom each take
+     * every S-th point pair of every protein segment; S = 1 is one lane per atom */
     const int L = cx.lna, S = SPLIT ? a.split : 1, SL = S * L;
     const int kp = (k + PACK - 1) / PACK; /* lane groups */
     const bool active = tid < kp * SL;
@@ -729,16 +755,8 @@ __global__ void __launch_bounds__(GD_MAX_TPB / PACK, GD_MIN_BLOCKS_PACK(UNROLL, 
           const int c0 = ci * D, c1 = min(pnp_pad, c0 + D);
           for (int sg = 0; sg < nseg; ++sg) {
             const int4 g = segs[sg];
-            int i0 = max(g.x, c0) - c0, i1 = min(g.y, c1) - c0;
+            const int i0 = max(g.x, c0) - c0, i1 = min(g.y, c1) - c0;
             if (i0 >= i1) continue;
-            if (S > 1) {
-              /* this split's run of point pairs (i0 is even; the odd tail goes to the last) */
-              const int np = (i1 - i0 + 1) >> 1;
-              const int e = i0 + 2 * (np * (sp + 1) / S);
-              i0 += 2 * (np * sp / S);
-              i1 = min(i1, e);
-              if (i0 >= i1) continue;
-            }
             const float4 *pr = reinterpret_cast<const float4 *>(pprow + g.z);
             const float4 q0 = __ldg(pr), q1 = __ldg(pr + 1), q2 = __ldg(pr + 2);
             Pair2 pq;
@@ -753,10 +771,20 @@ __global__ void __launch_bounds__(GD_MAX_TPB / PACK, GD_MIN_BLOCKS_PACK(UNROLL, 
              * even (the segment starts on one), so the near part keeps whole slot pairs */
             const int fs = g.x + ((__ldg(fcnt + sg * GD_FAR_BINS) + 1) & ~1) - c0;
             const int im = min(i1, max(i0, fs));
-            if (i0 < im)
-              pair_dispatch<UNROLL, PACK, false>(g.w, PA, PB, i0, im, ax, ay, az, pq, f, acc);
-            if (im < i1)
-              pair_dispatch<UNROLL, PACK, true>(g.w, PA, PB, im, i1, ax, ay, az, pq, f, acc);
+            if constexpr (SPLIT) {
+              /* the S lanes of an atom take every S-th point pair of the range */
+              if (g.w & 4)
+                pair_range_split<true, UNROLL>(PA, PB, i0, im, i1, sp, S, ax[0], ay[0], az[0],
+                                               pq, f, acc[0]);
+              else
+                pair_range_split<false, UNROLL>(PA, PB, i0, im, i1, sp, S, ax[0], ay[0], az[0],
+                                                pq, f, acc[0]);
+            } else {
+              if (i0 < im)
+                pair_dispatch<UNROLL, PACK, false>(g.w, PA, PB, i0, im, ax, ay, az, pq, f, acc);
+              if (im < i1)
+                pair_dispatch<UNROLL, PACK, true>(g.w, PA, PB, im, i1, ax, ay, az, pq, f, acc);
+            }
 #pragma unroll
             for (int h = 0; h < PACK; ++h) {
               if (!ok[h]) continue;
