@@ -105,6 +105,32 @@ def test_unroll_depths_give_identical_energies(raw):
     assert worst.max() <= TOL, worst
 
 
+def test_far_pair_form_does_not_depend_on_warp_mates(raw):
+    """Within each point segment the pair loop switches to the far form of the pair body at a
+    slot set by the largest distance of the warp's atoms from the pocket centre. The far form
+    gives the full form's result bit for bit, so a pose's energies do not depend on the poses
+    that share its warps: one pose per CTA, six per CTA, the poses in another order, and a pose
+    moved 15 A out of the pocket beside the others all give the same bytes."""
+    w = system.config(1, raw)
+    cx, ff = w.complexes[0], w.ff
+    rng = np.random.default_rng(33)
+    mm = rng.normal(0, 0.6, (12, 6)).astype(np.float32)
+    mm[5, :3] = [15.0, -4.0, 6.0]
+    perm = rng.permutation(12)
+    inv = np.empty_like(perm)
+    inv[perm] = np.arange(12)
+    runs = []
+    with engine.Engine(ff, [cx], w.params) as eng:
+        for k in (1, 6):
+            eng.set_tile(k, 1024)
+            runs.append(eng.eval_energy(0, 2, 4, mm))
+            runs.append(eng.eval_energy(0, 2, 4, mm[perm])[inv])
+        worst = _energy_check(eng, ff, cx, 0, 2, 4, mm, po.ref_map(ff, cx))
+    for r in runs[1:]:
+        assert r.tobytes() == runs[0].tobytes()
+    assert worst.max() <= TOL, worst
+
+
 def _init_and_compare(eng, ff, cx, w_params):
     eng.mc_init()
     eng.sync()
