@@ -3,9 +3,11 @@
  * the per-complex bookkeeping, the error reporting, and the launch and buffer helpers.
  *
  *   gd_capi.cu          the context, its uploads and tile lists, the Monte Carlo calls,
- *                       records, state, pose evaluation and placement (the reference's Run
- *                       and launcher, src/run.cu:33-288, src/kernel_cuda_lancher_siglegpu.cu)
+ *                       records and state (the reference's Run and launcher, src/run.cu:33-288,
+ *                       src/kernel_cuda_lancher_siglegpu.cu)
+ *   gd_capi_layout.cu   the device layout of one complex
  *   gd_capi_stream.cu   records downloaded while the run proceeds (gd_records_stream)
+ *   gd_capi_eval.cu     pose energies, placed coordinates and the energy trace
  *   gd_capi_noalloc.cu  pose energies without allocation (gd_eval_energy_noalloc)
  *   gd_capi_da.cu       the surrogate, delayed acceptance and its fallback controller, the
  *                       standalone network and k-means entry points
