@@ -15,7 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgeauxdock_b200.so")
 SOURCES = ["gd_kernels.cu", "gd_capi.cu", "gd_capi_layout.cu", "gd_capi_stream.cu",
-           "gd_capi_noalloc.cu", "gd_capi_da.cu", "gd_capi_eval.cu",
+           "gd_capi_noalloc.cu", "gd_capi_da.cu", "gd_capi_eval.cu", "gd_capi_tile.cu",
            "gd_peak.cu", "gd_mlp.cu", "gd_da.cu", "gd_umma.cu", "gd_kmeans.cu"]
 HEADERS = ["gd_capi_internal.cuh", "gd_device.cuh", "gd_numerics.h", "gd_mlp.cuh", "gd_mlp_fwd.cuh", "gd_umma.cuh", "gd_kmeans.cuh", os.path.join("..", "..", "include", "geauxdock_b200.h")]
 

@@ -6,6 +6,7 @@
  *                       records and state (the reference's Run and launcher, src/run.cu:33-288,
  *                       src/kernel_cuda_lancher_siglegpu.cu)
  *   gd_capi_layout.cu   the device layout of one complex
+ *   gd_capi_tile.cu     the tile, its autotuning, chains, RNG streams and the wait bound
  *   gd_capi_stream.cu   records downloaded while the run proceeds (gd_records_stream)
  *   gd_capi_eval.cu     pose energies, placed coordinates and the energy trace
  *   gd_capi_noalloc.cu  pose energies without allocation (gd_eval_energy_noalloc)
