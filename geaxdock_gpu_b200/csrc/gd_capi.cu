@@ -217,6 +217,10 @@ int check_complex(const gd_complex_desc &d, int idx) {
       return fail(GD_ERR_INVALID, "complex %d: protein point %d has a non-finite coordinate", idx,
                   i);
   }
+  /* the pair loop orders each segment's points by distance from the pocket centre */
+  for (int a = 0; a < 3; ++a)
+    if (!std::isfinite(d.pocket_center[a]))
+      return fail(GD_ERR_INVALID, "complex %d: the pocket centre has a non-finite coordinate", idx);
   for (int i = 0; i < d.pnk; ++i)
     if (d.kde_t[i] < 0 || d.kde_t[i] >= GD_MAXTP2)
       return fail(GD_ERR_INVALID, "complex %d: KDE type out of range", idx);

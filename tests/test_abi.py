@@ -111,6 +111,13 @@ def test_invalid_arguments_are_rejected_with_a_message():
     rc = lib.gd_create(C.byref(ff), C.byref(d), 1, C.byref(params), 0, C.byref(h))
     assert rc == abi.GD_ERR_INVALID
     assert b"non-finite" in lib.gd_last_error_string()
+    # so is a pocket centre off the number line (the points are ordered by distance from it)
+    off = copy.deepcopy(cx)
+    off.pocket_center = np.array([0.0, np.inf, 0.0], np.float32)
+    d = off.desc()
+    rc = lib.gd_create(C.byref(ff), C.byref(d), 1, C.byref(params), 0, C.byref(h))
+    assert rc == abi.GD_ERR_INVALID
+    assert b"pocket centre" in lib.gd_last_error_string()
     assert lib.gd_release_memory(-1) == abi.GD_ERR_INVALID
 
 
