@@ -1,4 +1,4 @@
-"""The pmf far radius behind the pair loop's far form, checked on the CPU.
+"""The pmf far radius and the far-point bins behind the pair loop's far form, checked on the CPU.
 
 The host sets the far radius r* of a type pair from (r/2 - 6)(r - pmf0) = 26 / log2(e)
 (`pmf_far_radius` in geaxdock_gpu_b200/csrc/gd_capi.cu, restated here). Beyond it the kernel's
@@ -53,3 +53,39 @@ def test_far_radius_bounds_the_fp32_pmf_exponent():
         v = np.float32(2.0) ** np.linspace(-20, 40, 2001).astype(np.float32)
         v = np.concatenate([v, np.nextafter(v, np.float32(0)), -v]).astype(np.float32)
         assert np.array_equal(_fma32(v, np.full_like(v, ee), v), v)
+
+
+def test_far_bins_put_only_far_points_past_the_switch_slot():
+    """The table and the switch slot, restated: the host counts each segment's points (ordered
+    by distance from the pocket centre) inside radius (b + 1) w for 64 bins, all of them at the
+    last (`layout_complex`); a warp takes b = min(63, floor((max atom distance + far_r) / w)) in
+    FP32 and switches at the count rounded up to even (`gd_mc_kernel`). Every point from there on
+    must lie beyond far_r of every atom of the warp, on random pockets and atoms, atoms inside
+    and outside the point cloud."""
+    rng = np.random.default_rng(5)
+    nb = 64
+    checked = 0
+    for trial in range(200):
+        n = int(rng.integers(1, 400))
+        centre = rng.normal(0, 20, 3).astype(np.float32)
+        pts = (centre + rng.normal(0, rng.uniform(3, 30), (n, 3))).astype(np.float32)
+        rad = np.linalg.norm(pts.astype(np.float64) - centre.astype(np.float64), axis=1)
+        order = np.argsort(rad, kind="stable")
+        pts, rad = pts[order], rad[order]
+        far_r = np.float32(far_radius(float(rng.uniform(2.5, 7.5))) + 0.01)
+        w = (rad.max() + 1e-3) / (nb - 1)
+        cnt = np.array([np.count_nonzero(rad < (b + 1) * w) for b in range(nb)])
+        cnt[-1] = n
+        inv_w = np.float32(1.0 / w)
+        atoms = (centre + rng.normal(0, rng.uniform(1, 25), (32, 3))).astype(np.float32)
+        d = atoms - centre
+        a = np.sqrt((d * d).sum(axis=1, dtype=np.float32), dtype=np.float32)
+        rho = (a + far_r).astype(np.float32)
+        b = int(np.minimum(np.floor(rho * inv_w), np.float32(nb - 1)).max())
+        split = (int(cnt[b]) + 1) & ~1
+        if split >= n:
+            continue
+        dist = np.linalg.norm(pts[split:, None, :].astype(np.float64) - atoms[None, :, :], axis=2)
+        assert dist.min() >= far_r - 1e-4, (trial, dist.min(), far_r)
+        checked += 1
+    assert checked > 50, checked
